@@ -1,0 +1,244 @@
+"""ctypes bindings for the oracle libraries -- TEST INFRASTRUCTURE ONLY.
+
+Arrays follow xFluid's layout (numpy shape (nk, nj, ni), faces
+(nk,nj,ni+1) / (nk,nj+1,ni) / (nk+1,nj,ni)); all values are float64.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SRC = HERE / "xfp_oracle.c"
+ORACLE_LIB = HERE / "_build" / "libxfp_oracle.so"
+REF_LIB = HERE / "_ref" / "libxfref.so"
+
+_dp = C.POINTER(C.c_double)
+_u8 = C.POINTER(C.c_uint8)
+
+
+def build_oracle(force: bool = False) -> Path:
+    """Compile the C restatement (gcc, -O2, no FP contraction)."""
+    if ORACLE_LIB.exists() and not force and ORACLE_LIB.stat().st_mtime >= ORACLE_SRC.stat().st_mtime:
+        return ORACLE_LIB
+    ORACLE_LIB.parent.mkdir(parents=True, exist_ok=True)
+    tmp = ORACLE_LIB.with_suffix(".so.tmp")
+    subprocess.check_call(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off",
+                           "-fno-fast-math", str(ORACLE_SRC), "-lm", "-o", str(tmp)])
+    os.replace(tmp, ORACLE_LIB)
+    return ORACLE_LIB
+
+
+def build_reference(ref_root: str | None = None) -> Path | None:
+    """Compile xFluid's own solver into oracle/_ref when its sources exist."""
+    env = dict(os.environ)
+    if ref_root:
+        env["XFLUID_REF"] = ref_root
+    root = Path(env.get("XFLUID_REF", "/root/reference"))
+    if not (root / "xFluid" / "xFluid" / "variationalpressure").is_dir():
+        return None
+    subprocess.check_call(["bash", str(HERE / "build_ref.sh")], env=env,
+                          stdout=subprocess.DEVNULL)
+    return REF_LIB
+
+
+def oracle_available() -> bool:
+    return ORACLE_LIB.exists()
+
+
+def reference_available() -> bool:
+    return REF_LIB.exists()
+
+
+def _p(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_dp if a.dtype == np.float64 else _u8)
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+class _Lib:
+    def __init__(self, path: Path):
+        if not path.exists():
+            raise FileNotFoundError(f"oracle library missing: {path}")
+        self.lib = C.CDLL(str(path))
+
+
+class Oracle(_Lib):
+    """The FP64 C restatement (oracle/xfp_oracle.c)."""
+
+    def __init__(self):
+        super().__init__(ORACLE_LIB if ORACLE_LIB.exists() else build_oracle())
+        L = self.lib
+        L.xo_assemble.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 11
+        L.xo_spmv.argtypes = [C.c_int] * 3 + [_dp] * 6
+        L.xo_factor.argtypes = [C.c_int] * 3 + [_dp] * 4 + [C.c_double] * 2 + [_dp] * 4
+        L.xo_precond.argtypes = [C.c_int] * 3 + [_dp] * 6
+        L.xo_pcg.argtypes = ([C.c_int] * 3 + [_dp] * 5 + [C.c_double, C.c_int, C.c_double, C.c_double,
+                             _dp, C.POINTER(C.c_int), _dp])
+        L.xo_pcg.restype = C.c_int
+        L.xo_apply.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 7
+        L.xo_apply_T.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 7
+        L.xo_rhs_T.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 7
+        L.xo_divergence_ref.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 4
+        L.xo_project.argtypes = ([C.c_int] * 3 + [_u8] + [_dp] * 6 + [C.c_double, C.c_int, _dp,
+                                 C.POINTER(C.c_int), _dp])
+        L.xo_project.restype = C.c_int
+
+    @staticmethod
+    def _dims(sc):
+        return sc.ni, sc.nj, sc.nk
+
+    def assemble(self, sc):
+        n = (sc.nk, sc.nj, sc.ni)
+        out = [np.zeros(n) for _ in range(5)]
+        u, v, w, wu, wv, ww = map(_f64, (sc.u, sc.v, sc.w, sc.wu, sc.wv, sc.ww))
+        self.lib.xo_assemble(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w),
+                             _p(wu), _p(wv), _p(ww), *[_p(a) for a in out])
+        return dict(zip(("diag", "ax", "ay", "az", "b"), out))
+
+    def spmv(self, sc, A, s):
+        z = np.zeros_like(A["diag"])
+        self.lib.xo_spmv(*self._dims(sc), _p(A["diag"]), _p(A["ax"]), _p(A["ay"]), _p(A["az"]),
+                         _p(_f64(s)), _p(z))
+        return z
+
+    def factor(self, sc, A, omega=0.97, ratio=0.25):
+        out = [np.zeros_like(A["diag"]) for _ in range(4)]
+        self.lib.xo_factor(*self._dims(sc), _p(A["diag"]), _p(A["ax"]), _p(A["ay"]), _p(A["az"]),
+                           omega, ratio, *[_p(a) for a in out])
+        return dict(zip(("inv", "lx", "ly", "lz"), out))
+
+    def precond(self, sc, F, r):
+        z = np.zeros_like(F["inv"])
+        self.lib.xo_precond(*self._dims(sc), _p(F["inv"]), _p(F["lx"]), _p(F["ly"]), _p(F["lz"]),
+                            _p(_f64(r)), _p(z))
+        return z
+
+    def pcg(self, sc, A, tol=1e-6, maxit=200, omega=0.97, ratio=0.25):
+        x = np.zeros_like(A["diag"])
+        it = C.c_int(0)
+        res = C.c_double(0)
+        ok = self.lib.xo_pcg(*self._dims(sc), _p(A["diag"]), _p(A["ax"]), _p(A["ay"]), _p(A["az"]),
+                             _p(A["b"]), tol, maxit, omega, ratio, _p(x), C.byref(it), C.byref(res))
+        return dict(ok=bool(ok), p=x, iters=it.value, resid=res.value)
+
+    def apply(self, sc, p):
+        u, v, w = (np.array(a, dtype=np.float64) for a in (sc.u, sc.v, sc.w))
+        wu, wv, ww = map(_f64, (sc.wu, sc.wv, sc.ww))
+        self.lib.xo_apply(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(wu), _p(wv), _p(ww),
+                          _p(_f64(p)), _p(u), _p(v), _p(w))
+        return u, v, w
+
+    def apply_T(self, sc, gu, gv, gw):
+        q = np.zeros((sc.nk, sc.nj, sc.ni))
+        wu, wv, ww = map(_f64, (sc.wu, sc.wv, sc.ww))
+        self.lib.xo_apply_T(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(wu), _p(wv), _p(ww),
+                            _p(_f64(gu)), _p(_f64(gv)), _p(_f64(gw)), _p(q))
+        return q
+
+    def rhs_T(self, sc, lam):
+        gu = np.zeros(sc.u.shape); gv = np.zeros(sc.v.shape); gw = np.zeros(sc.w.shape)
+        wu, wv, ww = map(_f64, (sc.wu, sc.wv, sc.ww))
+        self.lib.xo_rhs_T(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(wu), _p(wv), _p(ww),
+                          _p(_f64(lam)), _p(gu), _p(gv), _p(gw))
+        return gu, gv, gw
+
+    def divergence_ref(self, sc, u, v, w):
+        d = np.zeros((sc.nk, sc.nj, sc.ni))
+        self.lib.xo_divergence_ref(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(_f64(u)),
+                                   _p(_f64(v)), _p(_f64(w)), _p(d))
+        return d
+
+    def project(self, sc, tol=1e-6, maxit=200):
+        """Full projection (assemble, PCG, apply).  Returns dict with p, u, v, w."""
+        u, v, w = (np.array(a, dtype=np.float64) for a in (sc.u, sc.v, sc.w))
+        wu, wv, ww = map(_f64, (sc.wu, sc.wv, sc.ww))
+        p = np.zeros((sc.nk, sc.nj, sc.ni))
+        it = C.c_int(0)
+        res = C.c_double(0)
+        ok = self.lib.xo_project(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w),
+                                 _p(wu), _p(wv), _p(ww), tol, maxit, _p(p), C.byref(it), C.byref(res))
+        return dict(ok=bool(ok), p=p, u=u, v=v, w=w, iters=it.value, resid=res.value)
+
+    def weighted_divergence(self, sc, u, v, w):
+        """Per-cell m-weighted divergence that the projection drives to zero:
+        the right-hand side b assembled from the given face velocities."""
+        s2 = sc.copy()
+        s2.u, s2.v, s2.w = u, v, w
+        return self.assemble(s2)["b"]
+
+
+class Reference(_Lib):
+    """xFluid's own solver, built from the reference sources (oracle/_ref)."""
+
+    def __init__(self):
+        super().__init__(REF_LIB)
+        L = self.lib
+        L.xfref_solve.argtypes = ([C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_double, C.c_int, _dp,
+                                  C.POINTER(C.c_int), _dp])
+        L.xfref_solve.restype = C.c_int
+        L.xfref_project.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_double, C.c_int, _dp]
+        L.xfref_project.restype = C.c_int
+        L.xfref_apply.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 4
+        L.xfref_assemble.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 8
+        L.xfref_assemble.restype = C.c_int
+        L.xfref_factor.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 7
+        L.xfref_precond.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 5
+        L.xfref_divergence.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 4
+
+    def _in(self, sc):
+        return (sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(_f64(sc.u)),
+                _p(_f64(sc.v)), _p(_f64(sc.w)))
+
+    def solve(self, sc, tol=1e-6, maxit=200):
+        p = np.zeros((sc.nk, sc.nj, sc.ni))
+        it = C.c_int(0)
+        res = C.c_double(0)
+        ok = self.lib.xfref_solve(*self._in(sc), tol, maxit, _p(p), C.byref(it), C.byref(res))
+        return dict(ok=bool(ok), p=p, iters=it.value, resid=res.value)
+
+    def project(self, sc, tol=1e-6, maxit=200):
+        u, v, w = (np.array(a, dtype=np.float64) for a in (sc.u, sc.v, sc.w))
+        p = np.zeros((sc.nk, sc.nj, sc.ni))
+        ok = self.lib.xfref_project(sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(u),
+                                    _p(v), _p(w), tol, maxit, _p(p))
+        return dict(ok=bool(ok), p=p, u=u, v=v, w=w)
+
+    def apply(self, sc, p):
+        u, v, w = (np.array(a, dtype=np.float64) for a in (sc.u, sc.v, sc.w))
+        self.lib.xfref_apply(sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(_f64(p)),
+                             _p(u), _p(v), _p(w))
+        return u, v, w
+
+    def assemble(self, sc):
+        n = (sc.nk, sc.nj, sc.ni)
+        out = [np.zeros(n) for _ in range(5)]
+        maxrow = self.lib.xfref_assemble(*self._in(sc), *[_p(a) for a in out])
+        d = dict(zip(("diag", "ax", "ay", "az", "b"), out))
+        d["maxrow"] = maxrow
+        return d
+
+    def factor(self, sc):
+        n = (sc.nk, sc.nj, sc.ni)
+        out = [np.zeros(n) for _ in range(4)]
+        self.lib.xfref_factor(*self._in(sc), *[_p(a) for a in out])
+        return dict(zip(("inv", "lx", "ly", "lz"), out))
+
+    def precond(self, sc, r):
+        z = np.zeros((sc.nk, sc.nj, sc.ni))
+        self.lib.xfref_precond(*self._in(sc), _p(_f64(r)), _p(z))
+        return z
+
+    def divergence(self, sc, u, v, w):
+        d = np.zeros((sc.nk, sc.nj, sc.ni))
+        self.lib.xfref_divergence(sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(_f64(u)),
+                                  _p(_f64(v)), _p(_f64(w)), _p(d))
+        return d

@@ -1,0 +1,68 @@
+"""Generate the golden vectors in tests/golden/ from xFluid's own solver.
+
+The reference ships no tests, fixtures or known-answer vectors, so the golden
+vectors are produced by running the reference code itself: oracle/build_ref.sh
+compiles xFluid's VariationalPressureSolver / PCGSolver from the reference
+sources into oracle/_ref/libxfref.so and this script drives it on small seeded
+scenes (reference mode: all faces fully open).  Run from the repository root:
+
+    python tests/golden/make_golden.py
+
+Each ``<case>.npz`` holds the scene inputs and the reference's outputs:
+assembly (diag, ax, ay, az, b), MIC(0) factor (inv, lx, ly, lz), the
+preconditioner applied to a seeded residual (r -> z), the PCG pressure at
+tol 1e-6 (iterations, residual), the velocities after applyPressure, and the
+reference's divergence diagnostic after the projection.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle import Reference, build_reference  # noqa: E402
+from xfluid_b200 import scenes  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+TOL, MAXIT = 1e-6, 500
+
+
+def cases():
+    return {
+        "dam16": scenes.dam_break(16, seed=1, noise=0.3),
+        "dam20x14x18": scenes.dam_break(dims=(20, 14, 18), seed=2, noise=0.5),
+        "blob24x20x22": scenes.blob_scene(dims=(24, 20, 22), seed=5, fractional=False, dtype=np.float64),
+        "pool20x22x18": scenes.pool_drop(dims=(20, 22, 18), seed=2, dtype=np.float64).reference_mode(),
+    }
+
+
+def main():
+    if build_reference() is None:
+        raise SystemExit("reference sources not found; cannot regenerate golden vectors")
+    R = Reference()
+    for name, sc in cases().items():
+        A = R.assemble(sc)
+        F = R.factor(sc)
+        rng = np.random.default_rng(7)
+        r = rng.standard_normal(A["diag"].shape) * (A["diag"] != 0)
+        z = R.precond(sc, r)
+        sol = R.solve(sc, TOL, MAXIT)
+        assert sol["ok"], name
+        u2, v2, w2 = R.apply(sc, sol["p"])
+        div = R.divergence(sc, u2, v2, w2)
+        np.savez_compressed(
+            OUT / f"{name}.npz",
+            dims=np.array([sc.ni, sc.nj, sc.nk]), mat=sc.mat, u=sc.u, v=sc.v, w=sc.w,
+            diag=A["diag"], ax=A["ax"], ay=A["ay"], az=A["az"], b=A["b"], maxrow=A["maxrow"],
+            inv=F["inv"], lx=F["lx"], ly=F["ly"], lz=F["lz"], r=r, z=z,
+            p=sol["p"], iters=sol["iters"], resid=sol["resid"], tol=TOL, maxit=MAXIT,
+            u_out=u2, v_out=v2, w_out=w2, div=div)
+        print(f"{name}: {int((A['diag'] != 0).sum())} rows, {sol['iters']} iterations")
+
+
+if __name__ == "__main__":
+    main()

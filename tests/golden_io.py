@@ -1,0 +1,23 @@
+"""Loader for the committed golden vectors (tests/golden/*.npz), produced by
+tests/golden/make_golden.py from xFluid's own solver."""
+from pathlib import Path
+
+import numpy as np
+
+from xfluid_b200.scenes import Scene
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+CASES = sorted(p.stem for p in GOLDEN.glob("*.npz"))
+
+
+def load(name):
+    g = dict(np.load(GOLDEN / f"{name}.npz"))
+    ni, nj, nk = (int(x) for x in g["dims"])
+    sc = Scene(ni, nj, nk, g["mat"], g["u"], g["v"], g["w"], name=name)
+    return sc, g
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))
