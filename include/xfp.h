@@ -1,0 +1,170 @@
+/* xfp.h -- C ABI of the B200-native pressure projection (libxfp.so).
+ *
+ * Drop-in for xFluid's VariationalPressureSolver
+ * (xFluid/xFluid/variationalpressure/variational_pressuresolver.h:30-44): the
+ * same method -- the variational MAC-grid Poisson matrix, MIC(0)-preconditioned
+ * CG in natural (lexicographic) order, and the pressure-gradient velocity
+ * update -- computed by hand-written sm_100a CUDA kernels.
+ *
+ * Grid layout is xFluid's Array3d (xFluid/xFluid/array3d.h:143-146): flat index
+ * k*ni*nj + j*ni + i.  Face arrays follow xFluid/xFluid/FluidSimulator.h:177-181:
+ * u is (ni+1, nj, nk), v is (ni, nj+1, nk), w is (ni, nj, nk+1), each flattened
+ * the same way with its own extents.  material holds xFluid's Material values
+ * (xFluid/xFluid/material.h:4-8): 0 air, 1 fluid, 2 solid.
+ *
+ * Optional face weights wu/wv/ww (same shapes as u/v/w, values in [0,1]) are
+ * open fractions that scale every face's contribution (fractional solids).
+ * Pass NULL for all three to get exactly xFluid's matrix.
+ *
+ * Pointers are host memory unless xfp_options.device_pointers is set, in which
+ * case they must be device memory on the context's device.  Calls on one
+ * context are not re-entrant; use one context per host thread (each context
+ * owns its stream and its scratch memory).
+ *
+ * Return codes: XFP_OK, XFP_NOT_CONVERGED (the last iterate is still written;
+ * xFluid instead leaves the pressure grid unsized and applies it anyway,
+ * variational_pressuresolver.cpp:80-86 with FluidSimulator.cpp:506-508), or a
+ * negative XFP_ERR_* code; xfp_last_error() gives the message.
+ */
+#ifndef XFP_H
+#define XFP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XFP_OK 0
+#define XFP_NOT_CONVERGED 1
+#define XFP_ERR_ARGS (-1)
+#define XFP_ERR_CUDA (-2)
+#define XFP_ERR_TIMEOUT (-3)
+#define XFP_ERR_NOMEM (-4)
+#define XFP_ERR_BREAKDOWN (-5)
+#define XFP_ERR_UNSUPPORTED (-6)
+
+/* Arithmetic used inside the solve (independent of the I/O type). */
+#define XFP_PREC_F64 0   /* FP64 throughout, operation order of xFluid's solver */
+#define XFP_PREC_F32 1   /* plain FP32: stencil, vectors, dots and factor in FP32 */
+#define XFP_PREC_MIXED 2 /* FP32 stencil/vectors; FP64 dots, MIC(0) pivots and
+                            iterative-refinement residual */
+
+typedef struct xfp_ctx xfp_ctx;
+
+typedef struct xfp_options {
+  double tol;            /* stop when |r|_inf <= tol*|b|_inf (pcg_solver.h:249-254,273) */
+  int max_iter;          /* PCG iteration cap (pcg_solver.h:231 default 100) */
+  double omega;          /* MIC(0) modification parameter (pcg_solver.h:87, 0.97) */
+  double min_diag_ratio; /* MIC(0) pivot safeguard (pcg_solver.h:87, 0.25) */
+  int precision;         /* XFP_PREC_* */
+  int device_pointers;   /* 1: array arguments are device pointers */
+  int device;            /* CUDA device ordinal */
+  int check_every;       /* PCG iterations per host convergence read (0: 8) */
+  double timeout_ms;     /* bound on any device-side wait (0: 2000 ms) */
+  int max_refine;        /* mixed: iterative-refinement cycles (0: 20) */
+  double inner_tol;      /* mixed: relative residual reduction per cycle (0: 1e-4) */
+  int tile_k;            /* sweep tile height in k-lines (0: default) */
+  void* stream;          /* cudaStream_t to run on; NULL: the context's own stream */
+} xfp_options;
+
+typedef struct xfp_stats {
+  int status;            /* same as the return code */
+  int iterations;        /* PCG iterations (summed over refinement cycles) */
+  int refinements;       /* mixed precision: refinement cycles run */
+  double residual;       /* final |b - A p|_inf (recursive residual for F64/F32) */
+  double rel_residual;   /* residual / |b|_inf */
+  double b_inf;          /* |b|_inf */
+  long long rows;        /* unknown rows: fluid cells + solid cells next to fluid */
+  long long stored;      /* cells in the line-compacted storage (rows + padding) */
+  long long lines;       /* active x-lines */
+  double ms_setup;       /* layout + assembly */
+  double ms_factor;      /* MIC(0) factorisation */
+  double ms_solve;       /* PCG */
+  double ms_apply;       /* pressure scatter + velocity update */
+  double ms_total;       /* whole call incl. host<->device copies */
+  double bytes;          /* algorithmic bytes moved by the device kernels */
+} xfp_stats;
+
+/* Fills opt with defaults: tol 1e-5, max_iter 100, omega 0.97, ratio 0.25 --
+ * PCGSolver's constructor defaults (pcg_solver.h:229-232) -- FP64, host
+ * pointers, device 0. */
+void xfp_default_options(xfp_options* opt);
+
+/* Creates a context (device, stream, scratch pool).  Replaces constructing
+ * VariationalPressureSolver (variational_pressuresolver.cpp:8-9). */
+int xfp_create(xfp_ctx** ctx, const xfp_options* opt);
+int xfp_destroy(xfp_ctx* ctx);
+int xfp_set_options(xfp_ctx* ctx, const xfp_options* opt);
+const char* xfp_last_error(const xfp_ctx* ctx);
+const char* xfp_version(void);
+
+/* Solve for pressure.  Replaces VariationalPressureSolver::solve
+ * (variational_pressuresolver.cpp:50-118, with setSize/setVelocityField/
+ * setMaterial at :11-28): assembles the variational system (:231-327), runs
+ * MIC(0)-PCG (pcg_solver.h:243-285) and writes pressure for every cell
+ * (0 in rows without an unknown, :86-101).  pressure is ni*nj*nk. */
+int xfp_solve_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material,
+                  const double* u, const double* v, const double* w,
+                  const double* wu, const double* wv, const double* ww,
+                  double* pressure, xfp_stats* stats);
+int xfp_solve_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material,
+                  const float* u, const float* v, const float* w,
+                  const float* wu, const float* wv, const float* ww,
+                  float* pressure, xfp_stats* stats);
+
+/* Pressure-gradient update of u, v, w in place.  Replaces
+ * VariationalPressureSolver::applyPressure (variational_pressuresolver.cpp:120-220). */
+int xfp_apply_pressure_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material,
+                           const double* wu, const double* wv, const double* ww,
+                           const double* pressure, double* u, double* v, double* w);
+int xfp_apply_pressure_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material,
+                           const float* wu, const float* wv, const float* ww,
+                           const float* pressure, float* u, float* v, float* w);
+
+/* Solve and apply in one call, u/v/w updated in place: the pair
+ * FluidSimulator::_solvePressure issues (FluidSimulator.cpp:501-509).
+ * pressure may be NULL. */
+int xfp_project_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material,
+                    double* u, double* v, double* w, const double* wu, const double* wv,
+                    const double* ww, double* pressure, xfp_stats* stats);
+int xfp_project_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material,
+                    float* u, float* v, float* w, const float* wu, const float* wv,
+                    const float* ww, float* pressure, xfp_stats* stats);
+
+/* Adjoint of the projection u_out = u - G A^{-1} D u (no reference
+ * counterpart; xFluid is not differentiable).  Given g = dL/du_out (gu,gv,gw)
+ * writes dL/du_in = g - D^T A^{-1} G^T g into (du,dv,dw): a second MIC(0)-PCG
+ * solve with the same matrix plus the transposed gradient and divergence
+ * kernels.  Outputs may alias inputs. */
+int xfp_project_backward_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material,
+                             const double* wu, const double* wv, const double* ww,
+                             const double* gu, const double* gv, const double* gw,
+                             double* du, double* dv, double* dw, xfp_stats* stats);
+int xfp_project_backward_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material,
+                             const float* wu, const float* wv, const float* ww,
+                             const float* gu, const float* gv, const float* gw,
+                             float* du, float* dv, float* dw, xfp_stats* stats);
+
+/* Diagnostics: runs the internal stages on one scene and returns them on the
+ * dense grid (ni*nj*nk doubles each; any output may be NULL), in the
+ * context's precision.  Exposes, for verification against the reference:
+ *   diag/ax/ay/az/b  _calculate_coefficient (variational_pressuresolver.cpp:231-327);
+ *                    ax[c]=A(c,c-1), ay[c]=A(c,c-ni), az[c]=A(c,c-ni*nj)
+ *   inv/lx/ly/lz     factor_modified_incomplete_cholesky0 (pcg_solver.h:85-186);
+ *                    lx[c]=L(c,c-1) etc.
+ *   z = M^{-1} r     solve_lower + solve_lower_transpose_in_place (pcg_solver.h:192-220)
+ *   q = A r          multiply(FixedSparseMatrix) (sparse_matrix.h:264-276)
+ * r is a dense input (rows without an unknown are ignored). */
+int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material,
+                     const double* u, const double* v, const double* w,
+                     const double* wu, const double* wv, const double* ww,
+                     const double* r, double* diag, double* ax, double* ay, double* az,
+                     double* b, double* inv, double* lx, double* ly, double* lz,
+                     double* z, double* q);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XFP_H */

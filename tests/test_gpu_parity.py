@@ -1,0 +1,257 @@
+"""GPU parity: the CUDA path (through the C ABI) against xFluid's own solver
+(golden vectors) and the FP64 oracle.
+
+Tolerances (floating point, from the project's accuracy targets):
+  * FP64 assembly, MIC(0) factor, preconditioner and SpMV: bit-identical to the
+    reference (same operations in the same order).
+  * FP64 projection: pressure relative L2 <= 1e-5 against the reference, and
+    iteration count within 5% (the dot products are reduced in a different
+    order, so iterates differ at round-off level).
+  * Mixed precision vs the FP64 oracle solved to 1e-12: pressure rel L2 <= 1e-5.
+  * Plain FP32 vs the same: pressure rel L2 <= 2e-3 (FP32 round-off amplified
+    by the condition number; reported, not a target).
+"""
+import numpy as np
+import pytest
+
+from golden_io import CASES, load
+from gpu_util import bits_equal, debug_stages, make_ctx, project, rel_l2, set_tol, solve
+from xfluid_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib_built():
+    from xfluid_b200 import build
+    build.build()
+    from xfluid_b200 import _lib
+    return _lib.load()
+
+
+@pytest.fixture(scope="module")
+def ctx64(lib_built):
+    c = make_ctx("f64")
+    yield c
+    c.close()
+
+
+def _iters_close(a, b):
+    return abs(a - b) <= max(1, int(np.ceil(0.05 * b)))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_stages_f64_bitwise_vs_reference(ctx64, oracle_lib, name):
+    sc, g = load(name)
+    d = debug_stages(ctx64, sc, r=g["r"])
+    for k in ("diag", "ax", "ay", "az", "b"):
+        assert bits_equal(d[k], g[k]), f"assembly {k}"
+    for k in ("inv", "lx", "ly", "lz"):
+        assert bits_equal(d[k], g[k]), f"factor {k}"
+    assert bits_equal(d["z"], g["z"]), "preconditioner"
+    A = oracle_lib.assemble(sc)
+    q = oracle_lib.spmv(sc, A, g["r"])
+    assert bits_equal(d["q"], q), "spmv"
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_project_f64_vs_reference(ctx64, name):
+    sc, g = load(name)
+    set_tol(ctx64, float(g["tol"]), int(g["maxit"]))
+    rc, p, u, v, w, st = project(ctx64, sc)
+    assert rc == 0
+    assert rel_l2(p, g["p"]) <= 1e-5
+    assert _iters_close(st["iterations"], int(g["iters"]))
+    for a, key in ((u, "u_out"), (v, "v_out"), (w, "w_out")):
+        assert rel_l2(a, g[key]) <= 1e-5
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: scenes.dam_break(64, seed=1, noise=0.2),
+    lambda: scenes.blob_scene(dims=(70, 45, 53), seed=9, fractional=False, dtype=np.float64),
+    lambda: scenes.pool_drop(dims=(40, 48, 36), dtype=np.float64),
+    lambda: scenes.blob_scene(dims=(64, 64, 64), seed=12, fractional=True, dtype=np.float64),
+])
+def test_project_f64_vs_oracle(ctx64, oracle_lib, maker):
+    sc = maker()
+    ref = oracle_lib.project(sc, tol=1e-6, maxit=1000)
+    set_tol(ctx64, 1e-6, 1000)
+    rc, p, u, v, w, st = project(ctx64, sc)
+    assert rc == 0 and ref["ok"]
+    assert rel_l2(p, ref["p"]) <= 1e-5
+    assert _iters_close(st["iterations"], ref["iters"])
+    assert rel_l2(u, ref["u"]) <= 1e-5 and rel_l2(v, ref["v"]) <= 1e-5 and rel_l2(w, ref["w"]) <= 1e-5
+
+
+@pytest.mark.parametrize("prec,tol_p", [("mixed", 1e-5), ("f32", 2e-3)])
+def test_reduced_precision_vs_fp64_oracle(lib_built, oracle_lib, prec, tol_p):
+    sc = scenes.blob_scene(dims=(64, 60, 56), seed=21, fractional=True, dtype=np.float32)
+    ref = oracle_lib.project(sc, tol=1e-12, maxit=5000)
+    ctx = make_ctx(prec, tol=1e-6, max_iter=2000)
+    try:
+        rc, p, u, v, w, st = project(ctx, sc, dtype=np.float32)
+    finally:
+        ctx.close()
+    assert rc == 0
+    err = rel_l2(p, ref["p"])
+    assert err <= tol_p, f"{prec}: pressure rel L2 {err:.3e}"
+    if prec == "mixed":
+        assert st["rel_residual"] <= 1e-6
+
+
+@pytest.mark.parametrize("prec", ["f32", "mixed"])
+def test_reduced_precision_stages(lib_built, oracle_lib, prec):
+    sc, g = load("blob24x20x22")
+    ctx = make_ctx(prec)
+    try:
+        d = debug_stages(ctx, sc, r=g["r"])
+    finally:
+        ctx.close()
+    for k in ("diag", "ax", "ay", "az"):
+        assert np.array_equal(d[k], g[k])  # exactly representable in FP32
+    if prec == "mixed":
+        assert bits_equal(d["inv"], g["inv"])  # FP64 pivots
+    else:
+        assert rel_l2(d["inv"], g["inv"]) <= 1e-6
+    assert rel_l2(d["z"], g["z"]) <= 1e-5
+
+
+def test_fractional_stages_vs_oracle(ctx64, oracle_lib):
+    sc = scenes.pool_drop(dims=(30, 34, 28), dtype=np.float64)
+    A = oracle_lib.assemble(sc)
+    F = oracle_lib.factor(sc, A)
+    r = np.random.default_rng(5).standard_normal(A["diag"].shape) * (A["diag"] != 0)
+    d = debug_stages(ctx64, sc, r=r, fractional=True)
+    for k in ("diag", "ax", "ay", "az", "b"):
+        assert bits_equal(d[k], A[k]), k
+    for k in ("inv", "lx", "ly", "lz"):
+        assert bits_equal(d[k], F[k]), k
+    assert bits_equal(d["z"], oracle_lib.precond(sc, F, r))
+
+
+@pytest.mark.parametrize("dims", [(37, 19, 23), (5, 70, 9), (33, 3, 65), (17, 17, 100)])
+def test_ragged_shapes(ctx64, oracle_lib, dims):
+    sc = scenes.blob_scene(dims=dims, seed=31, fractional=False, dtype=np.float64)
+    A = oracle_lib.assemble(sc)
+    F = oracle_lib.factor(sc, A)
+    r = np.random.default_rng(1).standard_normal(A["diag"].shape) * (A["diag"] != 0)
+    d = debug_stages(ctx64, sc, r=r)
+    assert bits_equal(d["inv"], F["inv"])
+    assert bits_equal(d["z"], oracle_lib.precond(sc, F, r))
+
+
+def test_empty_scene(ctx64):
+    sc = scenes.dam_break(dims=(12, 10, 8))
+    sc.mat[:] = scenes.AIR
+    set_tol(ctx64, 1e-6, 100)
+    rc, p, u, v, w, st = project(ctx64, sc)
+    assert rc == 0 and st["iterations"] == 0 and st["rows"] == 0
+    assert np.all(p == 0) and np.array_equal(u, sc.u)
+
+
+def test_zero_rhs(ctx64):
+    sc = scenes.dam_break(dims=(16, 16, 16), noise=0.0, dt=0.0)
+    set_tol(ctx64, 1e-6, 100)
+    rc, p, u, v, w, st = project(ctx64, sc)
+    assert rc == 0 and st["iterations"] == 0 and np.all(p == 0)
+
+
+def test_not_converged_writes_iterate(ctx64, oracle_lib):
+    sc = scenes.dam_break(32, noise=0.5)
+    set_tol(ctx64, 1e-10, 3)
+    rc, p, st = solve(ctx64, sc)
+    assert rc == 1 and st["iterations"] == 3
+    assert np.abs(p).max() > 0
+    set_tol(ctx64, 1e-6, 200)
+
+
+def test_bad_arguments(ctx64):
+    import ctypes as C
+    from xfluid_b200 import _lib
+    st = _lib.XfpStats()
+    rc = ctx64.lib.xfp_solve_f64(ctx64.ptr, 0, 4, 4, None, None, None, None, None, None, None, None, C.byref(st))
+    assert rc == _lib.XFP_ERR_ARGS
+    assert "grid" in ctx64.last_error()
+
+
+def test_backward_matches_oracle_adjoint(ctx64, oracle_lib):
+    sc = scenes.pool_drop(dims=(20, 24, 18), dtype=np.float64)
+    rng = np.random.default_rng(3)
+    gu, gv, gw = (rng.standard_normal(a.shape) for a in (sc.u, sc.v, sc.w))
+    A = oracle_lib.assemble(sc)
+    q = oracle_lib.apply_T(sc, gu, gv, gw)
+    lam = oracle_lib.pcg(sc, dict(A, b=q), 1e-13, 5000)["p"]
+    du, dv, dw = oracle_lib.rhs_T(sc, lam)
+    ref = (gu - du, gv - dv, gw - dw)
+    from xfluid_b200.solver import VariationalPressureSolver
+    s = VariationalPressureSolver("f64", tol=1e-13, max_iter=5000)
+    s.setSize(sc.ni, sc.nj, sc.nk)
+    s.setMaterial(np.ascontiguousarray(sc.mat))
+    s.setFaceWeights(sc.wu, sc.wv, sc.ww)
+    out = s.backward(gu, gv, gw)
+    s.close()
+    for a, b in zip(out, ref):
+        assert rel_l2(a, b) <= 1e-8
+
+
+def test_device_pointers_match_host(lib_built):
+    torch = pytest.importorskip("torch")
+    from xfluid_b200.solver import VariationalPressureSolver
+    sc = scenes.blob_scene(dims=(48, 40, 44), seed=2, dtype=np.float32)
+    s = VariationalPressureSolver("mixed", tol=1e-6, max_iter=500)
+    s.setSize(sc.ni, sc.nj, sc.nk)
+    s.setMaterial(np.ascontiguousarray(sc.mat))
+    uh, vh, wh = sc.u.copy(), sc.v.copy(), sc.w.copy()
+    s.setVelocityField(uh, vh, wh)
+    s.setFaceWeights(sc.wu, sc.wv, sc.ww)
+    ph = np.zeros((sc.nk, sc.nj, sc.ni), np.float32)
+    assert s.project(ph)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    ud, vd, wd = dev(sc.u), dev(sc.v), dev(sc.w)
+    s.setMaterial(dev(sc.mat))
+    s.setVelocityField(ud, vd, wd)
+    s.setFaceWeights(dev(sc.wu), dev(sc.wv), dev(sc.ww))
+    pd = torch.zeros((sc.nk, sc.nj, sc.ni), dtype=torch.float32, device="cuda")
+    assert s.project(pd)
+    torch.cuda.synchronize()
+    assert np.array_equal(pd.cpu().numpy(), ph)
+    assert np.array_equal(ud.cpu().numpy(), uh)
+    s.close()
+
+
+def test_reference_interface_solve_then_apply(lib_built, oracle_lib):
+    """The nine-method surface: setters, solve(p), applyPressure(p)."""
+    from xfluid_b200.solver import VariationalPressureSolver
+    sc, g = load("dam16")
+    s = VariationalPressureSolver("f64")
+    s.set_solver_parameters(float(g["tol"]), int(g["maxit"]))
+    u, v, w = sc.u.copy(), sc.v.copy(), sc.w.copy()
+    s.setSize(sc.ni, sc.nj, sc.nk)
+    s.setVelocityField(u, v, w)
+    s.setMaterial(np.ascontiguousarray(sc.mat))
+    s.setDensity(20.0); s.setDx(1 / 16); s.setDt(0.01); s.setDisField(None)
+    p = np.zeros((sc.nk, sc.nj, sc.ni))
+    assert s.solve(p)
+    assert s.applyPressure(p)
+    assert rel_l2(p, g["p"]) <= 1e-5
+    assert rel_l2(u, g["u_out"]) <= 1e-5
+    s.close()
+
+
+def test_full_size_blob_projection_properties(lib_built, oracle_lib):
+    """256^3 benchmark scene: the projected velocity's weighted divergence is
+    within the solver tolerance and the result is deterministic."""
+    sc = scenes.blob_scene(256, seed=3, dtype=np.float32)
+    ctx = make_ctx("mixed", tol=1e-6, max_iter=1000)
+    try:
+        rc, p, u, v, w, st = project(ctx, sc, dtype=np.float32)
+        rc2, p2, *_ = project(ctx, sc, dtype=np.float32)
+    finally:
+        ctx.close()
+    assert rc == 0 and rc2 == 0
+    assert np.array_equal(p, p2)
+    s64 = sc.astype(np.float64)
+    d = oracle_lib.weighted_divergence(s64, u.astype(np.float64), v.astype(np.float64), w.astype(np.float64))
+    b = oracle_lib.assemble(s64)["b"]
+    # FP32 output velocities: round-off of the stored faces adds ~1e-7 relative
+    assert np.abs(d).max() <= 1e-6 * np.abs(b).max() + 4e-7 * 6

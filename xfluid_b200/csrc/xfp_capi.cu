@@ -1,0 +1,965 @@
+// xfp_capi.cu -- context, device workspace and the C ABI of libxfp (include/xfp.h).
+//
+// One call runs, on the context's stream:
+//   layout   line table + tile list of the material grid          (xfp_layout.cu)
+//   assemble the variational system into the compact layout      (xfp_ops.cu)
+//   factor   MIC(0) in natural order                              (xfp_sweep.cu)
+//   PCG      spmv+dot / x,r update / forward / backward+dot / s update per
+//            iteration, convergence read back every check_every iterations
+//   output   pressure scattered to the dense grid, velocity update (project)
+// Mixed precision wraps the FP32 PCG in FP64 iterative refinement.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/xfp.h"
+#include "xfp_common.cuh"
+#include "xfp_kernels.h"
+
+using namespace xfp;
+
+namespace {
+
+constexpr int NBLK_MAX = 148 * 8;   // blocks of the reduction kernels (partials slots)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct Timer {
+  cudaEvent_t ev[6] = {};
+};
+
+}  // namespace
+
+struct xfp_ctx {
+  xfp_options opt;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  int nsm = 148;
+  // I/O staging (host-pointer mode)
+  DevBuf io_mat, io_u, io_v, io_w, io_wu, io_wv, io_ww, io_p, io_gu, io_gv, io_gw;
+  // layout
+  DevBuf lines, lens, tile_active, tiles, counters;
+  // compact arrays
+  DevBuf A64[5];                  // diag, ax, ay, az, b (FP64)
+  DevBuf A32[5];                  // same in FP32
+  DevBuf F64[6], F32[6];          // factor scratch: L and missing per direction
+  DevBuf inv64, inv32, L32[3];
+  DevBuf x64, r64, x32, r32, s32, z32, s64, z64, dense;
+  // control
+  DevBuf prog, ctl, scal, scal2, partials, tpartials;
+  size_t prog_cap = 0;
+  // sizes of the current layout
+  int ni = 0, nj = 0, nk = 0, NJt = 0, NKt = 0, nw = 16;
+  long long M = 0, rows = 0, nlines_act = 0, ntiles = 0;
+  PcgScalars host_sc{};
+  // stats
+  double ms_setup = 0, ms_factor = 0, ms_solve = 0, ms_apply = 0;
+  int iters = 0, refinements = 0;
+  double res = 0, bnorm = 0;
+  cudaEvent_t ev[8] = {};
+};
+
+namespace {
+
+int fail(xfp_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+#define XFP_CUDA(ctx, call)                                                                    \
+  do {                                                                                         \
+    cudaError_t _e = (call);                                                                   \
+    if (_e != cudaSuccess) {                                                                   \
+      return fail(ctx, _e == cudaErrorMemoryAllocation ? XFP_ERR_NOMEM : XFP_ERR_CUDA,         \
+                  std::string(#call) + ": " + cudaGetErrorString(_e));                         \
+    }                                                                                          \
+  } while (0)
+
+size_t ncells(int ni, int nj, int nk) { return (size_t)ni * nj * nk; }
+size_t nu(int ni, int nj, int nk) { return (size_t)(ni + 1) * nj * nk; }
+size_t nv(int ni, int nj, int nk) { return (size_t)ni * (nj + 1) * nk; }
+size_t nw_(int ni, int nj, int nk) { return (size_t)ni * nj * (nk + 1); }
+
+long long spin_limit(const xfp_ctx* ctx) {
+  double ms = ctx->opt.timeout_ms > 0 ? ctx->opt.timeout_ms : 2000.0;
+  return (long long)std::max(1e4, ms * 4000.0);  // ~250 ns per backed-off poll
+}
+
+// Stage an input array on the device (or use it in place).
+template <typename T>
+int stage_in(xfp_ctx* ctx, DevBuf& buf, const T* src, size_t n, const T** dev) {
+  if (src == nullptr) { *dev = nullptr; return XFP_OK; }
+  if (ctx->opt.device_pointers) { *dev = src; return XFP_OK; }
+  XFP_CUDA(ctx, buf.ensure(n * sizeof(T)));
+  XFP_CUDA(ctx, cudaMemcpyAsync(buf.p, src, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  *dev = buf.as<T>();
+  return XFP_OK;
+}
+
+int check_dims(xfp_ctx* ctx, int ni, int nj, int nk, const void* mat) {
+  if (!ctx) return XFP_ERR_ARGS;
+  if (ni < 1 || nj < 1 || nk < 1) return fail(ctx, XFP_ERR_ARGS, "grid sizes must be >= 1");
+  if ((long long)ni + nj + nk >= (1LL << 30) || (long long)ni * nj * nk >= (1LL << 31))
+    return fail(ctx, XFP_ERR_ARGS, "grid too large");
+  if (nj > 65535 * 32) return fail(ctx, XFP_ERR_ARGS, "nj too large");
+  if (!mat) return fail(ctx, XFP_ERR_ARGS, "material is NULL");
+  return XFP_OK;
+}
+
+// ---------------------------------------------------------------- layout
+int build_layout(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk) {
+  const int nw = ctx->nw;
+  const long long nlines = (long long)nj * nk;
+  const int NJt = (nj + 31) / 32, NKt = (nk + nw - 1) / nw;
+  XFP_CUDA(ctx, ctx->lines.ensure(nlines * sizeof(Line)));
+  XFP_CUDA(ctx, ctx->lens.ensure((nlines + 1) * sizeof(int)));
+  XFP_CUDA(ctx, ctx->tile_active.ensure((size_t)NJt * NKt));
+  XFP_CUDA(ctx, ctx->tiles.ensure((size_t)NJt * NKt * sizeof(int)));
+  XFP_CUDA(ctx, ctx->counters.ensure(4 * sizeof(long long)));
+  size_t prog_bytes = (size_t)nk * NJt * sizeof(unsigned long long);
+  if (prog_bytes > ctx->prog_cap) {
+    XFP_CUDA(ctx, ctx->prog.ensure(prog_bytes));
+    XFP_CUDA(ctx, cudaMemsetAsync(ctx->prog.p, 0, ctx->prog.cap, ctx->stream));
+    ctx->prog_cap = ctx->prog.cap;
+  }
+  LayoutDev L{ctx->lines.as<Line>(), ctx->lens.as<int>(), ctx->tile_active.as<unsigned char>(),
+              ctx->tiles.as<int>(), ctx->counters.as<long long>()};
+  XFP_CUDA(ctx, layout_build(dmat, ni, nj, nk, nw, L, ctx->stream));
+  long long cnt[4];
+  XFP_CUDA(ctx, cudaMemcpyAsync(cnt, ctx->counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->ni = ni; ctx->nj = nj; ctx->nk = nk;
+  ctx->NJt = NJt; ctx->NKt = NKt;
+  ctx->M = cnt[0]; ctx->rows = cnt[1]; ctx->nlines_act = cnt[2]; ctx->ntiles = cnt[3];
+  return XFP_OK;
+}
+
+int ensure_compact(xfp_ctx* ctx, int prec) {
+  const size_t M = (size_t)std::max<long long>(ctx->M, 4) + 8;
+  if (prec == XFP_PREC_F64 || prec == XFP_PREC_MIXED) {
+    for (auto& b : ctx->A64) XFP_CUDA(ctx, b.ensure(M * 8));
+    for (auto& b : ctx->F64) XFP_CUDA(ctx, b.ensure(M * 8));
+    XFP_CUDA(ctx, ctx->inv64.ensure(M * 8));
+    XFP_CUDA(ctx, ctx->x64.ensure(M * 8));
+    XFP_CUDA(ctx, ctx->r64.ensure(M * 8));
+  }
+  if (prec == XFP_PREC_F64) {
+    XFP_CUDA(ctx, ctx->s64.ensure(M * 8));
+    XFP_CUDA(ctx, ctx->z64.ensure(M * 8));
+  }
+  if (prec == XFP_PREC_F32 || prec == XFP_PREC_MIXED) {
+    for (auto& b : ctx->A32) XFP_CUDA(ctx, b.ensure(M * 4));
+    XFP_CUDA(ctx, ctx->x32.ensure(M * 4));
+    XFP_CUDA(ctx, ctx->r32.ensure(M * 4));
+    XFP_CUDA(ctx, ctx->s32.ensure(M * 4));
+    XFP_CUDA(ctx, ctx->z32.ensure(M * 4));
+    for (auto& b : ctx->L32) XFP_CUDA(ctx, b.ensure(M * 4));
+  }
+  if (prec == XFP_PREC_F32) {
+    for (auto& b : ctx->F32) XFP_CUDA(ctx, b.ensure(M * 4));
+    XFP_CUDA(ctx, ctx->inv32.ensure(M * 4));
+  }
+  XFP_CUDA(ctx, ctx->ctl.ensure(sizeof(SweepCtl)));
+  XFP_CUDA(ctx, ctx->scal.ensure(sizeof(PcgScalars)));
+  XFP_CUDA(ctx, ctx->scal2.ensure(sizeof(PcgScalars)));
+  XFP_CUDA(ctx, ctx->partials.ensure(NBLK_MAX * sizeof(double)));
+  XFP_CUDA(ctx, ctx->tpartials.ensure(std::max<long long>(ctx->ntiles, 1) * sizeof(double)));
+  return XFP_OK;
+}
+
+SweepGrid make_grid(xfp_ctx* ctx, PcgScalars* sc, int bwd_mode) {
+  SweepGrid g;
+  g.ni = ctx->ni; g.nj = ctx->nj; g.nk = ctx->nk;
+  g.NJt = ctx->NJt; g.NKt = ctx->NKt;
+  g.ntiles = (int)ctx->ntiles;
+  g.maxT = ctx->ni + ctx->nj + ctx->nk;
+  g.bwd_mode = bwd_mode;
+  g.lines = ctx->lines.as<Line>();
+  g.tiles = ctx->tiles.as<int>();
+  g.tile_active = ctx->tile_active.as<unsigned char>();
+  g.prog = ctx->prog.as<unsigned long long>();
+  g.ctl = ctx->ctl.as<SweepCtl>();
+  g.spin_limit = spin_limit(ctx);
+  g.scal = sc;
+  return g;
+}
+
+template <typename VT, typename IT, typename CT>
+int run_sweep(xfp_ctx* ctx, int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d) {
+  if (g.ntiles <= 0) return XFP_OK;
+  int maxg = sweep_max_grid(op, d, ctx->nw);
+  if (maxg <= 0) return fail(ctx, XFP_ERR_CUDA, "sweep kernel cannot be resident");
+  int grid = std::min(maxg, g.ntiles);
+  XFP_CUDA(ctx, sweep_launch(op, g, d, ctx->nw, grid, ctx->stream));
+  return XFP_OK;
+}
+
+int check_sweep_error(xfp_ctx* ctx) {
+  SweepCtl c;
+  XFP_CUDA(ctx, cudaMemcpyAsync(&c, ctx->ctl.p, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (c.err) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "device wait timed out (site %u)", c.err_where);
+    // clear so the context stays usable
+    SweepCtl z{c.gen, 0, 0, 0};
+    cudaMemcpyAsync(ctx->ctl.p, &z, sizeof(z), cudaMemcpyHostToDevice, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return fail(ctx, XFP_ERR_TIMEOUT, buf);
+  }
+  return XFP_OK;
+}
+
+// ---------------------------------------------------------------- factor
+// Zero the factor scratch, then the lower sweep.
+template <typename VT, typename IT, typename CT>
+int factor(xfp_ctx* ctx, const CT* const A[4], CT* const F[6], IT* inv, CT omega, CT ratio) {
+  const size_t M = (size_t)ctx->M;
+  for (int q = 0; q < 6; ++q) XFP_CUDA(ctx, cudaMemsetAsync(F[q], 0, M * sizeof(CT), ctx->stream));
+  XFP_CUDA(ctx, cudaMemsetAsync(inv, 0, M * sizeof(IT), ctx->stream));
+  SweepData<VT, IT, CT> d;
+  d.diag = A[0]; d.ax = A[1]; d.ay = A[2]; d.az = A[3];
+  d.flx = F[0]; d.fly = F[1]; d.flz = F[2]; d.fmx = F[3]; d.fmy = F[4]; d.fmz = F[5];
+  d.oinv = inv;
+  d.omega = omega; d.ratio = ratio;
+  SweepGrid g = make_grid(ctx, nullptr, 0);
+  return run_sweep<VT, IT, CT>(ctx, SWEEP_FACTOR, g, d);
+}
+
+// ---------------------------------------------------------------- PCG
+// pcg_solver.h:243-285 on the compact system.  A: coefficient arrays (VT),
+// b: rhs (VT), x: solution (VT), L/inv: factor.  DT: dot accumulation type.
+template <typename VT, typename IT, typename DT>
+int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT* z,
+        const VT* const L[3], const IT* inv, double tol, int maxit, PcgScalars* dsc,
+        PcgScalars* hsc) {
+  const long long M = ctx->M;
+  cudaStream_t st = ctx->stream;
+  if (tol < 1e-30) tol = 1e-30;  // set_solver_parameters, pcg_solver.h:237
+  XFP_CUDA(ctx, cudaMemsetAsync(x, 0, M * sizeof(VT), st));
+  XFP_CUDA(ctx, cudaMemsetAsync(dsc, 0, sizeof(PcgScalars), st));
+  XFP_CUDA(ctx, copy_vec<VT>(b, r, M, st));
+  XFP_CUDA(ctx, absmax_init<VT>(r, M, dsc, ctx->partials.as<double>(), NBLK_MAX, tol, maxit, st));
+  SweepData<VT, IT, DT> d;
+  d.r = r; d.y = z; d.lx = L[0]; d.ly = L[1]; d.lz = L[2]; d.inv = inv;
+  d.partials = ctx->tpartials.as<double>();
+  SweepGrid g0 = make_grid(ctx, dsc, 0), g1 = make_grid(ctx, dsc, 1);
+  int rc;
+  if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g0, d)) != XFP_OK) return rc;
+  if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_BWD, g0, d)) != XFP_OK) return rc;
+  XFP_CUDA(ctx, copy_vec<VT>(z, s, M, st));
+  const int K = ctx->opt.check_every > 0 ? ctx->opt.check_every : 8;
+  DT* part = reinterpret_cast<DT*>(ctx->partials.p);
+  for (int done_iters = 0;;) {
+    for (int q = 0; q < K; ++q) {
+      XFP_CUDA(ctx, (spmv_dot<VT, VT, DT>(A[0], A[1], A[2], A[3], s, z, ctx->lines.as<Line>(), ctx->ni,
+                                          ctx->nj, ctx->nk, M, dsc, part, NBLK_MAX, 0, st)));
+      XFP_CUDA(ctx, (update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), NBLK_MAX, st)));
+      if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g1, d)) != XFP_OK) return rc;
+      if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_BWD, g1, d)) != XFP_OK) return rc;
+      XFP_CUDA(ctx, update_s<VT>(s, z, M, dsc, st));
+    }
+    done_iters += K;
+    XFP_CUDA(ctx, cudaMemcpyAsync(hsc, dsc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+    XFP_CUDA(ctx, cudaStreamSynchronize(st));
+    if ((rc = check_sweep_error(ctx)) != XFP_OK) return rc;
+    if (hsc->done) break;
+    if (done_iters > maxit + 2 * K) return fail(ctx, XFP_ERR_CUDA, "PCG loop did not terminate");
+  }
+  if (hsc->status == XFP_ERR_BREAKDOWN) return fail(ctx, XFP_ERR_BREAKDOWN, "PCG breakdown: rho is zero or NaN");
+  return hsc->status == 0 ? XFP_OK : XFP_NOT_CONVERGED;
+}
+
+void ev_record(xfp_ctx* ctx, int i) { cudaEventRecord(ctx->ev[i], ctx->stream); }
+float ev_ms(xfp_ctx* ctx, int a, int b) {
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev[a], ctx->ev[b]);
+  return ms;
+}
+
+// ---------------------------------------------------------------- solve driver
+// Assembles, factors and solves.  On return the solution is in x64 (F64,
+// MIXED) or x32 (F32) in compact layout.  rhs_from_adjoint: when non-null, the
+// assembled b is replaced by G^T g (backward pass) before solving.
+template <typename IOT>
+int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const IOT* du_,
+               const IOT* dv, const IOT* dw, const IOT* dwu, const IOT* dwv, const IOT* dww,
+               const IOT* adj_gu = nullptr, const IOT* adj_gv = nullptr, const IOT* adj_gw = nullptr) {
+  const int prec = ctx->opt.precision;
+  cudaStream_t st = ctx->stream;
+  int rc;
+  ev_record(ctx, 0);
+  if ((rc = build_layout(ctx, dmat, ni, nj, nk)) != XFP_OK) return rc;
+  if ((rc = ensure_compact(ctx, prec)) != XFP_OK) return rc;
+  const Line* lines = ctx->lines.as<Line>();
+  const long long M = ctx->M;
+  ctx->iters = 0; ctx->refinements = 0; ctx->res = 0; ctx->bnorm = 0;
+  PcgScalars* dsc = ctx->scal.as<PcgScalars>();
+  PcgScalars& hsc = ctx->host_sc;
+  const double tol = ctx->opt.tol, omega = ctx->opt.omega, ratio = ctx->opt.min_diag_ratio;
+  const int maxit = ctx->opt.max_iter;
+
+  if (prec == XFP_PREC_F64) {
+    double* A[5];
+    for (int q = 0; q < 5; ++q) A[q] = ctx->A64[q].as<double>();
+    XFP_CUDA(ctx, (assemble<IOT, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
+                                         A[3], A[4], st)));
+    if (adj_gu) XFP_CUDA(ctx, (apply_pressure_T<IOT, double>(dmat, dwu, dwv, dww, adj_gu, adj_gv, adj_gw, ni, nj,
+                                                             nk, lines, A[4], st)));
+    ev_record(ctx, 1);
+    double* F[6];
+    for (int q = 0; q < 6; ++q) F[q] = ctx->F64[q].as<double>();
+    const double* Ac[4] = {A[0], A[1], A[2], A[3]};
+    if ((rc = factor<double, double, double>(ctx, Ac, F, ctx->inv64.as<double>(), omega, ratio)) != XFP_OK) return rc;
+    ev_record(ctx, 2);
+    const double* Lc[3] = {F[0], F[1], F[2]};
+    rc = pcg<double, double, double>(ctx, Ac, A[4], ctx->x64.as<double>(), ctx->r64.as<double>(),
+                                     ctx->s64.as<double>(), ctx->z64.as<double>(), Lc, ctx->inv64.as<double>(),
+                                     tol, maxit, dsc, &hsc);
+    ev_record(ctx, 3);
+    ctx->iters = hsc.iters; ctx->res = hsc.res; ctx->bnorm = hsc.bnorm;
+  } else if (prec == XFP_PREC_F32) {
+    float* A[5];
+    for (int q = 0; q < 5; ++q) A[q] = ctx->A32[q].as<float>();
+    XFP_CUDA(ctx, (assemble<IOT, float>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
+                                        A[3], A[4], st)));
+    if (adj_gu) XFP_CUDA(ctx, (apply_pressure_T<IOT, float>(dmat, dwu, dwv, dww, adj_gu, adj_gv, adj_gw, ni, nj,
+                                                            nk, lines, A[4], st)));
+    ev_record(ctx, 1);
+    float* F[6];
+    for (int q = 0; q < 6; ++q) F[q] = ctx->F32[q].as<float>();
+    const float* Ac[4] = {A[0], A[1], A[2], A[3]};
+    if ((rc = factor<float, float, float>(ctx, Ac, F, ctx->inv32.as<float>(), (float)omega, (float)ratio)) != XFP_OK)
+      return rc;
+    ev_record(ctx, 2);
+    const float* Lc[3] = {F[0], F[1], F[2]};
+    rc = pcg<float, float, float>(ctx, Ac, A[4], ctx->x32.as<float>(), ctx->r32.as<float>(), ctx->s32.as<float>(),
+                                  ctx->z32.as<float>(), Lc, ctx->inv32.as<float>(), tol, maxit, dsc, &hsc);
+    ev_record(ctx, 3);
+    ctx->iters = hsc.iters; ctx->res = hsc.res; ctx->bnorm = hsc.bnorm;
+  } else {
+    // ---- mixed: FP64 system and refinement, FP32 inner PCG ----
+    double* A[5];
+    for (int q = 0; q < 5; ++q) A[q] = ctx->A64[q].as<double>();
+    XFP_CUDA(ctx, (assemble<IOT, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
+                                         A[3], A[4], st)));
+    if (adj_gu) XFP_CUDA(ctx, (apply_pressure_T<IOT, double>(dmat, dwu, dwv, dww, adj_gu, adj_gv, adj_gw, ni, nj,
+                                                             nk, lines, A[4], st)));
+    float* A32[4];
+    for (int q = 0; q < 4; ++q) {
+      A32[q] = ctx->A32[q].as<float>();
+      XFP_CUDA(ctx, (convert<double, float>(A[q], A32[q], M, st)));
+    }
+    ev_record(ctx, 1);
+    double* F[6];
+    for (int q = 0; q < 6; ++q) F[q] = ctx->F64[q].as<double>();
+    const double* Ac[4] = {A[0], A[1], A[2], A[3]};
+    if ((rc = factor<float, double, double>(ctx, Ac, F, ctx->inv64.as<double>(), omega, ratio)) != XFP_OK) return rc;
+    for (int q = 0; q < 3; ++q) XFP_CUDA(ctx, (convert<double, float>(F[q], ctx->L32[q].as<float>(), M, st)));
+    ev_record(ctx, 2);
+    const float* Lc[3] = {ctx->L32[0].as<float>(), ctx->L32[1].as<float>(), ctx->L32[2].as<float>()};
+    const float* A32c[4] = {A32[0], A32[1], A32[2], A32[3]};
+    double* x64 = ctx->x64.as<double>();
+    double* r64 = ctx->r64.as<double>();
+    PcgScalars* osc = ctx->scal2.as<PcgScalars>();
+    PcgScalars ho{};
+    XFP_CUDA(ctx, cudaMemsetAsync(x64, 0, M * sizeof(double), st));
+    XFP_CUDA(ctx, cudaMemsetAsync(osc, 0, sizeof(PcgScalars), st));
+    XFP_CUDA(ctx, absmax_init<double>(A[4], M, osc, ctx->partials.as<double>(), NBLK_MAX, tol, 1, st));
+    XFP_CUDA(ctx, cudaMemcpyAsync(&ho, osc, sizeof(ho), cudaMemcpyDeviceToHost, st));
+    XFP_CUDA(ctx, cudaStreamSynchronize(st));
+    const double bnorm = ho.bnorm, target = (tol < 1e-30 ? 1e-30 : tol) * bnorm;
+    ctx->bnorm = bnorm;
+    double res = bnorm;
+    int total = 0, cycles = 0, status = XFP_OK;
+    const int max_ref = ctx->opt.max_refine > 0 ? ctx->opt.max_refine : 20;
+    const double floor_tol = ctx->opt.inner_tol > 0 ? ctx->opt.inner_tol : 1e-6;
+    if (bnorm > 0) {
+      status = XFP_NOT_CONVERGED;
+      for (cycles = 0; cycles < max_ref && total < maxit; ++cycles) {
+        if (cycles > 0) {
+          XFP_CUDA(ctx, residual64(A[0], A[1], A[2], A[3], A[4], x64, r64, lines, ni, nj, nk, M, osc,
+                                   ctx->partials.as<double>(), NBLK_MAX, st));
+          XFP_CUDA(ctx, cudaMemcpyAsync(&ho, osc, sizeof(ho), cudaMemcpyDeviceToHost, st));
+          XFP_CUDA(ctx, cudaStreamSynchronize(st));
+          res = ho.res;
+          if (res <= target) { status = XFP_OK; break; }
+          XFP_CUDA(ctx, (convert<double, float>(r64, ctx->r32.as<float>(), M, st)));
+        } else {
+          XFP_CUDA(ctx, (convert<double, float>(A[4], ctx->r32.as<float>(), M, st)));
+        }
+        const double inner = std::min(0.5, std::max(floor_tol, 0.5 * target / res));
+        // inner rhs lives in s32 scratch's partner: use r32 as b, z32/s32/x32 work
+        float* b32 = ctx->A32[4].as<float>();
+        XFP_CUDA(ctx, copy_vec<float>(ctx->r32.as<float>(), b32, M, st));
+        int irc = pcg<float, double, double>(ctx, A32c, b32, ctx->x32.as<float>(), ctx->r32.as<float>(),
+                                             ctx->s32.as<float>(), ctx->z32.as<float>(), Lc,
+                                             ctx->inv64.as<double>(), inner, maxit - total, dsc, &hsc);
+        if (irc < 0) return irc;
+        total += hsc.iters;
+        XFP_CUDA(ctx, refine_update(x64, ctx->x32.as<float>(), M, st));
+      }
+      if (status != XFP_OK) {
+        XFP_CUDA(ctx, residual64(A[0], A[1], A[2], A[3], A[4], x64, r64, lines, ni, nj, nk, M, osc,
+                                 ctx->partials.as<double>(), NBLK_MAX, st));
+        XFP_CUDA(ctx, cudaMemcpyAsync(&ho, osc, sizeof(ho), cudaMemcpyDeviceToHost, st));
+        XFP_CUDA(ctx, cudaStreamSynchronize(st));
+        res = ho.res;
+        if (res <= target) status = XFP_OK;
+      }
+    }
+    ev_record(ctx, 3);
+    ctx->iters = total; ctx->refinements = cycles; ctx->res = res;
+    rc = status;
+  }
+  return rc;
+}
+
+template <typename IOT>
+int solution_dense(xfp_ctx* ctx, IOT* dense) {
+  const int prec = ctx->opt.precision;
+  const Line* lines = ctx->lines.as<Line>();
+  if (prec == XFP_PREC_F32) {
+    if (std::is_same<IOT, float>::value) {
+      XFP_CUDA(ctx, scatter_dense<float>(ctx->x32.as<float>(), lines, ctx->ni, ctx->nj, ctx->nk, (float*)dense,
+                                         ctx->stream));
+    } else {
+      XFP_CUDA(ctx, ctx->r64.ensure(ctx->M * 8 + 64));
+      XFP_CUDA(ctx, (convert<float, double>(ctx->x32.as<float>(), ctx->r64.as<double>(), ctx->M, ctx->stream)));
+      XFP_CUDA(ctx, scatter_dense<double>(ctx->r64.as<double>(), lines, ctx->ni, ctx->nj, ctx->nk, (double*)dense,
+                                          ctx->stream));
+    }
+  } else {
+    if (std::is_same<IOT, double>::value) {
+      XFP_CUDA(ctx, scatter_dense<double>(ctx->x64.as<double>(), lines, ctx->ni, ctx->nj, ctx->nk, (double*)dense,
+                                          ctx->stream));
+    } else {
+      XFP_CUDA(ctx, (convert<double, float>(ctx->x64.as<double>(), ctx->x32.as<float>(), ctx->M, ctx->stream)));
+      XFP_CUDA(ctx, scatter_dense<float>(ctx->x32.as<float>(), lines, ctx->ni, ctx->nj, ctx->nk, (float*)dense,
+                                         ctx->stream));
+    }
+  }
+  return XFP_OK;
+}
+
+double bytes_per_row_iter(int prec) { return prec == XFP_PREC_F64 ? 224.0 : prec == XFP_PREC_F32 ? 112.0 : 120.0; }
+
+void fill_stats(xfp_ctx* ctx, xfp_stats* s, int status, double ms_total) {
+  if (!s) return;
+  memset(s, 0, sizeof(*s));
+  s->status = status;
+  s->iterations = ctx->iters;
+  s->refinements = ctx->refinements;
+  s->residual = ctx->res;
+  s->b_inf = ctx->bnorm;
+  s->rel_residual = ctx->bnorm > 0 ? ctx->res / ctx->bnorm : 0.0;
+  s->rows = ctx->rows;
+  s->stored = ctx->M;
+  s->lines = ctx->nlines_act;
+  s->ms_setup = ctx->ms_setup;
+  s->ms_factor = ctx->ms_factor;
+  s->ms_solve = ctx->ms_solve;
+  s->ms_apply = ctx->ms_apply;
+  s->ms_total = ms_total;
+  const double cells = (double)ctx->ni * ctx->nj * ctx->nk;
+  s->bytes = bytes_per_row_iter(ctx->opt.precision) * (double)ctx->rows * ctx->iters + 33.0 * cells +
+             24.0 * (double)ctx->rows + 29.0 * cells;
+}
+
+template <typename IOT>
+int project_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* u, IOT* v, IOT* w,
+                 const IOT* wu, const IOT* wv, const IOT* ww, IOT* pressure, xfp_stats* stats,
+                 bool do_apply) {
+  int rc = check_dims(ctx, ni, nj, nk, mat);
+  if (rc) return rc;
+  if (!u || !v || !w) return fail(ctx, XFP_ERR_ARGS, "velocity arrays must not be NULL");
+  if ((wu == nullptr) != (wv == nullptr) || (wu == nullptr) != (ww == nullptr))
+    return fail(ctx, XFP_ERR_ARGS, "face weights: pass all three or none");
+  if (!do_apply && !pressure) return fail(ctx, XFP_ERR_ARGS, "pressure output is NULL");
+  XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, ctx->stream);
+  const uint8_t* dmat;
+  const IOT *du_, *dv, *dw, *dwu, *dwv, *dww;
+  if ((rc = stage_in(ctx, ctx->io_mat, mat, ncells(ni, nj, nk), &dmat))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_u, u, nu(ni, nj, nk), &du_))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_v, v, nv(ni, nj, nk), &dv))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_w, w, nw_(ni, nj, nk), &dw))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_wu, wu, nu(ni, nj, nk), &dwu))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_wv, wv, nv(ni, nj, nk), &dwv))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_ww, ww, nw_(ni, nj, nk), &dww))) return rc;
+  int status = solve_core<IOT>(ctx, ni, nj, nk, dmat, du_, dv, dw, dwu, dwv, dww);
+  if (status < 0) {
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return status;
+  }
+  IOT* dp;
+  if (ctx->opt.device_pointers && pressure) {
+    dp = pressure;
+  } else {
+    XFP_CUDA(ctx, ctx->io_p.ensure(ncells(ni, nj, nk) * sizeof(IOT)));
+    dp = ctx->io_p.as<IOT>();
+  }
+  if ((rc = solution_dense<IOT>(ctx, dp))) return rc;
+  if (do_apply) {
+    IOT* mu = const_cast<IOT*>(du_);
+    IOT* mv = const_cast<IOT*>(dv);
+    IOT* mw = const_cast<IOT*>(dw);
+    XFP_CUDA(ctx, (apply_pressure<IOT, IOT>(dmat, dwu, dwv, dww, dp, ni, nj, nk, mu, mv, mw, ctx->stream)));
+  }
+  ev_record(ctx, 4);
+  if (!ctx->opt.device_pointers) {
+    if (pressure)
+      XFP_CUDA(ctx, cudaMemcpyAsync(pressure, dp, ncells(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+    if (do_apply) {
+      XFP_CUDA(ctx, cudaMemcpyAsync(u, du_, nu(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+      XFP_CUDA(ctx, cudaMemcpyAsync(v, dv, nv(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+      XFP_CUDA(ctx, cudaMemcpyAsync(w, dw, nw_(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+  }
+  cudaEventRecord(t1, ctx->stream);
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->ms_setup = ev_ms(ctx, 0, 1);
+  ctx->ms_factor = ev_ms(ctx, 1, 2);
+  ctx->ms_solve = ev_ms(ctx, 2, 3);
+  ctx->ms_apply = ev_ms(ctx, 3, 4);
+  float tot = 0;
+  cudaEventElapsedTime(&tot, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  fill_stats(ctx, stats, status, tot);
+  XFP_CUDA(ctx, cudaGetLastError());
+  return status;
+}
+
+template <typename IOT>
+int apply_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, const IOT* wu, const IOT* wv,
+               const IOT* ww, const IOT* pressure, IOT* u, IOT* v, IOT* w) {
+  int rc = check_dims(ctx, ni, nj, nk, mat);
+  if (rc) return rc;
+  if (!u || !v || !w || !pressure) return fail(ctx, XFP_ERR_ARGS, "NULL array");
+  XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  const uint8_t* dmat;
+  const IOT *du_, *dv, *dw, *dwu, *dwv, *dww, *dp;
+  if ((rc = stage_in(ctx, ctx->io_mat, mat, ncells(ni, nj, nk), &dmat))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_u, u, nu(ni, nj, nk), &du_))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_v, v, nv(ni, nj, nk), &dv))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_w, w, nw_(ni, nj, nk), &dw))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_wu, wu, nu(ni, nj, nk), &dwu))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_wv, wv, nv(ni, nj, nk), &dwv))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_ww, ww, nw_(ni, nj, nk), &dww))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_p, pressure, ncells(ni, nj, nk), &dp))) return rc;
+  XFP_CUDA(ctx, (apply_pressure<IOT, IOT>(dmat, dwu, dwv, dww, dp, ni, nj, nk, const_cast<IOT*>(du_),
+                                          const_cast<IOT*>(dv), const_cast<IOT*>(dw), ctx->stream)));
+  if (!ctx->opt.device_pointers) {
+    XFP_CUDA(ctx, cudaMemcpyAsync(u, du_, nu(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+    XFP_CUDA(ctx, cudaMemcpyAsync(v, dv, nv(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+    XFP_CUDA(ctx, cudaMemcpyAsync(w, dw, nw_(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XFP_OK;
+}
+
+template <typename IOT>
+int backward_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, const IOT* wu, const IOT* wv,
+                  const IOT* ww, const IOT* gu, const IOT* gv, const IOT* gw, IOT* du, IOT* dv, IOT* dw,
+                  xfp_stats* stats) {
+  int rc = check_dims(ctx, ni, nj, nk, mat);
+  if (rc) return rc;
+  if (!gu || !gv || !gw || !du || !dv || !dw) return fail(ctx, XFP_ERR_ARGS, "NULL gradient array");
+  if ((wu == nullptr) != (wv == nullptr) || (wu == nullptr) != (ww == nullptr))
+    return fail(ctx, XFP_ERR_ARGS, "face weights: pass all three or none");
+  XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, ctx->stream);
+  const uint8_t* dmat;
+  const IOT *dgu, *dgv, *dgw, *dwu, *dwv, *dww;
+  if ((rc = stage_in(ctx, ctx->io_mat, mat, ncells(ni, nj, nk), &dmat))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_gu, gu, nu(ni, nj, nk), &dgu))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_gv, gv, nv(ni, nj, nk), &dgv))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_gw, gw, nw_(ni, nj, nk), &dgw))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_wu, wu, nu(ni, nj, nk), &dwu))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_wv, wv, nv(ni, nj, nk), &dwv))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_ww, ww, nw_(ni, nj, nk), &dww))) return rc;
+  // the assembly needs velocities only for b, which the adjoint replaces: use g
+  int status = solve_core<IOT>(ctx, ni, nj, nk, dmat, dgu, dgv, dgw, dwu, dwv, dww, dgu, dgv, dgw);
+  if (status < 0) return status;
+  // lambda to the dense grid, then d = g - D^T lambda
+  IOT *ou, *ov, *ow;
+  if (ctx->opt.device_pointers) {
+    ou = du; ov = dv; ow = dw;
+  } else {
+    XFP_CUDA(ctx, ctx->io_u.ensure(nu(ni, nj, nk) * sizeof(IOT)));
+    XFP_CUDA(ctx, ctx->io_v.ensure(nv(ni, nj, nk) * sizeof(IOT)));
+    XFP_CUDA(ctx, ctx->io_w.ensure(nw_(ni, nj, nk) * sizeof(IOT)));
+    ou = ctx->io_u.as<IOT>(); ov = ctx->io_v.as<IOT>(); ow = ctx->io_w.as<IOT>();
+  }
+  const int prec = ctx->opt.precision;
+  if (prec == XFP_PREC_F32) {
+    XFP_CUDA(ctx, ctx->dense.ensure(ncells(ni, nj, nk) * sizeof(float)));
+    XFP_CUDA(ctx, scatter_dense<float>(ctx->x32.as<float>(), ctx->lines.as<Line>(), ni, nj, nk,
+                                       ctx->dense.as<float>(), ctx->stream));
+    if (std::is_same<IOT, float>::value) {
+      XFP_CUDA(ctx, (rhs_T<float, float>(dmat, (const float*)dwu, (const float*)dwv, (const float*)dww,
+                                         ctx->dense.as<float>(), ctx->lines.as<Line>(), ni, nj, nk,
+                                         (const float*)dgu, (const float*)dgv, (const float*)dgw, (float*)ou,
+                                         (float*)ov, (float*)ow, ctx->stream)));
+    } else {
+      return fail(ctx, XFP_ERR_UNSUPPORTED, "FP32 precision with FP64 I/O is not supported for backward");
+    }
+  } else {
+    XFP_CUDA(ctx, ctx->dense.ensure(ncells(ni, nj, nk) * sizeof(double)));
+    XFP_CUDA(ctx, scatter_dense<double>(ctx->x64.as<double>(), ctx->lines.as<Line>(), ni, nj, nk,
+                                        ctx->dense.as<double>(), ctx->stream));
+    XFP_CUDA(ctx, (rhs_T<IOT, double>(dmat, dwu, dwv, dww, ctx->dense.as<double>(), ctx->lines.as<Line>(), ni, nj,
+                                      nk, dgu, dgv, dgw, ou, ov, ow, ctx->stream)));
+  }
+  ev_record(ctx, 4);
+  if (!ctx->opt.device_pointers) {
+    XFP_CUDA(ctx, cudaMemcpyAsync(du, ou, nu(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+    XFP_CUDA(ctx, cudaMemcpyAsync(dv, ov, nv(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+    XFP_CUDA(ctx, cudaMemcpyAsync(dw, ow, nw_(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  cudaEventRecord(t1, ctx->stream);
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->ms_setup = ev_ms(ctx, 0, 1);
+  ctx->ms_factor = ev_ms(ctx, 1, 2);
+  ctx->ms_solve = ev_ms(ctx, 2, 3);
+  ctx->ms_apply = ev_ms(ctx, 3, 4);
+  float tot = 0;
+  cudaEventElapsedTime(&tot, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  fill_stats(ctx, stats, status, tot);
+  return status;
+}
+
+// ---------------------------------------------------------------- diagnostics
+// Dense FP64 view of a compact array of type T.
+template <typename T>
+int dump_dense(xfp_ctx* ctx, const T* compact, double* host_out) {
+  if (!host_out) return XFP_OK;
+  const size_t n = ncells(ctx->ni, ctx->nj, ctx->nk);
+  XFP_CUDA(ctx, ctx->dense.ensure(n * sizeof(double)));
+  const double* src64;
+  if (std::is_same<T, double>::value) {
+    src64 = (const double*)compact;
+  } else {
+    XFP_CUDA(ctx, ctx->io_gw.ensure((ctx->M + 8) * sizeof(double)));
+    XFP_CUDA(ctx, (convert<float, double>((const float*)compact, ctx->io_gw.as<double>(), ctx->M, ctx->stream)));
+    src64 = ctx->io_gw.as<double>();
+  }
+  XFP_CUDA(ctx, scatter_dense<double>(src64, ctx->lines.as<Line>(), ctx->ni, ctx->nj, ctx->nk,
+                                      ctx->dense.as<double>(), ctx->stream));
+  XFP_CUDA(ctx, cudaMemcpyAsync(host_out, ctx->dense.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XFP_OK;
+}
+
+// VT/IT/CT as in the solve of the context's precision; A: coefficients used by
+// the factor (CT) and by the SpMV (VT).
+template <typename VT, typename IT, typename CT>
+int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* const F[6], IT* inv,
+               const VT* const L[3], const double* dr, double* out[11]) {
+  int rc;
+  const long long M = ctx->M;
+  cudaStream_t st = ctx->stream;
+  if ((rc = factor<VT, IT, CT>(ctx, Af, F, inv, (CT)ctx->opt.omega, (CT)ctx->opt.min_diag_ratio))) return rc;
+  if (!std::is_same<VT, CT>::value)
+    for (int q = 0; q < 3; ++q) XFP_CUDA(ctx, (convert<CT, VT>(F[q], const_cast<VT*>(L[q]), M, st)));
+  // r -> compact (VT), sweeps, SpMV
+  VT* r = reinterpret_cast<VT*>(ctx->r32.p ? ctx->r32.p : ctx->r64.p);
+  VT* z = reinterpret_cast<VT*>(ctx->z32.p ? ctx->z32.p : ctx->z64.p);
+  VT* qv = reinterpret_cast<VT*>(ctx->s32.p ? ctx->s32.p : ctx->s64.p);
+  if (std::is_same<VT, double>::value) {
+    r = (VT*)ctx->r64.p; z = (VT*)ctx->z64.p; qv = (VT*)ctx->s64.p;
+  }
+  if (dr) {
+    XFP_CUDA(ctx, ctx->io_p.ensure(ncells(ctx->ni, ctx->nj, ctx->nk) * sizeof(double)));
+    XFP_CUDA(ctx, cudaMemcpyAsync(ctx->io_p.p, dr, ncells(ctx->ni, ctx->nj, ctx->nk) * sizeof(double),
+                                  cudaMemcpyHostToDevice, st));
+    XFP_CUDA(ctx, ctx->io_gv.ensure((M + 8) * sizeof(double)));
+    XFP_CUDA(ctx, gather_compact<double>(ctx->io_p.as<double>(), ctx->lines.as<Line>(), ctx->ni, ctx->nj, ctx->nk,
+                                         ctx->io_gv.as<double>(), st));
+    if (std::is_same<VT, double>::value)
+      XFP_CUDA(ctx, copy_vec<double>(ctx->io_gv.as<double>(), (double*)r, M, st));
+    else
+      XFP_CUDA(ctx, (convert<double, float>(ctx->io_gv.as<double>(), (float*)r, M, st)));
+    SweepData<VT, IT, CT> d;
+    d.r = r; d.y = z; d.lx = L[0]; d.ly = L[1]; d.lz = L[2]; d.inv = inv;
+    d.partials = ctx->tpartials.as<double>();
+    SweepGrid g = make_grid(ctx, nullptr, 0);
+    if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_FWD, g, d))) return rc;
+    if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_BWD, g, d))) return rc;
+    XFP_CUDA(ctx, (spmv_dot<VT, VT, VT>(Av[0], Av[1], Av[2], Av[3], r, qv, ctx->lines.as<Line>(), ctx->ni, ctx->nj,
+                                        ctx->nk, M, nullptr, (VT*)nullptr, NBLK_MAX, 1, st)));
+  }
+  XFP_CUDA(ctx, cudaStreamSynchronize(st));
+  if ((rc = check_sweep_error(ctx))) return rc;
+  for (int q = 0; q < 5; ++q)
+    if ((rc = dump_dense<CT>(ctx, Af[q], out[q]))) return rc;
+  if ((rc = dump_dense<IT>(ctx, inv, out[5]))) return rc;
+  for (int q = 0; q < 3; ++q)
+    if ((rc = dump_dense<CT>(ctx, F[q], out[6 + q]))) return rc;
+  if (dr) {
+    if ((rc = dump_dense<VT>(ctx, z, out[9]))) return rc;
+    if ((rc = dump_dense<VT>(ctx, qv, out[10]))) return rc;
+  }
+  return XFP_OK;
+}
+
+}  // namespace
+
+// ============================================================================ C ABI
+extern "C" {
+
+const char* xfp_version(void) { return "xfp 0.1 (sm_100a)"; }
+
+void xfp_default_options(xfp_options* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->tol = 1e-5;
+  o->max_iter = 100;
+  o->omega = 0.97;
+  o->min_diag_ratio = 0.25;
+  o->precision = XFP_PREC_F64;
+  o->device_pointers = 0;
+  o->device = 0;
+  o->check_every = 8;
+  o->timeout_ms = 2000.0;
+  o->max_refine = 20;
+  o->inner_tol = 1e-6;
+  o->tile_k = 16;
+  o->stream = nullptr;
+}
+
+static int validate_options(xfp_ctx* ctx, const xfp_options* o) {
+  if (o->precision < XFP_PREC_F64 || o->precision > XFP_PREC_MIXED) return fail(ctx, XFP_ERR_ARGS, "bad precision");
+  if (!(o->omega >= 0.0 && o->omega <= 1.0)) return fail(ctx, XFP_ERR_ARGS, "omega must be in [0,1]");
+  if (!(o->min_diag_ratio >= 0.0)) return fail(ctx, XFP_ERR_ARGS, "min_diag_ratio must be >= 0");
+  if (o->tile_k != 0 && o->tile_k != 8 && o->tile_k != 16) return fail(ctx, XFP_ERR_ARGS, "tile_k must be 8 or 16");
+  return XFP_OK;
+}
+
+int xfp_create(xfp_ctx** out, const xfp_options* opt) {
+  if (!out) return XFP_ERR_ARGS;
+  *out = nullptr;
+  xfp_ctx* ctx = new xfp_ctx();
+  xfp_options o;
+  xfp_default_options(&o);
+  if (opt) o = *opt;
+  int rc = validate_options(ctx, &o);
+  if (rc) { delete ctx; return rc; }
+  ctx->opt = o;
+  ctx->device = o.device;
+  ctx->nw = o.tile_k ? o.tile_k : 16;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    delete ctx;
+    return XFP_ERR_CUDA;
+  }
+  if (o.device < 0 || o.device >= ndev || cudaSetDevice(o.device) != cudaSuccess) {
+    delete ctx;
+    return XFP_ERR_ARGS;
+  }
+  cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, o.device);
+  if (o.stream) {
+    ctx->stream = (cudaStream_t)o.stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete ctx;
+      return XFP_ERR_CUDA;
+    }
+    ctx->own_stream = true;
+  }
+  for (auto& e : ctx->ev) cudaEventCreate(&e);
+  if (ctx->ctl.ensure(sizeof(SweepCtl)) != cudaSuccess) { xfp_destroy(ctx); return XFP_ERR_NOMEM; }
+  SweepCtl c0{1, 0, 0, 0};
+  cudaMemcpy(ctx->ctl.p, &c0, sizeof(c0), cudaMemcpyHostToDevice);
+  *out = ctx;
+  return XFP_OK;
+}
+
+int xfp_destroy(xfp_ctx* ctx) {
+  if (!ctx) return XFP_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  DevBuf* all[] = {&ctx->io_mat, &ctx->io_u, &ctx->io_v, &ctx->io_w, &ctx->io_wu, &ctx->io_wv, &ctx->io_ww,
+                   &ctx->io_p, &ctx->io_gu, &ctx->io_gv, &ctx->io_gw, &ctx->lines, &ctx->lens,
+                   &ctx->tile_active, &ctx->tiles, &ctx->counters, &ctx->inv64, &ctx->inv32, &ctx->x64,
+                   &ctx->r64, &ctx->x32, &ctx->r32, &ctx->s32, &ctx->z32, &ctx->s64, &ctx->z64, &ctx->dense,
+                   &ctx->prog, &ctx->ctl, &ctx->scal, &ctx->scal2, &ctx->partials, &ctx->tpartials};
+  for (DevBuf* b : all) b->release();
+  for (auto& b : ctx->A64) b.release();
+  for (auto& b : ctx->A32) b.release();
+  for (auto& b : ctx->F64) b.release();
+  for (auto& b : ctx->F32) b.release();
+  for (auto& b : ctx->L32) b.release();
+  for (auto& e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return XFP_OK;
+}
+
+int xfp_set_options(xfp_ctx* ctx, const xfp_options* opt) {
+  if (!ctx || !opt) return XFP_ERR_ARGS;
+  int rc = validate_options(ctx, opt);
+  if (rc) return rc;
+  if (opt->device != ctx->device) return fail(ctx, XFP_ERR_ARGS, "device cannot change on a live context");
+  void* keep_stream = ctx->opt.stream;
+  ctx->opt = *opt;
+  ctx->opt.stream = keep_stream;
+  int nw = opt->tile_k ? opt->tile_k : 16;
+  if (nw != ctx->nw) {
+    ctx->nw = nw;
+    ctx->prog_cap = 0;  // progress words are re-zeroed for the new tile shape
+  }
+  return XFP_OK;
+}
+
+const char* xfp_last_error(const xfp_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int xfp_solve_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const double* u,
+                  const double* v, const double* w, const double* wu, const double* wv, const double* ww,
+                  double* pressure, xfp_stats* stats) {
+  return project_impl<double>(ctx, ni, nj, nk, material, const_cast<double*>(u), const_cast<double*>(v),
+                              const_cast<double*>(w), wu, wv, ww, pressure, stats, false);
+}
+int xfp_solve_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const float* u,
+                  const float* v, const float* w, const float* wu, const float* wv, const float* ww,
+                  float* pressure, xfp_stats* stats) {
+  return project_impl<float>(ctx, ni, nj, nk, material, const_cast<float*>(u), const_cast<float*>(v),
+                             const_cast<float*>(w), wu, wv, ww, pressure, stats, false);
+}
+int xfp_project_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, double* u, double* v,
+                    double* w, const double* wu, const double* wv, const double* ww, double* pressure,
+                    xfp_stats* stats) {
+  return project_impl<double>(ctx, ni, nj, nk, material, u, v, w, wu, wv, ww, pressure, stats, true);
+}
+int xfp_project_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, float* u, float* v,
+                    float* w, const float* wu, const float* wv, const float* ww, float* pressure,
+                    xfp_stats* stats) {
+  return project_impl<float>(ctx, ni, nj, nk, material, u, v, w, wu, wv, ww, pressure, stats, true);
+}
+int xfp_apply_pressure_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const double* wu,
+                           const double* wv, const double* ww, const double* pressure, double* u, double* v,
+                           double* w) {
+  return apply_impl<double>(ctx, ni, nj, nk, material, wu, wv, ww, pressure, u, v, w);
+}
+int xfp_apply_pressure_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const float* wu,
+                           const float* wv, const float* ww, const float* pressure, float* u, float* v,
+                           float* w) {
+  return apply_impl<float>(ctx, ni, nj, nk, material, wu, wv, ww, pressure, u, v, w);
+}
+int xfp_project_backward_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const double* wu,
+                             const double* wv, const double* ww, const double* gu, const double* gv,
+                             const double* gw, double* du, double* dv, double* dw, xfp_stats* stats) {
+  return backward_impl<double>(ctx, ni, nj, nk, material, wu, wv, ww, gu, gv, gw, du, dv, dw, stats);
+}
+int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const double* u,
+                     const double* v, const double* w, const double* wu, const double* wv, const double* ww,
+                     const double* r, double* diag, double* ax, double* ay, double* az, double* b, double* inv,
+                     double* lx, double* ly, double* lz, double* z, double* q) {
+  int rc = check_dims(ctx, ni, nj, nk, material);
+  if (rc) return rc;
+  if (!u || !v || !w) return fail(ctx, XFP_ERR_ARGS, "velocity arrays must not be NULL");
+  if (ctx->opt.device_pointers) return fail(ctx, XFP_ERR_UNSUPPORTED, "diagnostics take host pointers");
+  XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  const uint8_t* dmat;
+  const double *du_, *dv, *dw, *dwu, *dwv, *dww;
+  if ((rc = stage_in(ctx, ctx->io_mat, material, ncells(ni, nj, nk), &dmat))) return rc;
+  if ((rc = stage_in<double>(ctx, ctx->io_u, u, nu(ni, nj, nk), &du_))) return rc;
+  if ((rc = stage_in<double>(ctx, ctx->io_v, v, nv(ni, nj, nk), &dv))) return rc;
+  if ((rc = stage_in<double>(ctx, ctx->io_w, w, nw_(ni, nj, nk), &dw))) return rc;
+  if ((rc = stage_in<double>(ctx, ctx->io_wu, wu, nu(ni, nj, nk), &dwu))) return rc;
+  if ((rc = stage_in<double>(ctx, ctx->io_wv, wv, nv(ni, nj, nk), &dwv))) return rc;
+  if ((rc = stage_in<double>(ctx, ctx->io_ww, ww, nw_(ni, nj, nk), &dww))) return rc;
+  const int prec = ctx->opt.precision;
+  if ((rc = build_layout(ctx, dmat, ni, nj, nk))) return rc;
+  if ((rc = ensure_compact(ctx, prec))) return rc;
+  if (prec == XFP_PREC_F64) {
+    XFP_CUDA(ctx, ctx->s64.ensure((ctx->M + 8) * 8));
+    XFP_CUDA(ctx, ctx->z64.ensure((ctx->M + 8) * 8));
+  }
+  const Line* lines = ctx->lines.as<Line>();
+  double* out[11] = {diag, ax, ay, az, b, inv, lx, ly, lz, z, q};
+  cudaStream_t st = ctx->stream;
+  if (prec == XFP_PREC_F64) {
+    double* A[5];
+    for (int k = 0; k < 5; ++k) A[k] = ctx->A64[k].as<double>();
+    XFP_CUDA(ctx, (assemble<double, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
+                                            A[3], A[4], st)));
+    double* F[6];
+    for (int k = 0; k < 6; ++k) F[k] = ctx->F64[k].as<double>();
+    const double* Af[5] = {A[0], A[1], A[2], A[3], A[4]};
+    const double* Av[4] = {A[0], A[1], A[2], A[3]};
+    const double* L[3] = {F[0], F[1], F[2]};
+    return debug_core<double, double, double>(ctx, Af, Av, F, ctx->inv64.as<double>(), L, r, out);
+  } else if (prec == XFP_PREC_F32) {
+    float* A[5];
+    for (int k = 0; k < 5; ++k) A[k] = ctx->A32[k].as<float>();
+    XFP_CUDA(ctx, (assemble<double, float>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
+                                           A[3], A[4], st)));
+    float* F[6];
+    for (int k = 0; k < 6; ++k) F[k] = ctx->F32[k].as<float>();
+    const float* Af[5] = {A[0], A[1], A[2], A[3], A[4]};
+    const float* Av[4] = {A[0], A[1], A[2], A[3]};
+    const float* L[3] = {F[0], F[1], F[2]};
+    return debug_core<float, float, float>(ctx, Af, Av, F, ctx->inv32.as<float>(), L, r, out);
+  } else {
+    double* A[5];
+    for (int k = 0; k < 5; ++k) A[k] = ctx->A64[k].as<double>();
+    XFP_CUDA(ctx, (assemble<double, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
+                                            A[3], A[4], st)));
+    float* A32[4];
+    for (int k = 0; k < 4; ++k) {
+      A32[k] = ctx->A32[k].as<float>();
+      XFP_CUDA(ctx, (convert<double, float>(A[k], A32[k], ctx->M, st)));
+    }
+    double* F[6];
+    for (int k = 0; k < 6; ++k) F[k] = ctx->F64[k].as<double>();
+    const double* Af[5] = {A[0], A[1], A[2], A[3], A[4]};
+    const float* Av[4] = {A32[0], A32[1], A32[2], A32[3]};
+    const float* L[3] = {ctx->L32[0].as<float>(), ctx->L32[1].as<float>(), ctx->L32[2].as<float>()};
+    return debug_core<float, double, double>(ctx, Af, Av, F, ctx->inv64.as<double>(), L, r, out);
+  }
+}
+
+int xfp_project_backward_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const float* wu,
+                             const float* wv, const float* ww, const float* gu, const float* gv,
+                             const float* gw, float* du, float* dv, float* dw, xfp_stats* stats) {
+  return backward_impl<float>(ctx, ni, nj, nk, material, wu, wv, ww, gu, gv, gw, du, dv, dw, stats);
+}
+
+}  // extern "C"

@@ -1,0 +1,83 @@
+// xfp_common.cuh -- shared device helpers and layout structures for libxfp.
+//
+// Storage layout ("line-compacted"): the grid is cut into x-lines, one per
+// (j,k).  Each line that holds an unknown stores the cells of its active span
+// [lo, lo+len) contiguously, lo rounded down and len rounded up to a multiple
+// of XFP_ALIGN cells, at offset `off` in every per-cell array.  Because off and
+// lo are both multiples of XFP_ALIGN, cell i of ANY line sits at an address
+// congruent to i modulo XFP_ALIGN, so aligned vector loads of neighbour lines
+// stay aligned.  Cells inside a span that are not unknowns (air, uncoupled
+// solid) are padding: zero coefficients, zero vectors, null rows.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define XFP_ALIGN 4
+#define XFP_FULL 0xffffffffu
+
+namespace xfp {
+
+enum : uint8_t { MAT_AIR = 0, MAT_FLUID = 1, MAT_SOLID = 2 };
+
+// Per-line record: off (start in compact arrays), lo (first stored i), len
+// (stored cells, 0 = line has no unknown), nrows (unknowns on the line).
+struct __align__(16) Line {
+  int off, lo, len, nrows;
+};
+
+// Control block of the persistent sweep kernels (one per context).
+struct SweepCtl {
+  unsigned int gen;        // launch generation; progress words carry it in their high half
+  unsigned int finished;   // CTAs finished in the current launch
+  unsigned int err;        // nonzero: a bounded wait ran out (XFP_ERR_TIMEOUT)
+  unsigned int err_where;  // which wait (for diagnostics)
+};
+
+// Scalars of one PCG solve, resident on the device.
+struct PcgScalars {
+  double rho, alpha, beta, res, tolabs, bnorm, dot_tmp;
+  int done, iters, status, maxit;
+  unsigned int red_count;  // last-block-done counter of the reductions
+  unsigned int pad;
+};
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ double ld_relaxed(const double* p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ float ld_relaxed(const float* p) {
+  float v;
+  asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned int ld_volatile_u32(const unsigned int* p) {
+  return *(const volatile unsigned int*)p;
+}
+
+// Rounded arithmetic without contraction: the FP64 path follows xFluid's
+// operation order exactly, so no multiply-add may be fused.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rsqrt_ref(double x) { return __ddiv_rn(1.0, __dsqrt_rn(x)); }
+__device__ __forceinline__ float rsqrt_ref(float x) { return __fdiv_rn(1.0f, __fsqrt_rn(x)); }
+
+template <typename T>
+__device__ __forceinline__ T shfl_up(T v, int d) { return __shfl_up_sync(XFP_FULL, v, d); }
+template <typename T>
+__device__ __forceinline__ T shfl_down(T v, int d) { return __shfl_down_sync(XFP_FULL, v, d); }
+
+}  // namespace xfp

@@ -1,0 +1,123 @@
+// xfp_kernels.h -- host-side launchers of libxfp's device kernels (internal).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "xfp_common.cuh"
+
+namespace xfp {
+
+enum { SWEEP_FACTOR = 0, SWEEP_FWD = 1, SWEEP_BWD = 2 };
+
+// Static description of one sweep launch (tiles, progress words, control).
+struct SweepGrid {
+  int ni, nj, nk, NJt, NKt, ntiles, maxT;
+  int bwd_mode;                 // backward: 0 = initial rho, 1 = beta update
+  const Line* lines;            // [nk*nj]
+  const int* tiles;             // active tiles, topological order, J | K<<16
+  const unsigned char* tile_active;  // [NKt*NJt]
+  unsigned long long* prog;     // [nk*NJt] progress words
+  SweepCtl* ctl;
+  long long spin_limit;
+  PcgScalars* scal;             // forward/backward: skip when done; backward: rho/beta
+};
+
+// Arrays of one sweep.  VT: vector/L type of the solves, IT: invdiag type,
+// CT: factor arithmetic (and A input) type.
+template <typename VT, typename IT, typename CT>
+struct SweepData {
+  const VT* r = nullptr;        // forward: rhs r; backward: r for the fused z.r
+  VT* y = nullptr;              // forward: out y; backward: in y, out z (in place)
+  const VT* lx = nullptr;
+  const VT* ly = nullptr;
+  const VT* lz = nullptr;
+  const IT* inv = nullptr;
+  const CT* diag = nullptr;     // factor inputs
+  const CT* ax = nullptr;
+  const CT* ay = nullptr;
+  const CT* az = nullptr;
+  CT* flx = nullptr;            // factor outputs keyed by the higher cell: L and
+  CT* fly = nullptr;            // the dropped-fill sum ("missing") for that row
+  CT* flz = nullptr;
+  CT* fmx = nullptr;
+  CT* fmy = nullptr;
+  CT* fmz = nullptr;
+  IT* oinv = nullptr;
+  CT omega = CT(0.97), ratio = CT(0.25);
+  double* partials = nullptr;   // backward: one dot partial per tile
+};
+
+#define XFP_SWEEP_DECL(VT, IT, CT)                                                             \
+  cudaError_t sweep_launch(int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d, int nw, \
+                           int grid, cudaStream_t st);                                         \
+  int sweep_max_grid(int op, const SweepData<VT, IT, CT>& d, int nw);
+XFP_SWEEP_DECL(double, double, double)
+XFP_SWEEP_DECL(float, float, float)
+XFP_SWEEP_DECL(float, double, double)
+#undef XFP_SWEEP_DECL
+
+// ---- layout (xfp_layout.cu) ----
+// Builds the line table and the active-tile list for a material grid.
+// Returns on the host: stored cells M, unknown rows, active lines, active tiles.
+struct LayoutDev {
+  Line* lines;               // [nk*nj]
+  int* line_len_scan;        // scratch [nk*nj + 1]
+  unsigned char* tile_active;// [NKt*NJt]
+  int* tiles;                // [NKt*NJt]
+  long long* counters;       // [4] M, rows, lines, ntiles (device)
+};
+cudaError_t layout_build(const uint8_t* mat, int ni, int nj, int nk, int tile_k, LayoutDev L,
+                         cudaStream_t st);
+
+// ---- assembly / apply / vector kernels (xfp_ops.cu) ----
+template <typename FT, typename AT>
+cudaError_t assemble(const uint8_t* mat, const FT* u, const FT* v, const FT* w, const FT* wu,
+                     const FT* wv, const FT* ww, int ni, int nj, int nk, const Line* lines,
+                     AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st);
+
+template <typename T>
+cudaError_t scatter_dense(const T* x, const Line* lines, int ni, int nj, int nk, T* dense,
+                          cudaStream_t st);
+template <typename FT, typename PT>
+cudaError_t apply_pressure(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
+                           const PT* p, int ni, int nj, int nk, FT* u, FT* v, FT* w,
+                           cudaStream_t st);
+template <typename FT, typename PT>
+cudaError_t apply_pressure_T(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
+                             const FT* gu, const FT* gv, const FT* gw, int ni, int nj, int nk,
+                             const Line* lines, PT* q, cudaStream_t st);
+template <typename FT, typename PT>
+cudaError_t rhs_T(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww, const PT* lam,
+                  const Line* lines, int ni, int nj, int nk, const FT* gu, const FT* gv,
+                  const FT* gw, FT* du, FT* dv, FT* dw, cudaStream_t st);
+
+// PCG vector kernels over the compact arrays (length M).
+template <typename VT, typename AT, typename DT>
+cudaError_t spmv_dot(const AT* diag, const AT* ax, const AT* ay, const AT* az, const VT* s,
+                     VT* z, const Line* lines, int ni, int nj, int nk, long long M,
+                     PcgScalars* sc, DT* partials, int nblk_max, int mode, cudaStream_t st);
+template <typename VT, typename DT>
+cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgScalars* sc,
+                      double* partials, int nblk_max, cudaStream_t st);
+template <typename VT>
+cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st);
+template <typename VT>
+cudaError_t absmax_init(const VT* b, long long M, PcgScalars* sc, double* partials, int nblk_max,
+                        double tol, int maxit, cudaStream_t st);
+template <typename A, typename B>
+cudaError_t convert(const A* in, B* out, long long n, cudaStream_t st);
+template <typename T>
+cudaError_t gather_compact(const T* dense, const Line* lines, int ni, int nj, int nk, T* x,
+                           cudaStream_t st);
+template <typename T>
+cudaError_t copy_vec(const T* in, T* out, long long n, cudaStream_t st);
+
+// Mixed precision: r64 = b64 - A64 x64, |r|_inf and r32 = (float) r64 / scale.
+cudaError_t residual64(const double* diag, const double* ax, const double* ay, const double* az,
+                       const double* b, const double* x, double* r, const Line* lines, int ni,
+                       int nj, int nk, long long M, PcgScalars* sc, double* partials,
+                       int nblk_max, cudaStream_t st);
+cudaError_t refine_update(double* x64, const float* e32, long long M, cudaStream_t st);
+
+}  // namespace xfp

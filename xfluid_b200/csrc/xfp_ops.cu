@@ -1,0 +1,790 @@
+// xfp_ops.cu -- assembly, pressure update, adjoint pieces and the PCG vector
+// kernels of libxfp, over the line-compacted layout (xfp_common.cuh).
+//
+// Reference (paths relative to xFluid/xFluid/):
+//   assembly        variationalpressure/variational_pressuresolver.cpp:231-327
+//   applyPressure   variationalpressure/variational_pressuresolver.cpp:120-220
+//   SpMV            variationalpressure/sparse_matrix.h:264-276
+//   PCG loop        variationalpressure/pcg_solver.h:243-285
+//   dot/axpy/absmax variationalpressure/blas_wrapper.h:12-51
+#include <algorithm>
+#include <type_traits>
+
+#include "xfp_common.cuh"
+#include "xfp_kernels.h"
+
+namespace xfp {
+
+constexpr int RED_THREADS = 256;
+
+__device__ __forceinline__ size_t uix(int ni, int nj, int i, int j, int k) {
+  return ((size_t)k * nj + j) * (size_t)(ni + 1) + i;
+}
+__device__ __forceinline__ size_t vix(int ni, int nj, int i, int j, int k) {
+  return ((size_t)k * (nj + 1) + j) * (size_t)ni + i;
+}
+__device__ __forceinline__ size_t wix(int ni, int nj, int i, int j, int k) {
+  return ((size_t)k * nj + j) * (size_t)ni + i;
+}
+
+// ---------------------------------------------------------------------------
+// Assembly: one warp per x-line, lanes over the line's stored span.
+//  fluid c, neighbour n across face f (weight m), order +i,-i,+j,-j,+k,-k
+//  (xfluidutil.cpp:33-41):
+//    n fluid: A(c,c)+=m,    A(c,n)=-m,    b(c)+=vsign*u*m      (:294-301)
+//    n air:   A(c,c)+=2m,                 b(c)+=vsign*u*m      (:302-308)
+//    n solid: A(c,c)+=0.5m, A(c,n)=-0.5m, b(c)+=vsign*u*0.5*m  (:309-316)
+//  solid s: rows added from its fluid neighbours' loops (:318-320) in the
+//  loop order i-major, j, k-minor, i.e. neighbours -x,-y,-z,+z,+y,+x.
+// ---------------------------------------------------------------------------
+template <typename FT, typename AT>
+__global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __restrict__ u,
+                                const FT* __restrict__ v, const FT* __restrict__ w,
+                                const FT* __restrict__ wu, const FT* __restrict__ wv,
+                                const FT* __restrict__ ww, int ni, int nj, int nk,
+                                const Line* __restrict__ lines, AT* __restrict__ diag,
+                                AT* __restrict__ ax, AT* __restrict__ ay, AT* __restrict__ az,
+                                AT* __restrict__ b) {
+  const int lane = threadIdx.x & 31;
+  const long long nlines = (long long)nj * nk;
+  const size_t nn = (size_t)ni * nj;
+  for (long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
+       line += (long long)gridDim.x * (blockDim.x >> 5)) {
+    const Line L = lines[line];
+    if (L.len == 0) continue;
+    const int j = (int)(line % nj), k = (int)(line / nj);
+    for (int q = lane; q < L.len; q += 32) {
+      const int i = L.lo + q;
+      const size_t c = (size_t)k * nn + (size_t)j * ni + i;
+      const size_t o = (size_t)L.off + q;
+      AT d = AT(0), bb = AT(0), ox = AT(0), oy = AT(0), oz = AT(0);
+      const uint8_t m = i < ni ? mat[c] : MAT_AIR;
+      if (m == MAT_FLUID || m == MAT_SOLID) {
+        // neighbour (di,dj,dk), face value, weight, vsign
+        auto face = [&](int nb, AT& uf, AT& mf, AT& vs, int& ii, int& jj, int& kk) -> bool {
+          const int di = nb == 0 ? 1 : nb == 1 ? -1 : 0;
+          const int dj = nb == 2 ? 1 : nb == 3 ? -1 : 0;
+          const int dk = nb == 4 ? 1 : nb == 5 ? -1 : 0;
+          ii = i + di; jj = j + dj; kk = k + dk;
+          if (ii < 0 || jj < 0 || kk < 0 || ii >= ni || jj >= nj || kk >= nk) return false;
+          vs = (di + dj + dk) > 0 ? AT(-1) : AT(1);
+          const int fi = i + (di > 0), fj = j + (dj > 0), fk = k + (dk > 0);
+          if (di) {
+            const size_t f = uix(ni, nj, fi, fj, fk);
+            uf = (AT)u[f]; mf = wu ? (AT)wu[f] : AT(1);
+          } else if (dj) {
+            const size_t f = vix(ni, nj, fi, fj, fk);
+            uf = (AT)v[f]; mf = wv ? (AT)wv[f] : AT(1);
+          } else {
+            const size_t f = wix(ni, nj, fi, fj, fk);
+            uf = (AT)w[f]; mf = ww ? (AT)ww[f] : AT(1);
+          }
+          return true;
+        };
+        if (m == MAT_FLUID) {
+#pragma unroll
+          for (int nb = 0; nb < 6; ++nb) {
+            AT uf, mf, vs;
+            int ii, jj, kk;
+            if (!face(nb, uf, mf, vs, ii, jj, kk)) continue;
+            const uint8_t mn = mat[(size_t)kk * nn + (size_t)jj * ni + ii];
+            AT off = AT(0);
+            if (mn == MAT_FLUID) {
+              d = add_rn(d, mul_rn(AT(1), mf));
+              off = mul_rn(AT(-1), mf);
+              bb = add_rn(bb, mul_rn(mul_rn(vs, uf), mf));
+            } else if (mn == MAT_AIR) {
+              d = add_rn(d, mul_rn(AT(2), mf));
+              bb = add_rn(bb, mul_rn(mul_rn(vs, uf), mf));
+            } else {
+              d = add_rn(d, mul_rn(AT(0.5), mf));
+              off = mul_rn(AT(-0.5), mf);
+              bb = add_rn(bb, mul_rn(mul_rn(mul_rn(vs, uf), AT(0.5)), mf));
+            }
+            if (nb == 1) ox = off;
+            if (nb == 3) oy = off;
+            if (nb == 5) oz = off;
+          }
+        } else {
+          const int order[6] = {1, 3, 5, 4, 2, 0};
+#pragma unroll
+          for (int t = 0; t < 6; ++t) {
+            const int nb = order[t];
+            AT uf, mf, vs;
+            int ii, jj, kk;
+            if (!face(nb, uf, mf, vs, ii, jj, kk)) continue;
+            if (mat[(size_t)kk * nn + (size_t)jj * ni + ii] != MAT_FLUID) continue;
+            d = add_rn(d, mul_rn(AT(0.5), mf));
+            const AT off = mul_rn(AT(-0.5), mf);
+            bb = add_rn(bb, mul_rn(mul_rn(mul_rn(vs, uf), AT(0.5)), mf));
+            if (nb == 1) ox = off;
+            if (nb == 3) oy = off;
+            if (nb == 5) oz = off;
+          }
+        }
+      }
+      diag[o] = d; ax[o] = ox; ay[o] = oy; az[o] = oz; b[o] = bb;
+    }
+  }
+}
+
+template <typename FT, typename AT>
+cudaError_t assemble(const uint8_t* mat, const FT* u, const FT* v, const FT* w, const FT* wu,
+                     const FT* wv, const FT* ww, int ni, int nj, int nk, const Line* lines,
+                     AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st) {
+  const long long nlines = (long long)nj * nk;
+  long long blocks = (nlines + 7) / 8;
+  if (blocks > 65535 * 8) blocks = 65535 * 8;
+  assemble_kernel<FT, AT><<<(unsigned)blocks, 256, 0, st>>>(mat, u, v, w, wu, wv, ww, ni, nj, nk, lines,
+                                                          diag, ax, ay, az, b);
+  return cudaGetLastError();
+}
+template cudaError_t assemble<double, double>(const uint8_t*, const double*, const double*,
+                                              const double*, const double*, const double*,
+                                              const double*, int, int, int, const Line*, double*,
+                                              double*, double*, double*, double*, cudaStream_t);
+template cudaError_t assemble<float, float>(const uint8_t*, const float*, const float*, const float*,
+                                            const float*, const float*, const float*, int, int, int,
+                                            const Line*, float*, float*, float*, float*, float*,
+                                            cudaStream_t);
+template cudaError_t assemble<float, double>(const uint8_t*, const float*, const float*,
+                                             const float*, const float*, const float*, const float*,
+                                             int, int, int, const Line*, double*, double*, double*,
+                                             double*, double*, cudaStream_t);
+template cudaError_t assemble<double, float>(const uint8_t*, const double*, const double*,
+                                             const double*, const double*, const double*,
+                                             const double*, int, int, int, const Line*, float*,
+                                             float*, float*, float*, float*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Compact -> dense pressure grid: every cell written, 0 outside unknowns
+// (variational_pressuresolver.cpp:86-101 copies every cell of the solution).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void scatter_dense_kernel(const T* __restrict__ x, const Line* __restrict__ lines, int ni,
+                                     int nj, int nk, T* __restrict__ dense) {
+  const size_t n = (size_t)ni * nj * nk;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % ni);
+    const size_t line = c / ni;
+    const Line L = lines[line];
+    T val = T(0);
+    if ((unsigned)(i - L.lo) < (unsigned)L.len) val = x[(size_t)L.off + (i - L.lo)];
+    dense[c] = val;
+  }
+}
+template <typename T>
+cudaError_t scatter_dense(const T* x, const Line* lines, int ni, int nj, int nk, T* dense,
+                          cudaStream_t st) {
+  size_t n = (size_t)ni * nj * nk;
+  unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32);
+  scatter_dense_kernel<T><<<blocks, 256, 0, st>>>(x, lines, ni, nj, nk, dense);
+  return cudaGetLastError();
+}
+template cudaError_t scatter_dense<double>(const double*, const Line*, int, int, int, double*, cudaStream_t);
+template cudaError_t scatter_dense<float>(const float*, const Line*, int, int, int, float*, cudaStream_t);
+
+// Dense -> compact (cells of every stored span; padding cells get 0).
+template <typename T>
+__global__ void gather_compact_kernel(const T* __restrict__ dense, const Line* __restrict__ lines, int ni,
+                                      int nj, int nk, T* __restrict__ x) {
+  const int lane = threadIdx.x & 31;
+  const long long nlines = (long long)nj * nk;
+  for (long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
+       line += (long long)gridDim.x * (blockDim.x >> 5)) {
+    const Line L = lines[line];
+    for (int q = lane; q < L.len; q += 32) {
+      const int i = L.lo + q;
+      x[(size_t)L.off + q] = i < ni ? dense[(size_t)line * ni + i] : T(0);
+    }
+  }
+}
+template <typename T>
+cudaError_t gather_compact(const T* dense, const Line* lines, int ni, int nj, int nk, T* x,
+                           cudaStream_t st) {
+  const long long nlines = (long long)nj * nk;
+  long long blocks = std::min<long long>((nlines + 7) / 8, 65535LL * 8);
+  gather_compact_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(dense, lines, ni, nj, nk, x);
+  return cudaGetLastError();
+}
+template cudaError_t gather_compact<double>(const double*, const Line*, int, int, int, double*, cudaStream_t);
+template cudaError_t gather_compact<float>(const float*, const Line*, int, int, int, float*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// applyPressure: per face, left/right cells (out of range counts as solid,
+// :151-152); fluid|fluid and fluid|solid use both pressures, fluid|air uses the
+// ghost -p (:161-198); u -= 1.0*(p2-p1) (:200).  Faces with weight 0 are closed.
+// ---------------------------------------------------------------------------
+template <typename PT>
+__device__ __forceinline__ bool face_dp(const uint8_t* mat, const PT* p, int ni, int nj, int nk,
+                                        int il, int jl, int kl, int ir, int jr, int kr, PT& dp) {
+  const size_t nn = (size_t)ni * nj;
+  const bool inl = il >= 0 && jl >= 0 && kl >= 0 && il < ni && jl < nj && kl < nk;
+  const bool inr = ir >= 0 && jr >= 0 && kr >= 0 && ir < ni && jr < nj && kr < nk;
+  const size_t cl = inl ? (size_t)kl * nn + (size_t)jl * ni + il : 0;
+  const size_t cr = inr ? (size_t)kr * nn + (size_t)jr * ni + ir : 0;
+  const uint8_t ml = inl ? mat[cl] : MAT_SOLID;
+  const uint8_t mr = inr ? mat[cr] : MAT_SOLID;
+  if (ml != MAT_FLUID && mr != MAT_FLUID) return false;
+  PT p1, p2;
+  if (ml == MAT_FLUID && mr == MAT_FLUID) {
+    p2 = p[cr]; p1 = p[cl];
+  } else if (ml == MAT_FLUID) {
+    p1 = p[cl];
+    if (mr == MAT_SOLID) {
+      if (!inr) return false;
+      p2 = p[cr];
+    } else {
+      p2 = -p1;
+    }
+  } else {
+    p2 = p[cr];
+    if (ml == MAT_SOLID) {
+      if (!inl) return false;
+      p1 = p[cl];
+    } else {
+      p1 = -p2;
+    }
+  }
+  dp = sub_rn(p2, p1);
+  return true;
+}
+
+template <typename FT, typename PT>
+__global__ void apply_kernel(const uint8_t* __restrict__ mat, const FT* __restrict__ wt,
+                             const PT* __restrict__ p, int ni, int nj, int nk, int axis,
+                             FT* __restrict__ f) {
+  const int si = ni + (axis == 0), sj = nj + (axis == 1), sk = nk + (axis == 2);
+  const size_t n = (size_t)si * sj * sk;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % si);
+    const int j = (int)((idx / si) % sj);
+    const int k = (int)(idx / ((size_t)si * sj));
+    if (wt && wt[idx] == FT(0)) continue;
+    PT dp;
+    if (face_dp(mat, p, ni, nj, nk, i - (axis == 0), j - (axis == 1), k - (axis == 2), i, j, k, dp)) {
+      f[idx] = sub_rn(f[idx], (FT)mul_rn(PT(1), dp));
+    }
+  }
+}
+template <typename FT, typename PT>
+cudaError_t apply_pressure(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
+                           const PT* p, int ni, int nj, int nk, FT* u, FT* v, FT* w,
+                           cudaStream_t st) {
+  for (int axis = 0; axis < 3; ++axis) {
+    size_t n = (size_t)(ni + (axis == 0)) * (nj + (axis == 1)) * (nk + (axis == 2));
+    unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32);
+    apply_kernel<FT, PT><<<blocks, 256, 0, st>>>(mat, axis == 0 ? wu : axis == 1 ? wv : ww, p, ni, nj, nk,
+                                                axis, axis == 0 ? u : axis == 1 ? v : w);
+  }
+  return cudaGetLastError();
+}
+template cudaError_t apply_pressure<double, double>(const uint8_t*, const double*, const double*,
+                                                    const double*, const double*, int, int, int,
+                                                    double*, double*, double*, cudaStream_t);
+template cudaError_t apply_pressure<float, float>(const uint8_t*, const float*, const float*,
+                                                  const float*, const float*, int, int, int, float*,
+                                                  float*, float*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Adjoint of the pressure update: q = G^T g, where applyPressure computes
+// u_out = u - G p (dp = p2 - p1 per updated face).  Gather per unknown cell.
+// ---------------------------------------------------------------------------
+template <typename FT, typename PT>
+__global__ void apply_T_kernel(const uint8_t* __restrict__ mat, const FT* __restrict__ wu,
+                               const FT* __restrict__ wv, const FT* __restrict__ ww,
+                               const FT* __restrict__ gu, const FT* __restrict__ gv,
+                               const FT* __restrict__ gw, int ni, int nj, int nk,
+                               const Line* __restrict__ lines, PT* __restrict__ q) {
+  const int lane = threadIdx.x & 31;
+  const long long nlines = (long long)nj * nk;
+  const size_t nn = (size_t)ni * nj;
+  for (long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
+       line += (long long)gridDim.x * (blockDim.x >> 5)) {
+    const Line L = lines[line];
+    if (L.len == 0) continue;
+    const int j = (int)(line % nj), k = (int)(line / nj);
+    for (int qq = lane; qq < L.len; qq += 32) {
+      const int i = L.lo + qq;
+      PT acc = PT(0);
+      if (i < ni) {
+        const uint8_t mc = mat[(size_t)k * nn + (size_t)j * ni + i];
+        if (mc == MAT_FLUID || mc == MAT_SOLID) {
+          // faces: low/high per axis; c is the right cell of its low face and
+          // the left cell of its high face
+          for (int axis = 0; axis < 3; ++axis) {
+            for (int side = 0; side < 2; ++side) {
+              const int di = axis == 0, dj = axis == 1, dk = axis == 2;
+              // face index (fi,fj,fk) and the other cell
+              const int fi = i + (side ? di : 0), fj = j + (side ? dj : 0), fk = k + (side ? dk : 0);
+              const int oi = side ? i + di : i - di, oj = side ? j + dj : j - dj, ok = side ? k + dk : k - dk;
+              size_t f;
+              const FT* wt;
+              const FT* gb;
+              if (axis == 0) { f = uix(ni, nj, fi, fj, fk); wt = wu; gb = gu; }
+              else if (axis == 1) { f = vix(ni, nj, fi, fj, fk); wt = wv; gb = gv; }
+              else { f = wix(ni, nj, fi, fj, fk); wt = ww; gb = gw; }
+              if (wt && wt[f] == FT(0)) continue;
+              const bool ino = oi >= 0 && oj >= 0 && ok >= 0 && oi < ni && oj < nj && ok < nk;
+              const uint8_t mo = ino ? mat[(size_t)ok * nn + (size_t)oj * ni + oi] : MAT_SOLID;
+              // c is 'r' when side==0 (low face), 'l' when side==1
+              const uint8_t ml = side ? mc : mo, mr = side ? mo : mc;
+              if (ml != MAT_FLUID && mr != MAT_FLUID) continue;
+              const PT g = (PT)gb[f];
+              PT coef = PT(0);
+              if (ml == MAT_FLUID && mr == MAT_FLUID) {
+                coef = side ? PT(-1) : PT(1);
+              } else if (ml == MAT_FLUID) {  // right is solid or air
+                if (mr == MAT_SOLID) {
+                  if (!ino && !side) continue;
+                  if (side && !ino) continue;
+                  coef = side ? PT(-1) : PT(1);
+                } else {
+                  coef = side ? PT(-2) : PT(0);
+                }
+              } else {  // left is solid or air, right is fluid
+                if (ml == MAT_SOLID) {
+                  if (!ino) continue;
+                  coef = side ? PT(-1) : PT(1);
+                } else {
+                  coef = side ? PT(0) : PT(2);
+                }
+              }
+              acc += coef * g;
+            }
+          }
+        }
+      }
+      q[(size_t)L.off + qq] = acc;
+    }
+  }
+}
+template <typename FT, typename PT>
+cudaError_t apply_pressure_T(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
+                             const FT* gu, const FT* gv, const FT* gw, int ni, int nj, int nk,
+                             const Line* lines, PT* q, cudaStream_t st) {
+  const long long nlines = (long long)nj * nk;
+  long long blocks = std::min<long long>((nlines + 7) / 8, 65535LL * 8);
+  apply_T_kernel<FT, PT><<<(unsigned)blocks, 256, 0, st>>>(mat, wu, wv, ww, gu, gv, gw, ni, nj, nk, lines, q);
+  return cudaGetLastError();
+}
+template cudaError_t apply_pressure_T<double, double>(const uint8_t*, const double*, const double*,
+                                                      const double*, const double*, const double*,
+                                                      const double*, int, int, int, const Line*,
+                                                      double*, cudaStream_t);
+template cudaError_t apply_pressure_T<float, float>(const uint8_t*, const float*, const float*,
+                                                    const float*, const float*, const float*,
+                                                    const float*, int, int, int, const Line*,
+                                                    float*, cudaStream_t);
+template cudaError_t apply_pressure_T<double, float>(const uint8_t*, const double*, const double*,
+                                                     const double*, const double*, const double*,
+                                                     const double*, int, int, int, const Line*,
+                                                     float*, cudaStream_t);
+template cudaError_t apply_pressure_T<float, double>(const uint8_t*, const float*, const float*,
+                                                     const float*, const float*, const float*,
+                                                     const float*, int, int, int, const Line*,
+                                                     double*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Adjoint of the right-hand side: d = g - D^T lam per face, D the assembly's
+// b = D u (coefficients vsign*m, halved next to solid; solid rows mirrored).
+// lam is the dense cell grid.
+// ---------------------------------------------------------------------------
+template <typename FT, typename PT>
+__global__ void rhs_T_kernel(const uint8_t* __restrict__ mat, const FT* __restrict__ wt,
+                             const PT* __restrict__ lam, int ni, int nj, int nk, int axis,
+                             const FT* __restrict__ g, FT* __restrict__ out) {
+  const int si = ni + (axis == 0), sj = nj + (axis == 1), sk = nk + (axis == 2);
+  const size_t n = (size_t)si * sj * sk;
+  const size_t nn = (size_t)ni * nj;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % si);
+    const int j = (int)((idx / si) % sj);
+    const int k = (int)(idx / ((size_t)si * sj));
+    const int il = i - (axis == 0), jl = j - (axis == 1), kl = k - (axis == 2);
+    const bool inl = il >= 0 && jl >= 0 && kl >= 0;
+    const bool inr = i < ni && j < nj && k < nk;
+    PT acc = PT(0);
+    if (inl && inr) {
+      const size_t cl = (size_t)kl * nn + (size_t)jl * ni + il, cr = (size_t)k * nn + (size_t)j * ni + i;
+      const uint8_t ml = mat[cl], mr = mat[cr];
+      const PT m = wt ? (PT)wt[idx] : PT(1);
+      // from the left cell: this is its high face, vsign = -1
+      if (ml == MAT_FLUID) acc += -(mr == MAT_SOLID ? PT(0.5) : PT(1)) * m * lam[cl];
+      else if (ml == MAT_SOLID && mr == MAT_FLUID) acc += -PT(0.5) * m * lam[cl];
+      // from the right cell: its low face, vsign = +1
+      if (mr == MAT_FLUID) acc += (ml == MAT_SOLID ? PT(0.5) : PT(1)) * m * lam[cr];
+      else if (mr == MAT_SOLID && ml == MAT_FLUID) acc += PT(0.5) * m * lam[cr];
+    }
+    out[idx] = (FT)((PT)g[idx] - acc);
+  }
+}
+template <typename FT, typename PT>
+cudaError_t rhs_T(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww, const PT* lam,
+                  const Line* lines, int ni, int nj, int nk, const FT* gu, const FT* gv,
+                  const FT* gw, FT* du, FT* dv, FT* dw, cudaStream_t st) {
+  (void)lines;
+  for (int axis = 0; axis < 3; ++axis) {
+    size_t n = (size_t)(ni + (axis == 0)) * (nj + (axis == 1)) * (nk + (axis == 2));
+    unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32);
+    rhs_T_kernel<FT, PT><<<blocks, 256, 0, st>>>(mat, axis == 0 ? wu : axis == 1 ? wv : ww, lam, ni, nj, nk,
+                                                axis, axis == 0 ? gu : axis == 1 ? gv : gw,
+                                                axis == 0 ? du : axis == 1 ? dv : dw);
+  }
+  return cudaGetLastError();
+}
+template cudaError_t rhs_T<double, double>(const uint8_t*, const double*, const double*, const double*,
+                                           const double*, const Line*, int, int, int, const double*,
+                                           const double*, const double*, double*, double*, double*,
+                                           cudaStream_t);
+template cudaError_t rhs_T<float, float>(const uint8_t*, const float*, const float*, const float*,
+                                         const float*, const Line*, int, int, int, const float*,
+                                         const float*, const float*, float*, float*, float*,
+                                         cudaStream_t);
+template cudaError_t rhs_T<float, double>(const uint8_t*, const float*, const float*, const float*,
+                                          const double*, const Line*, int, int, int, const float*,
+                                          const float*, const float*, float*, float*, float*,
+                                          cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Block reduction helpers.  Every reduction is deterministic: fixed per-thread
+// order, fixed tree, per-block partials summed in block order by the last
+// block (last-block-done counter in PcgScalars::red_count).
+// ---------------------------------------------------------------------------
+template <typename DT>
+__device__ __forceinline__ DT block_sum(DT v, DT* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = add_rn(v, __shfl_xor_sync(XFP_FULL, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  DT t = DT(0);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t = add_rn(t, sh[q]);
+  __syncthreads();
+  return t;  // valid in thread 0
+}
+__device__ __forceinline__ double block_max(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(XFP_FULL, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t = fmax(t, sh[q]);
+  __syncthreads();
+  return t;
+}
+// Returns true in thread 0 of the last block to finish.
+__device__ __forceinline__ bool last_block(PcgScalars* sc) {
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned t = atomicAdd(&sc->red_count, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  return s_last;
+}
+
+// ---------------------------------------------------------------------------
+// z = A s (7-point, row order of sparse_matrix.h:264-276: columns c-nn, c-ni,
+// c-1, c, c+1, c+ni, c+nn; absent entries skipped) fused with the partial dot
+// s.z.  mode 0: alpha = rho / (s.z) (pcg_solver.h:269); mode 1: no dot.
+// One warp per x-line; the warp's lanes walk the line span.
+// ---------------------------------------------------------------------------
+template <typename VT, typename AT, typename DT>
+__global__ void __launch_bounds__(256) spmv_dot_kernel(
+    const AT* __restrict__ diag, const AT* __restrict__ ax, const AT* __restrict__ ay,
+    const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
+    const Line* __restrict__ lines, int ni, int nj, int nk, PcgScalars* sc,
+    DT* __restrict__ partials, int mode) {
+  __shared__ DT sh[32];
+  if (sc && *(volatile int*)&sc->done) return;
+  const int lane = threadIdx.x & 31;
+  const long long nlines = (long long)nj * nk;
+  DT acc = DT(0);
+  for (long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
+       line += (long long)gridDim.x * (blockDim.x >> 5)) {
+    const Line L = lines[line];
+    if (L.len == 0) continue;
+    const int j = (int)(line % nj), k = (int)(line / nj);
+    Line Lym = {0, 0, 0, 0}, Lyp = {0, 0, 0, 0}, Lzm = {0, 0, 0, 0}, Lzp = {0, 0, 0, 0};
+    if (j > 0) Lym = lines[line - 1];
+    if (j + 1 < nj) Lyp = lines[line + 1];
+    if (k > 0) Lzm = lines[line - nj];
+    if (k + 1 < nk) Lzp = lines[line + nj];
+    for (int q = lane; q < L.len; q += 32) {
+      const int i = L.lo + q;
+      const size_t c = (size_t)L.off + q;
+      VT acc_z = VT(0);
+      const VT dz = (VT)az[c], dy = (VT)ay[c], dx = (VT)ax[c], dd = (VT)diag[c];
+      if (dz != VT(0)) acc_z = add_rn(acc_z, mul_rn(dz, s[(size_t)Lzm.off + (i - Lzm.lo)]));
+      if (dy != VT(0)) acc_z = add_rn(acc_z, mul_rn(dy, s[(size_t)Lym.off + (i - Lym.lo)]));
+      if (dx != VT(0)) acc_z = add_rn(acc_z, mul_rn(dx, s[c - 1]));
+      const VT sc_ = s[c];
+      if (dd != VT(0)) acc_z = add_rn(acc_z, mul_rn(dd, sc_));
+      if (q + 1 < L.len) {
+        const VT cx = (VT)ax[c + 1];
+        if (cx != VT(0)) acc_z = add_rn(acc_z, mul_rn(cx, s[c + 1]));
+      }
+      if ((unsigned)(i - Lyp.lo) < (unsigned)Lyp.len) {
+        const size_t n = (size_t)Lyp.off + (i - Lyp.lo);
+        const VT cy = (VT)ay[n];
+        if (cy != VT(0)) acc_z = add_rn(acc_z, mul_rn(cy, s[n]));
+      }
+      if ((unsigned)(i - Lzp.lo) < (unsigned)Lzp.len) {
+        const size_t n = (size_t)Lzp.off + (i - Lzp.lo);
+        const VT cz = (VT)az[n];
+        if (cz != VT(0)) acc_z = add_rn(acc_z, mul_rn(cz, s[n]));
+      }
+      z[c] = acc_z;
+      if (mode == 0) acc = add_rn(acc, mul_rn((DT)sc_, (DT)acc_z));
+    }
+  }
+  if (mode != 0) return;
+  DT t = block_sum(acc, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+  if (last_block(sc) && threadIdx.x == 0) {
+    DT tot = DT(0);
+    for (unsigned b = 0; b < gridDim.x; ++b) tot = add_rn(tot, ((volatile DT*)partials)[b]);
+    if (std::is_same<DT, float>::value)
+      sc->alpha = (double)__fdiv_rn((float)sc->rho, (float)tot);
+    else
+      sc->alpha = __ddiv_rn(sc->rho, (double)tot);
+    sc->red_count = 0;
+  }
+}
+template <typename VT, typename AT, typename DT>
+cudaError_t spmv_dot(const AT* diag, const AT* ax, const AT* ay, const AT* az, const VT* s, VT* z,
+                     const Line* lines, int ni, int nj, int nk, long long M, PcgScalars* sc,
+                     DT* partials, int nblk_max, int mode, cudaStream_t st) {
+  (void)M;
+  const long long nlines = (long long)nj * nk;
+  int blocks = (int)std::min<long long>((nlines + 7) / 8, (long long)nblk_max);
+  spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(diag, ax, ay, az, s, z, lines, ni, nj, nk, sc,
+                                                     partials, mode);
+  return cudaGetLastError();
+}
+template cudaError_t spmv_dot<double, double, double>(const double*, const double*, const double*,
+                                                      const double*, const double*, double*,
+                                                      const Line*, int, int, int, long long,
+                                                      PcgScalars*, double*, int, int, cudaStream_t);
+template cudaError_t spmv_dot<float, float, float>(const float*, const float*, const float*,
+                                                   const float*, const float*, float*, const Line*,
+                                                   int, int, int, long long, PcgScalars*, float*,
+                                                   int, int, cudaStream_t);
+template cudaError_t spmv_dot<float, float, double>(const float*, const float*, const float*,
+                                                    const float*, const float*, float*, const Line*,
+                                                    int, int, int, long long, PcgScalars*, double*,
+                                                    int, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// x += alpha s ; r += (-alpha) z ; |r|_inf  (pcg_solver.h:270-276).  The last
+// block decides convergence: |r|_inf <= tol*|b|_inf, or the iteration cap.
+// ---------------------------------------------------------------------------
+template <typename VT>
+__global__ void __launch_bounds__(256) update_xr_kernel(VT* __restrict__ x, VT* __restrict__ r,
+                                                        const VT* __restrict__ s,
+                                                        const VT* __restrict__ z, long long M,
+                                                        PcgScalars* sc, double* __restrict__ partials) {
+  __shared__ double sh[32];
+  if (*(volatile int*)&sc->done) return;
+  const VT alpha = (VT)sc->alpha;
+  const VT nalpha = -alpha;
+  double m = 0.0;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x) {
+    x[c] = add_rn(x[c], mul_rn(alpha, s[c]));
+    const VT rv = add_rn(r[c], mul_rn(nalpha, z[c]));
+    r[c] = rv;
+    m = fmax(m, (double)fabs(rv));
+  }
+  double t = block_max(m, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+  if (last_block(sc) && threadIdx.x == 0) {
+    double tot = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) tot = fmax(tot, ((volatile double*)partials)[b]);
+    sc->res = tot;
+    sc->iters += 1;
+    if (tot <= sc->tolabs) {
+      sc->done = 1;
+      sc->status = 0;
+    } else if (sc->iters >= sc->maxit) {
+      sc->done = 1;
+      sc->status = 1;
+    }
+    sc->red_count = 0;
+  }
+}
+template <typename VT, typename DT>
+cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgScalars* sc,
+                      double* partials, int nblk_max, cudaStream_t st) {
+  int blocks = (int)std::min<long long>((M + 255) / 256, (long long)nblk_max);
+  if (blocks < 1) blocks = 1;
+  update_xr_kernel<VT><<<blocks, 256, 0, st>>>(x, r, s, z, M, sc, partials);
+  return cudaGetLastError();
+}
+template cudaError_t update_xr<double, double>(double*, double*, const double*, const double*, long long,
+                                               PcgScalars*, double*, int, cudaStream_t);
+template cudaError_t update_xr<float, float>(float*, float*, const float*, const float*, long long,
+                                             PcgScalars*, double*, int, cudaStream_t);
+template cudaError_t update_xr<float, double>(float*, float*, const float*, const float*, long long,
+                                              PcgScalars*, double*, int, cudaStream_t);
+
+// s = z + beta s  (add_scaled(beta, s, z) then swap, pcg_solver.h:280)
+template <typename VT>
+__global__ void update_s_kernel(VT* __restrict__ s, const VT* __restrict__ z, long long M,
+                                PcgScalars* sc) {
+  if (*(volatile int*)&sc->done) return;
+  const VT beta = (VT)sc->beta;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x)
+    s[c] = add_rn(z[c], mul_rn(beta, s[c]));
+}
+template <typename VT>
+cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st) {
+  int blocks = (int)std::min<long long>((M + 255) / 256, 148LL * 16);
+  if (blocks < 1) blocks = 1;
+  update_s_kernel<VT><<<blocks, 256, 0, st>>>(s, z, M, sc);
+  return cudaGetLastError();
+}
+template cudaError_t update_s<double>(double*, const double*, long long, PcgScalars*, cudaStream_t);
+template cudaError_t update_s<float>(float*, const float*, long long, PcgScalars*, cudaStream_t);
+
+// |b|_inf, tolerance and loop state at the start of a solve (pcg_solver.h:247-254).
+template <typename VT>
+__global__ void absmax_init_kernel(const VT* __restrict__ b, long long M, PcgScalars* sc,
+                                   double* __restrict__ partials, double tol, int maxit) {
+  __shared__ double sh[32];
+  double m = 0.0;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, (double)fabs(b[c]));
+  double t = block_max(m, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+  if (last_block(sc) && threadIdx.x == 0) {
+    double tot = 0.0;
+    for (unsigned q = 0; q < gridDim.x; ++q) tot = fmax(tot, ((volatile double*)partials)[q]);
+    sc->bnorm = tot;
+    sc->res = tot;
+    sc->tolabs = tol * tot;
+    sc->iters = 0;
+    sc->maxit = maxit;
+    sc->status = 0;
+    sc->done = (tot == 0.0 || maxit <= 0) ? 1 : 0;
+    if (tot != 0.0 && maxit <= 0) sc->status = 1;
+    sc->red_count = 0;
+  }
+}
+template <typename VT>
+cudaError_t absmax_init(const VT* b, long long M, PcgScalars* sc, double* partials, int nblk_max,
+                        double tol, int maxit, cudaStream_t st) {
+  int blocks = (int)std::min<long long>((M + 255) / 256, (long long)nblk_max);
+  if (blocks < 1) blocks = 1;
+  absmax_init_kernel<VT><<<blocks, 256, 0, st>>>(b, M, sc, partials, tol, maxit);
+  return cudaGetLastError();
+}
+template cudaError_t absmax_init<double>(const double*, long long, PcgScalars*, double*, int, double, int,
+                                         cudaStream_t);
+template cudaError_t absmax_init<float>(const float*, long long, PcgScalars*, double*, int, double, int,
+                                        cudaStream_t);
+
+template <typename A, typename B>
+__global__ void convert_kernel(const A* __restrict__ in, B* __restrict__ out, long long n) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+    out[c] = (B)in[c];
+}
+template <typename A, typename B>
+cudaError_t convert(const A* in, B* out, long long n, cudaStream_t st) {
+  int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+  if (blocks < 1) blocks = 1;
+  convert_kernel<A, B><<<blocks, 256, 0, st>>>(in, out, n);
+  return cudaGetLastError();
+}
+template cudaError_t convert<double, float>(const double*, float*, long long, cudaStream_t);
+template cudaError_t convert<float, double>(const float*, double*, long long, cudaStream_t);
+
+template <typename T>
+cudaError_t copy_vec(const T* in, T* out, long long n, cudaStream_t st) {
+  return cudaMemcpyAsync(out, in, n * sizeof(T), cudaMemcpyDeviceToDevice, st);
+}
+template cudaError_t copy_vec<double>(const double*, double*, long long, cudaStream_t);
+template cudaError_t copy_vec<float>(const float*, float*, long long, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Mixed precision: FP64 residual r = b - A x with |r|_inf (into sc->res), on
+// the FP64 copy of A; and x64 += e32 after each FP32 inner solve.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) residual64_kernel(
+    const double* __restrict__ diag, const double* __restrict__ ax, const double* __restrict__ ay,
+    const double* __restrict__ az, const double* __restrict__ b, const double* __restrict__ x,
+    double* __restrict__ r, const Line* __restrict__ lines, int ni, int nj, int nk, PcgScalars* sc,
+    double* __restrict__ partials) {
+  __shared__ double sh[32];
+  const int lane = threadIdx.x & 31;
+  const long long nlines = (long long)nj * nk;
+  double m = 0.0;
+  for (long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
+       line += (long long)gridDim.x * (blockDim.x >> 5)) {
+    const Line L = lines[line];
+    if (L.len == 0) continue;
+    const int j = (int)(line % nj), k = (int)(line / nj);
+    Line Lym = {0, 0, 0, 0}, Lyp = {0, 0, 0, 0}, Lzm = {0, 0, 0, 0}, Lzp = {0, 0, 0, 0};
+    if (j > 0) Lym = lines[line - 1];
+    if (j + 1 < nj) Lyp = lines[line + 1];
+    if (k > 0) Lzm = lines[line - nj];
+    if (k + 1 < nk) Lzp = lines[line + nj];
+    for (int q = lane; q < L.len; q += 32) {
+      const int i = L.lo + q;
+      const size_t c = (size_t)L.off + q;
+      double a = 0.0;
+      if (az[c] != 0.0) a += az[c] * x[(size_t)Lzm.off + (i - Lzm.lo)];
+      if (ay[c] != 0.0) a += ay[c] * x[(size_t)Lym.off + (i - Lym.lo)];
+      if (ax[c] != 0.0) a += ax[c] * x[c - 1];
+      a += diag[c] * x[c];
+      if (q + 1 < L.len && ax[c + 1] != 0.0) a += ax[c + 1] * x[c + 1];
+      if ((unsigned)(i - Lyp.lo) < (unsigned)Lyp.len) {
+        const size_t n = (size_t)Lyp.off + (i - Lyp.lo);
+        if (ay[n] != 0.0) a += ay[n] * x[n];
+      }
+      if ((unsigned)(i - Lzp.lo) < (unsigned)Lzp.len) {
+        const size_t n = (size_t)Lzp.off + (i - Lzp.lo);
+        if (az[n] != 0.0) a += az[n] * x[n];
+      }
+      const double rv = b[c] - a;
+      r[c] = rv;
+      m = fmax(m, fabs(rv));
+    }
+  }
+  double t = block_max(m, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+  if (last_block(sc) && threadIdx.x == 0) {
+    double tot = 0.0;
+    for (unsigned q = 0; q < gridDim.x; ++q) tot = fmax(tot, ((volatile double*)partials)[q]);
+    sc->res = tot;
+    sc->red_count = 0;
+  }
+}
+cudaError_t residual64(const double* diag, const double* ax, const double* ay, const double* az,
+                       const double* b, const double* x, double* r, const Line* lines, int ni,
+                       int nj, int nk, long long M, PcgScalars* sc, double* partials,
+                       int nblk_max, cudaStream_t st) {
+  (void)M;
+  const long long nlines = (long long)nj * nk;
+  int blocks = (int)std::min<long long>((nlines + 7) / 8, (long long)nblk_max);
+  residual64_kernel<<<blocks, 256, 0, st>>>(diag, ax, ay, az, b, x, r, lines, ni, nj, nk, sc, partials);
+  return cudaGetLastError();
+}
+
+__global__ void refine_update_kernel(double* __restrict__ x64, const float* __restrict__ e32, long long M) {
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x)
+    x64[c] += (double)e32[c];
+}
+cudaError_t refine_update(double* x64, const float* e32, long long M, cudaStream_t st) {
+  int blocks = (int)std::min<long long>((M + 255) / 256, 148LL * 16);
+  if (blocks < 1) blocks = 1;
+  refine_update_kernel<<<blocks, 256, 0, st>>>(x64, e32, M);
+  return cudaGetLastError();
+}
+
+}  // namespace xfp
