@@ -154,6 +154,7 @@ int xfp_project_backward_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t
  *                    ax[c]=A(c,c-1), ay[c]=A(c,c-ni), az[c]=A(c,c-ni*nj)
  *   inv/lx/ly/lz     factor_modified_incomplete_cholesky0 (pcg_solver.h:85-186);
  *                    lx[c]=L(c,c-1) etc.
+ *   y = L^{-1} r     solve_lower (pcg_solver.h:192-204)
  *   z = M^{-1} r     solve_lower + solve_lower_transpose_in_place (pcg_solver.h:192-220)
  *   q = A r          multiply(FixedSparseMatrix) (sparse_matrix.h:264-276)
  * r is a dense input (rows without an unknown are ignored). */
@@ -162,7 +163,7 @@ int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* materi
                      const double* wu, const double* wv, const double* ww,
                      const double* r, double* diag, double* ax, double* ay, double* az,
                      double* b, double* inv, double* lx, double* ly, double* lz,
-                     double* z, double* q);
+                     double* y, double* z, double* q);
 
 #ifdef __cplusplus
 }

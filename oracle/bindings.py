@@ -81,6 +81,8 @@ class Oracle(_Lib):
         L.xo_spmv.argtypes = [C.c_int] * 3 + [_dp] * 6
         L.xo_factor.argtypes = [C.c_int] * 3 + [_dp] * 4 + [C.c_double] * 2 + [_dp] * 4
         L.xo_precond.argtypes = [C.c_int] * 3 + [_dp] * 6
+        L.xo_forward.argtypes = [C.c_int] * 3 + [_dp] * 6
+        L.xo_backward.argtypes = [C.c_int] * 3 + [_dp] * 6
         L.xo_pcg.argtypes = ([C.c_int] * 3 + [_dp] * 5 + [C.c_double, C.c_int, C.c_double, C.c_double,
                              _dp, C.POINTER(C.c_int), _dp])
         L.xo_pcg.restype = C.c_int
@@ -120,6 +122,18 @@ class Oracle(_Lib):
         z = np.zeros_like(F["inv"])
         self.lib.xo_precond(*self._dims(sc), _p(F["inv"]), _p(F["lx"]), _p(F["ly"]), _p(F["lz"]),
                             _p(_f64(r)), _p(z))
+        return z
+
+    def forward(self, sc, F, r):
+        y = np.zeros_like(F["inv"])
+        self.lib.xo_forward(*self._dims(sc), _p(F["inv"]), _p(F["lx"]), _p(F["ly"]), _p(F["lz"]),
+                            _p(_f64(r)), _p(y))
+        return y
+
+    def backward(self, sc, F, y):
+        z = np.zeros_like(F["inv"])
+        self.lib.xo_backward(*self._dims(sc), _p(F["inv"]), _p(F["lx"]), _p(F["ly"]), _p(F["lz"]),
+                             _p(_f64(y)), _p(z))
         return z
 
     def pcg(self, sc, A, tol=1e-6, maxit=200, omega=0.97, ratio=0.25):

@@ -251,6 +251,32 @@ void xo_precond(int ni, int nj, int nk, const double* inv, const double* lx,
   } while (c != 0);
 }
 
+/* The two halves of xo_precond separately: y = L^{-1} r, z = L^{-T} y. */
+void xo_forward(int ni, int nj, int nk, const double* inv, const double* lx,
+                const double* ly, const double* lz, const double* r, double* y) {
+  grid_t g = mkgrid(ni, nj, nk);
+  memcpy(y, r, g.n * sizeof(double));
+  for (size_t c = 0; c < g.n; ++c) {
+    y[c] *= inv[c];
+    if (c + 1 < g.n && lx[c + 1] != 0.0) y[c + 1] -= lx[c + 1] * y[c];
+    if (c + ni < g.n && ly[c + ni] != 0.0) y[c + ni] -= ly[c + ni] * y[c];
+    if (c + g.nn < g.n && lz[c + g.nn] != 0.0) y[c + g.nn] -= lz[c + g.nn] * y[c];
+  }
+}
+void xo_backward(int ni, int nj, int nk, const double* inv, const double* lx,
+                 const double* ly, const double* lz, const double* y, double* z) {
+  grid_t g = mkgrid(ni, nj, nk);
+  memcpy(z, y, g.n * sizeof(double));
+  size_t c = g.n;
+  do {
+    --c;
+    if (c + 1 < g.n && lx[c + 1] != 0.0) z[c] -= lx[c + 1] * z[c + 1];
+    if (c + ni < g.n && ly[c + ni] != 0.0) z[c] -= ly[c + ni] * z[c + ni];
+    if (c + g.nn < g.n && lz[c + g.nn] != 0.0) z[c] -= lz[c + g.nn] * z[c + g.nn];
+    z[c] *= inv[c];
+  } while (c != 0);
+}
+
 /* BLAS::dot / abs_max / add_scaled (blas_wrapper.h:12-51): sequential loops. */
 static double dot(size_t n, const double* x, const double* y) {
   double s = 0;

@@ -18,6 +18,9 @@ def load(name):
 
 
 def bits_equal(a, b):
-    a = np.ascontiguousarray(a, dtype=np.float64)
-    b = np.ascontiguousarray(b, dtype=np.float64)
+    """Bit-identical FP64 arrays, except that -0.0 and +0.0 compare equal (the
+    reference keeps the sign of zero in rows without an unknown; the GPU
+    output grid holds +0.0 there)."""
+    a = np.ascontiguousarray(a, dtype=np.float64) + 0.0
+    b = np.ascontiguousarray(b, dtype=np.float64) + 0.0
     return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))

@@ -27,7 +27,7 @@ def make_ctx(precision="f64", **kw):
 def debug_stages(ctx, sc, r=None, fractional=False):
     """Dense internal stages (assembly, factor, M^-1 r, A r) from the GPU."""
     shp = (sc.nk, sc.nj, sc.ni)
-    names = ("diag", "ax", "ay", "az", "b", "inv", "lx", "ly", "lz", "z", "q")
+    names = ("diag", "ax", "ay", "az", "b", "inv", "lx", "ly", "lz", "y", "z", "q")
     out = {k: np.zeros(shp) for k in names}
     w = (sc.wu, sc.wv, sc.ww) if fractional else (None, None, None)
     args = [ptr(np.ascontiguousarray(sc.mat, np.uint8)), *(ptr(f64(a)) for a in (sc.u, sc.v, sc.w)),
@@ -81,6 +81,9 @@ def rel_l2(a, b):
 
 
 def bits_equal(a, b):
-    a = np.ascontiguousarray(a, dtype=np.float64)
-    b = np.ascontiguousarray(b, dtype=np.float64)
+    """Bit-identical FP64 arrays, except that -0.0 and +0.0 compare equal (the
+    reference keeps the sign of zero in rows without an unknown; the GPU
+    output grid holds +0.0 there)."""
+    a = np.ascontiguousarray(a, dtype=np.float64) + 0.0
+    b = np.ascontiguousarray(b, dtype=np.float64) + 0.0
     return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))

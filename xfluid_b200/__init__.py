@@ -4,14 +4,12 @@ natural order and the pressure-gradient update -- behind xFluid's solver
 interface.  The compute path is libxfp.so (include/xfp.h); see solver.py for
 the Python mirror of VariationalPressureSolver.
 """
+import importlib
+
 __all__ = ["VariationalPressureSolver", "project_scene", "scenes"]
 
 
 def __getattr__(name):
     if name in ("VariationalPressureSolver", "project_scene"):
-        from . import solver
-        return getattr(solver, name)
-    if name == "scenes":
-        from . import scenes
-        return scenes
+        return getattr(importlib.import_module(__name__ + ".solver"), name)
     raise AttributeError(name)

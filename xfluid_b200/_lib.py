@@ -101,7 +101,7 @@ def load() -> C.CDLL:
     L.xfp_apply_pressure_f32.argtypes = dims + [vp] * 7
     L.xfp_project_backward_f64.argtypes = dims + [vp] * 9 + [C.POINTER(XfpStats)]
     L.xfp_project_backward_f32.argtypes = dims + [vp] * 9 + [C.POINTER(XfpStats)]
-    L.xfp_debug_stages.argtypes = dims + [vp] * 18
+    L.xfp_debug_stages.argtypes = dims + [vp] * 19
     for name in EXPORTS:
         f = getattr(L, name)
         if name not in ("xfp_default_options", "xfp_last_error", "xfp_version"):

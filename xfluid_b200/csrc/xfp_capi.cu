@@ -13,6 +13,8 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
+#include <cstdlib>
 
 #include "../../include/xfp.h"
 #include "xfp_common.cuh"
@@ -70,8 +72,8 @@ struct xfp_ctx {
   DevBuf inv64, inv32, L32[3];
   DevBuf x64, r64, x32, r32, s32, z32, s64, z64, dense;
   // control
-  DevBuf prog, ctl, scal, scal2, partials, tpartials;
-  size_t prog_cap = 0;
+  DevBuf ctl, scal, scal2, partials, tpartials, sy, sz, trace;
+  bool tracing = false;
   // sizes of the current layout
   int ni = 0, nj = 0, nk = 0, NJt = 0, NKt = 0, nw = 16;
   long long M = 0, rows = 0, nlines_act = 0, ntiles = 0;
@@ -123,7 +125,7 @@ int stage_in(xfp_ctx* ctx, DevBuf& buf, const T* src, size_t n, const T** dev) {
 int check_dims(xfp_ctx* ctx, int ni, int nj, int nk, const void* mat) {
   if (!ctx) return XFP_ERR_ARGS;
   if (ni < 1 || nj < 1 || nk < 1) return fail(ctx, XFP_ERR_ARGS, "grid sizes must be >= 1");
-  if ((long long)ni + nj + nk >= (1LL << 30) || (long long)ni * nj * nk >= (1LL << 31))
+  if ((long long)ni + nj + nk >= (1LL << 20) || (long long)ni * nj * nk >= (1LL << 31))
     return fail(ctx, XFP_ERR_ARGS, "grid too large");
   if (nj > 65535 * 32) return fail(ctx, XFP_ERR_ARGS, "nj too large");
   if (!mat) return fail(ctx, XFP_ERR_ARGS, "material is NULL");
@@ -140,12 +142,6 @@ int build_layout(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk) {
   XFP_CUDA(ctx, ctx->tile_active.ensure((size_t)NJt * NKt));
   XFP_CUDA(ctx, ctx->tiles.ensure((size_t)NJt * NKt * sizeof(int)));
   XFP_CUDA(ctx, ctx->counters.ensure(4 * sizeof(long long)));
-  size_t prog_bytes = (size_t)nk * NJt * sizeof(unsigned long long);
-  if (prog_bytes > ctx->prog_cap) {
-    XFP_CUDA(ctx, ctx->prog.ensure(prog_bytes));
-    XFP_CUDA(ctx, cudaMemsetAsync(ctx->prog.p, 0, ctx->prog.cap, ctx->stream));
-    ctx->prog_cap = ctx->prog.cap;
-  }
   LayoutDev L{ctx->lines.as<Line>(), ctx->lens.as<int>(), ctx->tile_active.as<unsigned char>(),
               ctx->tiles.as<int>(), ctx->counters.as<long long>()};
   XFP_CUDA(ctx, layout_build(dmat, ni, nj, nk, nw, L, ctx->stream));
@@ -188,6 +184,15 @@ int ensure_compact(xfp_ctx* ctx, int prec) {
   XFP_CUDA(ctx, ctx->scal2.ensure(sizeof(PcgScalars)));
   XFP_CUDA(ctx, ctx->partials.ensure(NBLK_MAX * sizeof(double)));
   XFP_CUDA(ctx, ctx->tpartials.ensure(std::max<long long>(ctx->ntiles, 1) * sizeof(double)));
+  // stamped tile-boundary words: 4 per cell; zeroed when (re)allocated so no
+  // stale word can carry a live generation
+  const size_t sbytes = M * 4 * sizeof(unsigned long long);
+  for (DevBuf* b : {&ctx->sy, &ctx->sz}) {
+    if (b->cap < sbytes || !b->p) {
+      XFP_CUDA(ctx, b->ensure(sbytes));
+      XFP_CUDA(ctx, cudaMemsetAsync(b->p, 0, b->cap, ctx->stream));
+    }
+  }
   return XFP_OK;
 }
 
@@ -200,11 +205,10 @@ SweepGrid make_grid(xfp_ctx* ctx, PcgScalars* sc, int bwd_mode) {
   g.bwd_mode = bwd_mode;
   g.lines = ctx->lines.as<Line>();
   g.tiles = ctx->tiles.as<int>();
-  g.tile_active = ctx->tile_active.as<unsigned char>();
-  g.prog = ctx->prog.as<unsigned long long>();
   g.ctl = ctx->ctl.as<SweepCtl>();
   g.spin_limit = spin_limit(ctx);
   g.scal = sc;
+  g.trace = ctx->tracing ? ctx->trace.as<int>() : nullptr;
   return g;
 }
 
@@ -222,11 +226,32 @@ int check_sweep_error(xfp_ctx* ctx) {
   SweepCtl c;
   XFP_CUDA(ctx, cudaMemcpyAsync(&c, ctx->ctl.p, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream));
   XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (c.err && ctx->tracing) {
+    std::vector<int> t(ctx->trace.cap / sizeof(int));
+    cudaMemcpy(t.data(), ctx->trace.p, ctx->trace.cap, cudaMemcpyDeviceToHost);
+    int blk = c.err_thread / ((ctx->nw + 1) * 32);
+    fprintf(stderr, "xfp trace: failing block %d, op %d, nw %d (site 0 = not waiting)\n", blk, c.err_op, ctx->nw);
+    for (int b = 0; b < 1024; ++b) {
+      bool any = false;
+      for (int w = 0; w <= ctx->nw; ++w) any |= t[((size_t)b * (ctx->nw + 1) + w) * 4] > 0;
+      if (!any && b != blk) continue;
+      fprintf(stderr, " block %d:", b);
+      for (int w = 0; w <= ctx->nw; ++w) {
+        const int* r = &t[((size_t)b * (ctx->nw + 1) + w) * 4];
+        fprintf(stderr, " w%d[site %d step %d lane %d pub %d]", w, r[0], r[1], r[3], r[2]);
+      }
+      fprintf(stderr, "\n");
+    }
+  }
   if (c.err) {
-    char buf[128];
-    snprintf(buf, sizeof buf, "device wait timed out (site %u)", c.err_where);
+    char buf[256];
+    snprintf(buf, sizeof buf,
+             "device wait timed out (site %u, op %d, tile %d, step %d, thread %d, ntiles %lld, seen %016llx, "
+             "expect %08x)",
+             c.err_where, c.err_op, c.err_tile, c.err_tau, c.err_thread, ctx->ntiles, c.err_word, c.err_expect);
     // clear so the context stays usable
-    SweepCtl z{c.gen, 0, 0, 0};
+    SweepCtl z{};
+    z.gen = c.gen;
     cudaMemcpyAsync(ctx->ctl.p, &z, sizeof(z), cudaMemcpyHostToDevice, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     return fail(ctx, XFP_ERR_TIMEOUT, buf);
@@ -243,8 +268,10 @@ int factor(xfp_ctx* ctx, const CT* const A[4], CT* const F[6], IT* inv, CT omega
   XFP_CUDA(ctx, cudaMemsetAsync(inv, 0, M * sizeof(IT), ctx->stream));
   SweepData<VT, IT, CT> d;
   d.diag = A[0]; d.ax = A[1]; d.ay = A[2]; d.az = A[3];
-  d.flx = F[0]; d.fly = F[1]; d.flz = F[2]; d.fmx = F[3]; d.fmy = F[4]; d.fmz = F[5];
+  d.flx = F[0]; d.fly = F[1]; d.flz = F[2];
   d.oinv = inv;
+  d.sy = ctx->sy.as<unsigned long long>();
+  d.sz = ctx->sz.as<unsigned long long>();
   d.omega = omega; d.ratio = ratio;
   SweepGrid g = make_grid(ctx, nullptr, 0);
   return run_sweep<VT, IT, CT>(ctx, SWEEP_FACTOR, g, d);
@@ -267,6 +294,8 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   SweepData<VT, IT, DT> d;
   d.r = r; d.y = z; d.lx = L[0]; d.ly = L[1]; d.lz = L[2]; d.inv = inv;
   d.partials = ctx->tpartials.as<double>();
+  d.sy = ctx->sy.as<unsigned long long>();
+  d.sz = ctx->sz.as<unsigned long long>();
   SweepGrid g0 = make_grid(ctx, dsc, 0), g1 = make_grid(ctx, dsc, 1);
   int rc;
   if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g0, d)) != XFP_OK) return rc;
@@ -690,7 +719,7 @@ int dump_dense(xfp_ctx* ctx, const T* compact, double* host_out) {
 // the factor (CT) and by the SpMV (VT).
 template <typename VT, typename IT, typename CT>
 int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* const F[6], IT* inv,
-               const VT* const L[3], const double* dr, double* out[11]) {
+               const VT* const L[3], const double* dr, double* out[12]) {
   int rc;
   const long long M = ctx->M;
   cudaStream_t st = ctx->stream;
@@ -718,8 +747,12 @@ int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* c
     SweepData<VT, IT, CT> d;
     d.r = r; d.y = z; d.lx = L[0]; d.ly = L[1]; d.lz = L[2]; d.inv = inv;
     d.partials = ctx->tpartials.as<double>();
+    d.sy = ctx->sy.as<unsigned long long>();
+    d.sz = ctx->sz.as<unsigned long long>();
     SweepGrid g = make_grid(ctx, nullptr, 0);
     if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_FWD, g, d))) return rc;
+    XFP_CUDA(ctx, cudaStreamSynchronize(st));
+    if ((rc = dump_dense<VT>(ctx, z, out[9]))) return rc;
     if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_BWD, g, d))) return rc;
     XFP_CUDA(ctx, (spmv_dot<VT, VT, VT>(Av[0], Av[1], Av[2], Av[3], r, qv, ctx->lines.as<Line>(), ctx->ni, ctx->nj,
                                         ctx->nk, M, nullptr, (VT*)nullptr, NBLK_MAX, 1, st)));
@@ -732,8 +765,8 @@ int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* c
   for (int q = 0; q < 3; ++q)
     if ((rc = dump_dense<CT>(ctx, F[q], out[6 + q]))) return rc;
   if (dr) {
-    if ((rc = dump_dense<VT>(ctx, z, out[9]))) return rc;
-    if ((rc = dump_dense<VT>(ctx, qv, out[10]))) return rc;
+    if ((rc = dump_dense<VT>(ctx, z, out[10]))) return rc;
+    if ((rc = dump_dense<VT>(ctx, qv, out[11]))) return rc;
   }
   return XFP_OK;
 }
@@ -803,8 +836,14 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
     ctx->own_stream = true;
   }
   for (auto& e : ctx->ev) cudaEventCreate(&e);
+  if (getenv("XFP_TRACE")) {
+    ctx->tracing = true;
+    ctx->trace.ensure(1024 * 40 * 4 * sizeof(int));
+    cudaMemset(ctx->trace.p, 0xff, ctx->trace.cap);
+  }
   if (ctx->ctl.ensure(sizeof(SweepCtl)) != cudaSuccess) { xfp_destroy(ctx); return XFP_ERR_NOMEM; }
-  SweepCtl c0{1, 0, 0, 0};
+  SweepCtl c0{};
+  c0.gen = 1;
   cudaMemcpy(ctx->ctl.p, &c0, sizeof(c0), cudaMemcpyHostToDevice);
   *out = ctx;
   return XFP_OK;
@@ -818,7 +857,7 @@ int xfp_destroy(xfp_ctx* ctx) {
                    &ctx->io_p, &ctx->io_gu, &ctx->io_gv, &ctx->io_gw, &ctx->lines, &ctx->lens,
                    &ctx->tile_active, &ctx->tiles, &ctx->counters, &ctx->inv64, &ctx->inv32, &ctx->x64,
                    &ctx->r64, &ctx->x32, &ctx->r32, &ctx->s32, &ctx->z32, &ctx->s64, &ctx->z64, &ctx->dense,
-                   &ctx->prog, &ctx->ctl, &ctx->scal, &ctx->scal2, &ctx->partials, &ctx->tpartials};
+                   &ctx->sy, &ctx->sz, &ctx->ctl, &ctx->scal, &ctx->scal2, &ctx->partials, &ctx->tpartials};
   for (DevBuf* b : all) b->release();
   for (auto& b : ctx->A64) b.release();
   for (auto& b : ctx->A32) b.release();
@@ -841,10 +880,7 @@ int xfp_set_options(xfp_ctx* ctx, const xfp_options* opt) {
   ctx->opt = *opt;
   ctx->opt.stream = keep_stream;
   int nw = opt->tile_k ? opt->tile_k : 16;
-  if (nw != ctx->nw) {
-    ctx->nw = nw;
-    ctx->prog_cap = 0;  // progress words are re-zeroed for the new tile shape
-  }
+  ctx->nw = nw;
   return XFP_OK;
 }
 
@@ -890,7 +926,7 @@ int xfp_project_backward_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t
 int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const double* u,
                      const double* v, const double* w, const double* wu, const double* wv, const double* ww,
                      const double* r, double* diag, double* ax, double* ay, double* az, double* b, double* inv,
-                     double* lx, double* ly, double* lz, double* z, double* q) {
+                     double* lx, double* ly, double* lz, double* y, double* z, double* q) {
   int rc = check_dims(ctx, ni, nj, nk, material);
   if (rc) return rc;
   if (!u || !v || !w) return fail(ctx, XFP_ERR_ARGS, "velocity arrays must not be NULL");
@@ -913,7 +949,7 @@ int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* materi
     XFP_CUDA(ctx, ctx->z64.ensure((ctx->M + 8) * 8));
   }
   const Line* lines = ctx->lines.as<Line>();
-  double* out[11] = {diag, ax, ay, az, b, inv, lx, ly, lz, z, q};
+  double* out[12] = {diag, ax, ay, az, b, inv, lx, ly, lz, y, z, q};
   cudaStream_t st = ctx->stream;
   if (prec == XFP_PREC_F64) {
     double* A[5];

@@ -28,10 +28,13 @@ struct __align__(16) Line {
 
 // Control block of the persistent sweep kernels (one per context).
 struct SweepCtl {
-  unsigned int gen;        // launch generation; progress words carry it in their high half
+  unsigned int gen;        // launch generation; stamped words carry it in their high half
   unsigned int finished;   // CTAs finished in the current launch
   unsigned int err;        // nonzero: a bounded wait ran out (XFP_ERR_TIMEOUT)
-  unsigned int err_where;  // which wait (for diagnostics)
+  unsigned int err_where;  // which wait ran out first (diagnostics)
+  int err_tile, err_tau, err_thread, err_op;
+  unsigned long long err_word;   // the word the failed wait last saw
+  unsigned int err_expect, err_pad;
 };
 
 // Scalars of one PCG solve, resident on the device.

@@ -16,11 +16,10 @@ struct SweepGrid {
   int bwd_mode;                 // backward: 0 = initial rho, 1 = beta update
   const Line* lines;            // [nk*nj]
   const int* tiles;             // active tiles, topological order, J | K<<16
-  const unsigned char* tile_active;  // [NKt*NJt]
-  unsigned long long* prog;     // [nk*NJt] progress words
   SweepCtl* ctl;
   long long spin_limit;
   PcgScalars* scal;             // forward/backward: skip when done; backward: rho/beta
+  int* trace;                   // optional: per (block, warp) {site, step, progress, tile} while waiting
 };
 
 // Arrays of one sweep.  VT: vector/L type of the solves, IT: invdiag type,
@@ -37,15 +36,16 @@ struct SweepData {
   const CT* ax = nullptr;
   const CT* ay = nullptr;
   const CT* az = nullptr;
-  CT* flx = nullptr;            // factor outputs keyed by the higher cell: L and
-  CT* fly = nullptr;            // the dropped-fill sum ("missing") for that row
+  CT* flx = nullptr;            // factor outputs: L keyed by the higher cell,
+  CT* fly = nullptr;            // lx[c] = L(c,c-1), ly[c] = L(c,c-ni), lz[c] = L(c,c-nn)
   CT* flz = nullptr;
-  CT* fmx = nullptr;
-  CT* fmy = nullptr;
-  CT* fmz = nullptr;
   IT* oinv = nullptr;
   CT omega = CT(0.97), ratio = CT(0.25);
   double* partials = nullptr;   // backward: one dot partial per tile
+  // Tile-boundary values published for neighbouring tiles: per cell up to 4
+  // 64-bit words (32-bit payload chunk | launch generation << 32).
+  unsigned long long* sy = nullptr;  // to the j-neighbour tile
+  unsigned long long* sz = nullptr;  // to the k-neighbour tile
 };
 
 #define XFP_SWEEP_DECL(VT, IT, CT)                                                             \

@@ -13,23 +13,30 @@
 //
 // Work decomposition.  A thread owns one x-line (j,k) and walks it in i.  A
 // warp holds 32 consecutive j at one k; a CTA ("tile") holds NW warps, i.e. a
-// 32 x NW block of lines.  Cell (i,j,k) is processed at wavefront time
+// 32 x NW block of lines.  Cell (i,j,k) is processed at wavefront step
 // tau = i+j+k (forward; mirrored for the backward sweep), so at each step
-//   x-neighbour  = the same lane's previous step        (register)
-//   y-neighbour  = the neighbouring lane's previous step  (warp shuffle)
-//   z-neighbour  = the neighbouring warp's previous step  (shared-memory ring,
-//                  per-warp progress counters in shared memory)
-// Lines of neighbouring tiles arrive through a loader warp per CTA that waits
-// on the producing tile's published progress (global memory, release/acquire,
-// generation-tagged) and stages the boundary values into shared-memory rings.
-// Warps never wait on a global barrier: each waits only on the producers its
-// cells actually depend on, so independent regions run concurrently.
+//   x-neighbour  = the same lane's previous step          (register)
+//   y-neighbour  = the neighbouring lane's previous step   (warp shuffle)
+//   z-neighbour  = the neighbouring warp's previous step   (shared-memory ring)
+// Values of neighbouring tiles come through a loader warp per CTA.
 //
-// Tiles are visited in a topological order (J+K ascending) and assigned
-// round-robin to a grid that is fully co-resident (cooperative launch), so a
-// CTA only ever waits on tiles that earlier CTAs hold: no deadlock.  Every
-// wait is bounded (spin_limit polls); on expiry the kernel records an error in
-// SweepCtl::err, all CTAs drain and the host reports XFP_ERR_TIMEOUT.
+// Hand-off without fences.  Every exchanged value travels inside 64-bit words
+// that also carry a stamp (the step, or the launch generation): a consumer
+// polls the data word itself until the stamp it expects appears.  An aligned
+// 64-bit access is single-copy atomic, so no flag/fence pair is needed on the
+// per-step path; payloads wider than 32 bits are split into stamped 32-bit
+// halves.  Tile boundaries are published the same way in global memory
+// (stamped with the launch generation) by the boundary lanes/warps, and the
+// loader warp of the consuming tile polls them.  Ring back-pressure uses
+// progress counters that consumers publish every few steps, after a warp
+// barrier, so every lane has used (in registers) every ring value it read
+// before the counter moves; warps issue in order, so those reads are complete.
+//
+// Tiles are visited in topological order (J+K ascending) and assigned
+// round-robin to a fully co-resident grid (cooperative launch), so a CTA only
+// waits on tiles earlier CTAs hold.  Every wait is bounded (spin_limit polls);
+// on expiry the kernel records SweepCtl::err, all waits drain quickly and the
+// host reports XFP_ERR_TIMEOUT.
 #include <climits>
 #include <type_traits>
 
@@ -38,96 +45,195 @@
 
 namespace xfp {
 
-constexpr int RING = 16;    // intra-CTA ring depth in wavefront steps
-constexpr int LRING = 64;   // loader ring depth
-constexpr int PUB = 8;      // publish global progress every PUB steps
+// Consumers publish ring progress every QPUB steps.  Deadlock freedom needs
+// RING > QPUB (a producer waits for the consumer to publish the step that
+// frees its slot) and LRING >= LB + QPUB - 1 (same for the loader batch).
+constexpr int QPUB = 4;  // (RING >= 8 for every payload)
 constexpr int INF_T = INT_MAX;
 
 template <typename T>
 struct Pair {
   T a, b;
 };
-template <typename T>
-__device__ __forceinline__ Pair<T> shfl_up(Pair<T> v, int d) {
-  return {__shfl_up_sync(XFP_FULL, v.a, d), __shfl_up_sync(XFP_FULL, v.b, d)};
-}
-template <typename T>
-__device__ __forceinline__ Pair<T> shfl_down(Pair<T> v, int d) {
-  return {__shfl_down_sync(XFP_FULL, v.a, d), __shfl_down_sync(XFP_FULL, v.b, d)};
-}
 
-template <int OP, typename VT, typename IT, typename CT>
-struct OpTraits {
-  // ring element: what a producer sends to one consumer direction
-  using R = typename std::conditional<OP == SWEEP_FACTOR, Pair<CT>, VT>::type;
+// ---- payload <-> 32-bit words ----
+template <typename T>
+struct Words {
+  static constexpr int P = sizeof(T) / 4;
 };
-
-__device__ __forceinline__ unsigned long long prog_word(unsigned gen, unsigned v) {
-  return ((unsigned long long)gen << 32) | v;
+template <typename T>
+__device__ __forceinline__ void to_words(const T& v, uint32_t* w) {
+  union {
+    T v;
+    uint32_t w[sizeof(T) / 4];
+  } u;
+  u.v = v;
+#pragma unroll
+  for (int p = 0; p < (int)(sizeof(T) / 4); ++p) w[p] = u.w[p];
 }
-// Completed-steps value of a progress word for generation gen (0 if stale).
-__device__ __forceinline__ unsigned prog_value(unsigned long long w, unsigned gen) {
-  return (unsigned)(w >> 32) == gen ? (unsigned)w : 0u;
+template <typename T>
+__device__ __forceinline__ T from_words(const uint32_t* w) {
+  union {
+    T v;
+    uint32_t w[sizeof(T) / 4];
+  } u;
+#pragma unroll
+  for (int p = 0; p < (int)(sizeof(T) / 4); ++p) u.w[p] = w[p];
+  return u.v;
+}
+template <typename T>
+__device__ __forceinline__ T shfl_up_any(const T& v) {
+  uint32_t w[sizeof(T) / 4];
+  to_words(v, w);
+#pragma unroll
+  for (int p = 0; p < (int)(sizeof(T) / 4); ++p) w[p] = __shfl_up_sync(XFP_FULL, w[p], 1);
+  return from_words<T>(w);
+}
+template <typename T>
+__device__ __forceinline__ T shfl_down_any(const T& v) {
+  uint32_t w[sizeof(T) / 4];
+  to_words(v, w);
+#pragma unroll
+  for (int p = 0; p < (int)(sizeof(T) / 4); ++p) w[p] = __shfl_down_sync(XFP_FULL, w[p], 1);
+  return from_words<T>(w);
+}
+
+__device__ __forceinline__ unsigned long long stamped(uint32_t stamp, uint32_t word) {
+  return ((unsigned long long)stamp << 32) | word;
+}
+__device__ __forceinline__ unsigned long long ld_vol64(const unsigned long long* p) {
+  return *(const volatile unsigned long long*)p;
+}
+__device__ __forceinline__ void st_vol64(unsigned long long* p, unsigned long long v) {
+  *(volatile unsigned long long*)p = v;
+}
+__device__ __forceinline__ unsigned long long ld_gpu64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void st_gpu64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v));
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
 struct Spin {
   long long n = 0;
   __device__ __forceinline__ bool step(const SweepCtl* ctl, long long limit) {
     ++n;
-    if (n > 64) __nanosleep(n > 4096 ? 256 : 32);
-    if ((n & 63) == 0 && ld_volatile_u32(&ctl->err)) return false;
+    if (n > 256) __nanosleep(n > 8192 ? 256 : 20);
+    if ((n & 255) == 0 && ld_volatile_u32(&ctl->err)) return false;
     return n < limit;
   }
 };
 
-__device__ __forceinline__ void raise_timeout(SweepCtl* ctl, unsigned where) {
-  atomicOr(&ctl->err, 1u);
-  atomicMax(&ctl->err_where, where);
+// Records the first wait that ran out (site, tile, step, thread) and raises
+// the error flag every other wait checks.
+__device__ __forceinline__ void raise_timeout(SweepCtl* ctl, unsigned where, int tile = -1, int tau = -1,
+                                              int op = -1, unsigned long long seen = 0, unsigned expect = 0) {
+  if (atomicCAS(&ctl->err, 0u, 1u) == 0u) {
+    ctl->err_word = seen;
+    ctl->err_expect = expect;
+    ctl->err_where = where;
+    ctl->err_tile = tile;
+    ctl->err_tau = tau;
+    ctl->err_thread = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    ctl->err_op = op;
+  }
+}
+
+// Poll a stamped shared-memory payload until every word carries `stamp`.
+__device__ __forceinline__ void trace_wait(const SweepGrid& g, int site, int step) {
+  if (g.trace && !ld_volatile_u32(&g.ctl->err)) {
+    int* t = g.trace + ((size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 4;
+    *(volatile int*)&t[0] = site;
+    *(volatile int*)&t[1] = step;
+    *(volatile int*)&t[3] = (int)(threadIdx.x & 31);
+  }
+}
+template <typename T>
+__device__ __forceinline__ T poll_smem(const unsigned long long* base, int stride, uint32_t stamp,
+                                       const SweepGrid& g, unsigned where) {
+  constexpr int P = Words<T>::P;
+  uint32_t w[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    unsigned long long v = ld_vol64(base + (size_t)p * stride);
+    if ((uint32_t)(v >> 32) != stamp) {
+      trace_wait(g, (int)where, (int)(stamp & 0xfffff));
+      Spin sp;
+      do {
+        if (!sp.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, where, -1, (int)(stamp & 0xfffff), -1, v, stamp); break; }
+        v = ld_vol64(base + (size_t)p * stride);
+      } while ((uint32_t)(v >> 32) != stamp);
+      trace_wait(g, 0, (int)(stamp & 0xfffff));
+    }
+    w[p] = (uint32_t)v;
+  }
+  return from_words<T>(w);
 }
 
 template <int OP, typename VT, typename IT, typename CT>
-struct Smem {
-  using R = typename OpTraits<OP, VT, IT, CT>::R;
-  static __host__ __device__ size_t bytes(int nw) {
-    size_t b = sizeof(R) * ((size_t)nw * RING * 32 + (size_t)LRING * nw + (size_t)LRING * 32);
-    b = (b + 15) & ~size_t(15);
-    b += sizeof(int) * (4 * nw + 8) + sizeof(double) * (nw + 2);
-    return b;
-  }
+struct OpTraits {
+  // what a producer sends to one consumer direction
+  using X = typename std::conditional<OP == SWEEP_FACTOR, Pair<CT>, VT>::type;
+  static constexpr int P = Words<X>::P;
+  static constexpr int RING = 32 / P;   // intra-CTA ring depth (steps)
+  static constexpr int LRING = 64 / P;  // loader ring depth (steps)
+  static constexpr int LB = 16 / P;     // loader batch (steps fetched per round trip)
+  static constexpr int PF = (sizeof(VT) == 4 && OP != SWEEP_FACTOR) ? 8 : 4;  // cell prefetch depth (steps)
+  static_assert(RING > QPUB, "ring must be deeper than the progress interval");
+  static_assert(LRING >= LB + QPUB - 1, "loader ring too shallow");
 };
+
+template <int OP, typename VT, typename IT, typename CT>
+__host__ __device__ constexpr size_t smem_bytes(int nw) {
+  using T = OpTraits<OP, VT, IT, CT>;
+  return 8 * ((size_t)nw * T::RING * T::P * 32 + (size_t)T::LRING * T::P * nw +
+              (size_t)T::LRING * T::P * 32) +
+         sizeof(int) * (4 * (size_t)nw + 8) + sizeof(double) * (nw + 2);
+}
 
 template <int OP, typename VT, typename IT, typename CT, int NW>
 __global__ void __launch_bounds__((NW + 1) * 32, 1)
     sweep_kernel(SweepGrid g, SweepData<VT, IT, CT> d) {
-  using R = typename OpTraits<OP, VT, IT, CT>::R;
+  using TR = OpTraits<OP, VT, IT, CT>;
+  using X = typename TR::X;
+  constexpr int P = TR::P, RING = TR::RING, LRING = TR::LRING, LB = TR::LB, PF = TR::PF;
   constexpr bool REV = (OP == SWEEP_BWD);
+  constexpr bool DOT32 = std::is_same<VT, float>::value && !std::is_same<IT, double>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* ring = reinterpret_cast<R*>(smem_raw);               // [NW][RING][32]
-  R* jring = ring + (size_t)NW * RING * 32;               // [LRING][NW]
-  R* kring = jring + (size_t)LRING * NW;                  // [LRING][32]
-  size_t ofs = sizeof(R) * ((size_t)NW * RING * 32 + (size_t)LRING * NW + (size_t)LRING * 32);
-  ofs = (ofs + 15) & ~size_t(15);
-  int* s_tlo = reinterpret_cast<int*>(smem_raw + ofs);    // [NW]
-  int* s_thi = s_tlo + NW;                                // [NW]
-  volatile int* s_prog = s_thi + NW;                      // [NW]
-  int* s_misc = s_thi + 2 * NW;                           // [NW + 8]: lprog, tile lo/hi, flags
-  volatile int* s_lprog = s_misc;
-  double* s_red = reinterpret_cast<double*>(smem_raw + ofs + sizeof(int) * (4 * NW + 8));
+  unsigned long long* ring = reinterpret_cast<unsigned long long*>(smem_raw);  // [NW][RING][P][32]
+  unsigned long long* jring = ring + (size_t)NW * RING * P * 32;              // [LRING][P][NW]
+  unsigned long long* kring = jring + (size_t)LRING * P * NW;                 // [LRING][P][32]
+  int* s_tlo = reinterpret_cast<int*>(kring + (size_t)LRING * P * 32);        // [NW]
+  int* s_thi = s_tlo + NW;                                                    // [NW]
+  volatile int* s_prog = s_thi + NW;                                          // [NW] published progress
+  int* s_misc = s_thi + 2 * NW;                                               // [NW + 8]
+  double* s_red = reinterpret_cast<double*>(s_misc + NW + 8);                 // [NW + 2]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned gen = ld_volatile_u32(&g.ctl->gen);
   const int nj = g.nj, nk = g.nk, maxT = g.maxT;
 
-  bool skip = false;
-  if (OP != SWEEP_FACTOR && g.scal != nullptr) skip = *(volatile int*)&g.scal->done != 0;
-  if (skip) return;  // converged: nothing runs, generation unchanged
+  if (OP != SWEEP_FACTOR && g.scal != nullptr && *(volatile int*)&g.scal->done != 0) return;
 
-  for (int pos = blockIdx.x; pos < g.ntiles; pos += gridDim.x) {
-    if (ld_volatile_u32(&g.ctl->err)) break;
+  // Invalidate the rings: stamps below are unique per (tile sequence, step).
+  {
+    const size_t nwords = (size_t)(NW * RING * 32 + LRING * NW + LRING * 32) * P;
+    for (size_t q = threadIdx.x; q < nwords; q += blockDim.x) ring[q] = ~0ull;
+  }
+  __syncthreads();
+
+  for (int pos = blockIdx.x, seq = 0; pos < g.ntiles; pos += gridDim.x, ++seq) {
     const int tpos = REV ? g.ntiles - 1 - pos : pos;
     const int packed = g.tiles[tpos];
     const int J = packed & 0xffff, K = packed >> 16;
     const int j0 = J * 32, k0 = K * NW;
+    const uint32_t tstamp = (uint32_t)(seq & 0x7ff) << 20;   // | step (< 2^20)
 
     // ---------------- setup: per-warp wavefront ranges ----------------
     Line L = {0, 0, 0, 0};
@@ -138,7 +244,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
       s = j + k;
       int tl = INF_T, th = INT_MIN;
       if (L.len > 0) {
-        int a = L.lo + s, b = L.lo + L.len - 1 + s;
+        const int a = L.lo + s, b = L.lo + L.len - 1 + s;
         if (!REV) { tl = a; th = b; } else { tl = maxT - b; th = maxT - a; }
       }
       const int Tlo = __reduce_min_sync(XFP_FULL, tl);
@@ -147,9 +253,6 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
         s_tlo[warp] = Tlo;
         s_thi[warp] = Thi;
         s_prog[warp] = (Tlo == INF_T) ? INF_T : Tlo - 1;
-        if (Tlo == INF_T && k < nk) {  // no cells: tell consumers in other tiles
-          st_release_u64(&g.prog[(size_t)k * g.NJt + J], prog_word(gen, 0xffffffffu));
-        }
       }
     }
     __syncthreads();
@@ -161,7 +264,6 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
       }
       s_misc[1] = lo;
       s_misc[2] = hi;
-      *s_lprog = lo == INF_T ? INF_T : lo - 1;
     }
     __syncthreads();
     const int tileLo = s_misc[1], tileHi = s_misc[2];
@@ -173,19 +275,20 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
       // ======================= compute warp =======================
       const int Tlo = s_tlo[warp], Thi = s_thi[warp];
       const int k = k0 + warp;
-      const int zsrc = REV ? warp + 1 : warp - 1;   // producer warp in this tile (or loader)
+      const int zsrc = REV ? warp + 1 : warp - 1;   // producer warp in this tile (or the loader)
       const int zdst = REV ? warp - 1 : warp + 1;   // consumer warp in this tile
       const bool zsrc_in = zsrc >= 0 && zsrc < NW;
       const bool zdst_in = zdst >= 0 && zdst < NW;
       const int zsrc_lo = zsrc_in ? s_tlo[zsrc] : 0, zsrc_hi = zsrc_in ? s_thi[zsrc] : -1;
       const int zdst_lo = zdst_in ? s_tlo[zdst] : 0, zdst_hi = zdst_in ? s_thi[zdst] : -1;
-      const bool jb = REV ? (lane == 31) : (lane == 0);   // lane fed by the loader (j boundary)
-      const bool kb = !zsrc_in;                            // warp fed by the loader (k boundary)
-      unsigned long long* gprog = &g.prog[(size_t)k * g.NJt + J];
-      R* myring = ring + (size_t)warp * RING * 32;
-      const R* zring = zsrc_in ? ring + (size_t)zsrc * RING * 32 : nullptr;
+      const bool jb = REV ? (lane == 31) : (lane == 0);   // fed by the loader (j boundary)
+      const bool kb = !zsrc_in;                            // fed by the loader (k boundary)
+      // boundary producers publish stamped values for the neighbouring tiles
+      const bool jpub = REV ? (lane == 0) : (lane == 31);
+      const bool kpub = REV ? (warp == 0) : (warp == NW - 1);
+      unsigned long long* myring = ring + (size_t)warp * RING * P * 32;
+      const unsigned long long* zring = zsrc_in ? ring + (size_t)zsrc * RING * P * 32 : nullptr;
 
-      // Upper-neighbour lines for the factor's outgoing values.
       Line Ly = {0, 0, 0, 0}, Lz = {0, 0, 0, 0};
       if (OP == SWEEP_FACTOR) {
         const int j = j0 + lane;
@@ -193,288 +296,394 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
         if (j < nj && k + 1 < nk) Lz = g.lines[(size_t)(k + 1) * nj + j];
       }
 
-      // Values this lane produced at the previous step, per consumer direction.
-      R out_x{}, out_y{};
-      bool ok = true;
-      for (int tau = Tlo; tau <= Thi && ok; ++tau) {
-        const int i = REV ? (maxT - tau) - s : tau - s;
+      // Cell data of the next PF steps is kept in flight in a rotating register
+      // buffer.  Loads are unconditional from a clamped index (cell 0 when the
+      // step is outside the lane's span) and masked at use, so the step has
+      // no divergent branches.
+      struct CellData {
+        VT r, lx, ly, lz, rr;
+        IT inv;
+        CT dg, upx, upy, upz;
+        int cyup, czup;
+      };
+      const int di = REV ? -1 : 1;
+      auto load_cell = [&](int i) -> CellData {
+        CellData cd;
         const bool in = (unsigned)(i - L.lo) < (unsigned)L.len;
-        const long long c = (long long)L.off + (i - L.lo);
-
-        // ---- cell data (independent of the wavefront) ----
-        VT r_c = VT(0), lx_c = VT(0), ly_c = VT(0), lz_c = VT(0);
-        IT inv_c = IT(0);
-        CT dg = CT(0), upx = CT(0), upy = CT(0), upz = CT(0);
-        long long cyup = -1, czup = -1;
+        const int c = in ? L.off + (i - L.lo) : 0;
+        cd.rr = VT(0);
+        cd.r = cd.lx = cd.ly = cd.lz = VT(0);
+        cd.inv = IT(0);
+        cd.dg = cd.upx = cd.upy = cd.upz = CT(0);
+        cd.cyup = cd.czup = -1;
+        // L2 prefetch of the lane's line data LOOK steps further on: the lines
+        // are then L2-resident when the register pipeline loads them.
+        constexpr int LOOK = 32;
+        const int ip = i + LOOK * di;
+        const bool inp = (unsigned)(ip - L.lo) < (unsigned)L.len;
+        const int cp = inp ? L.off + (ip - L.lo) : 0;
         if constexpr (OP == SWEEP_FWD) {
-          if (in) { r_c = d.r[c]; lx_c = d.lx[c]; ly_c = d.ly[c]; lz_c = d.lz[c]; inv_c = d.inv[c]; }
+          cd.r = d.r[c]; cd.lx = d.lx[c]; cd.ly = d.ly[c]; cd.lz = d.lz[c]; cd.inv = d.inv[c];
+          if (inp) {
+            prefetch_l2(d.r + cp); prefetch_l2(d.lx + cp); prefetch_l2(d.ly + cp);
+            prefetch_l2(d.lz + cp); prefetch_l2(d.inv + cp);
+          }
         } else if constexpr (OP == SWEEP_BWD) {
-          if (in) { r_c = d.y[c]; lx_c = d.lx[c]; ly_c = d.ly[c]; lz_c = d.lz[c]; inv_c = d.inv[c]; }
+          cd.r = d.y[c]; cd.lx = d.lx[c]; cd.ly = d.ly[c]; cd.lz = d.lz[c]; cd.inv = d.inv[c];
+          cd.rr = d.r[c];
+          if (inp) {
+            prefetch_l2(d.y + cp); prefetch_l2(d.lx + cp); prefetch_l2(d.ly + cp);
+            prefetch_l2(d.lz + cp); prefetch_l2(d.inv + cp); prefetch_l2(d.r + cp);
+          }
         } else {
-          if (in) {
-            dg = d.diag[c];
-            if (i + 1 - L.lo < L.len) upx = d.ax[c + 1];
-            if ((unsigned)(i - Ly.lo) < (unsigned)Ly.len) {
-              cyup = (long long)Ly.off + (i - Ly.lo);
-              upy = d.ay[cyup];
-            }
-            if ((unsigned)(i - Lz.lo) < (unsigned)Lz.len) {
-              czup = (long long)Lz.off + (i - Lz.lo);
-              upz = d.az[czup];
-            }
-          }
+          cd.dg = d.diag[c];
+          const bool hx = in && (i + 1 - L.lo < L.len);
+          const CT ux = d.ax[hx ? c + 1 : 0];
+          cd.upx = hx ? ux : CT(0);
+          const bool hy = (unsigned)(i - Ly.lo) < (unsigned)Ly.len;
+          cd.cyup = hy ? Ly.off + (i - Ly.lo) : -1;
+          const CT uy = d.ay[hy ? cd.cyup : 0];
+          cd.upy = hy ? uy : CT(0);
+          const bool hz = (unsigned)(i - Lz.lo) < (unsigned)Lz.len;
+          cd.czup = hz ? Lz.off + (i - Lz.lo) : -1;
+          const CT uz = d.az[hz ? cd.czup : 0];
+          cd.upz = hz ? uz : CT(0);
         }
+        return cd;
+      };
+      const int i0 = REV ? (maxT - Tlo) - s : Tlo - s;
+      // pf[q] holds the data of step base+q; it is refilled for step base+q+PF
+      // right after use and first read again PF steps later (static indices,
+      // no register moves, so the load latency stays hidden).
+      CellData pf[PF];
+#pragma unroll
+      for (int q = 0; q < PF; ++q) pf[q] = load_cell(i0 + q * di);
 
-        // ---- y-neighbour value: neighbouring lane's previous step ----
-        R vy = REV ? shfl_down(out_y, 1) : shfl_up(out_y, 1);
-        // ---- z-neighbour value ----
-        R vz{};
-        if (!kb) {
-          if (tau - 1 >= zsrc_lo && tau - 1 <= zsrc_hi) {
-            Spin spin;
-            while (s_prog[zsrc] < tau - 1) {
-              if (!spin.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 1); ok = false; break; }
-            }
-            __threadfence_block();
-            vz = zring[(size_t)((tau - 1) & (RING - 1)) * 32 + lane];
+      X out_x{}, out_y{};
+      int cons_seen = zdst_in ? (int)s_prog[zdst] : INF_T;   // cached consumer progress
+      for (int base = Tlo; base <= Thi; base += PF) {
+#pragma unroll
+      for (int q = 0; q < PF; ++q) {
+        const int tau = base + q;
+        if (tau > Thi) break;
+        const int i = i0 + (tau - Tlo) * di;
+        const CellData cd = pf[q];
+        pf[q] = load_cell(i + PF * di);
+        const bool in = (unsigned)(i - L.lo) < (unsigned)L.len;
+        const int c = L.off + (i - L.lo);
+
+        // ---- neighbour values produced at the previous step ----
+        // z: previous warp (ring) or the loader (kring); j boundary: loader
+        // (jring, one word per warp, read by all lanes as a broadcast).
+        const bool zneed = kb || (tau - 1 >= zsrc_lo && tau - 1 <= zsrc_hi);   // warp-uniform
+        const uint32_t ez = tstamp | (kb ? tau : tau - 1), ej = tstamp | tau;
+        const unsigned long long* zaddr =
+            kb ? kring + (size_t)(tau & (LRING - 1)) * P * 32 + lane
+               : zring + (size_t)((tau - 1) & (RING - 1)) * P * 32 + lane;
+        const unsigned long long* jaddr = jring + (size_t)(tau & (LRING - 1)) * P * NW + warp;
+        unsigned long long wz[P], wj[P];
+        auto fetch = [&]() {
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            wz[p] = zneed ? ld_vol64(zaddr + (size_t)p * 32) : 0ull;
+            wj[p] = ld_vol64(jaddr + (size_t)p * NW);
           }
-        }
-        if (jb || kb) {
-          if (tau >= tileLo) {
-            Spin spin;
-            while (*s_lprog < tau) {
-              if (!spin.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 2); ok = false; break; }
-            }
-            __threadfence_block();
-            const int slot = tau & (LRING - 1);
-            if (jb) vy = jring[(size_t)slot * NW + warp];
-            if (kb) vz = kring[(size_t)slot * 32 + lane];
+        };
+        auto ready = [&]() -> bool {
+          bool ok = true;
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            ok &= !zneed || (uint32_t)(wz[p] >> 32) == ez;
+            ok &= !jb || (uint32_t)(wj[p] >> 32) == ej;
           }
+          return ok;
+        };
+        fetch();
+        if (!__all_sync(XFP_FULL, ready())) {
+          trace_wait(g, kb ? 2 : 1, tau);
+          Spin sp;
+          do {
+            if (!sp.step(g.ctl, g.spin_limit)) {
+              raise_timeout(g.ctl, kb ? 2 : 1, tpos, tau, OP, wz[0], ez);
+              break;
+            }
+            fetch();
+          } while (!__all_sync(XFP_FULL, ready()));
+          trace_wait(g, 0, tau);
         }
-        if (!__all_sync(XFP_FULL, ok)) { ok = false; break; }
+        X vz{};
+        if (zneed) {
+          uint32_t w[P];
+#pragma unroll
+          for (int p = 0; p < P; ++p) w[p] = (uint32_t)wz[p];
+          vz = from_words<X>(w);
+        }
+        X vy = REV ? shfl_down_any(out_y) : shfl_up_any(out_y);
+        if (jb) {
+          uint32_t w[P];
+#pragma unroll
+          for (int p = 0; p < P; ++p) w[p] = (uint32_t)wj[p];
+          vy = from_words<X>(w);
+        }
 
         // ---- the cell itself ----
-        R o_x{}, o_y{}, o_z{};
+        X o_x{}, o_y{}, o_z{};
         if constexpr (OP == SWEEP_FWD) {
           // solve_lower: columns c-nn, c-ni, c-1 scatter into row c in that
           // order, then result[c] *= invdiag[c]  (pcg_solver.h:198-203)
-          VT t = r_c;
-          t = sub_rn(t, mul_rn(lz_c, vz));
-          t = sub_rn(t, mul_rn(ly_c, vy));
-          t = sub_rn(t, mul_rn(lx_c, out_x));
-          VT y = in ? VT(mul_rn((IT)t, inv_c)) : VT(0);
+          VT t = cd.r;
+          t = sub_rn(t, mul_rn(cd.lz, vz));
+          t = sub_rn(t, mul_rn(cd.ly, vy));
+          t = sub_rn(t, mul_rn(cd.lx, out_x));
+          const VT y = in ? VT(mul_rn((IT)t, cd.inv)) : VT(0);
           if (in) d.y[c] = y;
           o_x = y; o_y = y; o_z = y;
         } else if constexpr (OP == SWEEP_BWD) {
           // solve_lower_transpose_in_place: x[c] -= L(m,c) x[m] for m = c+1,
           // c+ni, c+nn in that order, then x[c] *= invdiag[c]  (:215-218).
-          // Products L(m,c) x[m] arrive ready-made from the producers.
-          VT t = r_c;
+          // The products L(m,c) x[m] arrive ready-made from the producers.
+          VT t = cd.r;
           t = sub_rn(t, out_x);
           t = sub_rn(t, vy);
           t = sub_rn(t, vz);
-          VT z = in ? VT(mul_rn((IT)t, inv_c)) : VT(0);
-          if (in) {
-            d.y[c] = z;
-            const VT rr = d.r[c];
-            if (std::is_same<VT, float>::value && !std::is_same<IT, double>::value)
-              dot_acc_f = __fadd_rn(dot_acc_f, __fmul_rn((float)z, (float)rr));
-            else
-              dot_acc = __dadd_rn(dot_acc, __dmul_rn((double)z, (double)rr));
-          }
-          o_x = mul_rn(lx_c, z);
-          o_y = mul_rn(ly_c, z);
-          o_z = mul_rn(lz_c, z);
+          const VT z = in ? VT(mul_rn((IT)t, cd.inv)) : VT(0);
+          if (in) d.y[c] = z;
+          const VT rr = in ? cd.rr : VT(0);
+          if (DOT32) dot_acc_f = __fadd_rn(dot_acc_f, __fmul_rn((float)z, (float)rr));
+          else dot_acc = __dadd_rn(dot_acc, __dmul_rn((double)z, (double)rr));
+          o_x = mul_rn(in ? cd.lx : VT(0), z);
+          o_y = mul_rn(in ? cd.ly : VT(0), z);
+          o_z = mul_rn(in ? cd.lz : VT(0), z);
         } else {
           // factor_modified_incomplete_cholesky0 for column c: updates from
           // columns c-nn, c-ni, c-1 in that order (:137-184), each
           // d -= L*L then d -= omega*L*missing; pivot safeguard (:126-131).
-          IT inv = IT(0);
-          if (in && dg != CT(0)) {
-            CT dd = dg;
-            const Pair<CT> src[3] = {vz, vy, out_x};
+          const bool act = in && cd.dg != CT(0);
+          CT dd = cd.dg;
+          const X src[3] = {vz, vy, out_x};
 #pragma unroll
-            for (int q = 0; q < 3; ++q) {
-              dd = sub_rn(dd, mul_rn(src[q].a, src[q].a));
-              dd = sub_rn(dd, mul_rn(mul_rn(d.omega, src[q].a), src[q].b));
-            }
-            CT iv = (dd < mul_rn(d.ratio, dg)) ? rsqrt_ref(dg) : rsqrt_ref(dd);
-            inv = (IT)iv;
-            // column c's entries L(m,c) = A(m,c)*invdiag[c] for m = c+1,
-            // c+ni, c+nn, and for each the sum of the other two (dropped fill)
-            const CT px = mul_rn(upx, iv), py = mul_rn(upy, iv), pz = mul_rn(upz, iv);
-            o_x = {px, add_rn(py, pz)};
-            o_y = {py, add_rn(px, pz)};
-            o_z = {pz, add_rn(px, py)};
-            if (upx != CT(0)) { d.flx[c + 1] = px; d.fmx[c + 1] = o_x.b; }
-            if (cyup >= 0) { d.fly[cyup] = py; d.fmy[cyup] = o_y.b; }
-            if (czup >= 0) { d.flz[czup] = pz; d.fmz[czup] = o_z.b; }
+          for (int t = 0; t < 3; ++t) {
+            dd = sub_rn(dd, mul_rn(src[t].a, src[t].a));
+            dd = sub_rn(dd, mul_rn(mul_rn(d.omega, src[t].a), src[t].b));
           }
-          if (in) d.oinv[c] = inv;
+          const CT iv = act ? ((dd < mul_rn(d.ratio, cd.dg)) ? rsqrt_ref(cd.dg) : rsqrt_ref(dd)) : CT(0);
+          // column c's entries L(m,c) = A(m,c)*invdiag[c] for m = c+1,
+          // c+ni, c+nn, and for each the sum of the other two (dropped fill)
+          const CT px = mul_rn(cd.upx, iv), py = mul_rn(cd.upy, iv), pz = mul_rn(cd.upz, iv);
+          o_x = {px, add_rn(py, pz)};
+          o_y = {py, add_rn(px, pz)};
+          o_z = {pz, add_rn(px, py)};
+          if (act && cd.upx != CT(0)) d.flx[c + 1] = px;
+          if (act && cd.cyup >= 0) d.fly[cd.cyup] = py;
+          if (act && cd.czup >= 0) d.flz[cd.czup] = pz;
+          if (in) d.oinv[c] = (IT)iv;
         }
 
-        // ---- hand the z-direction value to the consumer warp ----
-        if (zdst_in && tau - RING + 1 >= zdst_lo && tau - RING + 1 <= zdst_hi) {
-          Spin spin;
-          while (s_prog[zdst] < tau - RING + 1) {
-            if (!spin.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 3); ok = false; break; }
-          }
+        // ---- publish for the other tiles (stamped with the generation) ----
+        if (in && jpub) {
+          uint32_t w[P];
+          to_words(o_y, w);
+#pragma unroll
+          for (int p = 0; p < P; ++p) st_gpu64(&d.sy[(size_t)c * P + p], stamped(gen, w[p]));
         }
-        myring[(size_t)(tau & (RING - 1)) * 32 + lane] = o_z;
+        if (in && kpub) {
+          uint32_t w[P];
+          to_words(o_z, w);
+#pragma unroll
+          for (int p = 0; p < P; ++p) st_gpu64(&d.sz[(size_t)c * P + p], stamped(gen, w[p]));
+        }
+
+        // ---- hand the z value to the consumer warp (ring back-pressure) ----
+        if (zdst_in) {
+          // slot tau%RING last held step tau-RING, which the consumer reads at
+          // step tau-RING+1; its progress is published every QPUB steps
+          const int need = tau - RING + 1;
+          if (need > cons_seen && need >= zdst_lo && need <= zdst_hi) {
+            trace_wait(g, 4, tau);
+            Spin sp;
+            while ((cons_seen = s_prog[zdst]) < need) {
+              if (!sp.step(g.ctl, g.spin_limit)) {
+                raise_timeout(g.ctl, 4, tpos, tau, OP, (unsigned long long)(unsigned)cons_seen, (unsigned)need);
+                break;
+              }
+            }
+            trace_wait(g, 0, tau);
+          }
+          uint32_t w[P];
+          to_words(o_z, w);
+          unsigned long long* slot = myring + (size_t)(tau & (RING - 1)) * P * 32 + lane;
+#pragma unroll
+          for (int p = 0; p < P; ++p) st_vol64(slot + (size_t)p * 32, stamped(tstamp | tau, w[p]));
+        }
         out_x = o_x;
         out_y = o_y;
-        __syncwarp();
-        if (lane == 0) {
-          __threadfence_block();
-          s_prog[warp] = tau;
-        }
-        if (((tau - Tlo + 1) & (PUB - 1)) == 0 && tau != Thi) {
+        // Progress is published only once every lane has finished the step
+        // (a slot is reused as soon as its consumer's progress says it was read).
+        if (((tau - Tlo) & (QPUB - 1)) == QPUB - 1) {
           __syncwarp();
           if (lane == 0) {
-            __threadfence();
-            st_release_u64(gprog, prog_word(gen, (unsigned)(tau + 1)));
+            s_prog[warp] = tau;
+            if (g.trace && !ld_volatile_u32(&g.ctl->err))
+              *(volatile int*)&g.trace[((size_t)blockIdx.x * (NW + 1) + warp) * 4 + 2] = tau;
           }
         }
-        if (!__all_sync(XFP_FULL, ok)) { ok = false; break; }
+      }
       }
       __syncwarp();
-      if (lane == 0) {
-        __threadfence();
-        if (k < nk) st_release_u64(gprog, prog_word(gen, 0xffffffffu));
-        s_prog[warp] = INF_T;
-      }
+      if (lane == 0) s_prog[warp] = INF_T;
     } else if (warp == NW && tileLo != INF_T) {
       // ======================= loader warp =======================
       // lane r < NW feeds jring row r (line k0+r); every lane l feeds kring
-      // column l (line j0+l).
+      // column l (line j0+l).  Sources are the neighbouring tiles' stamped
+      // boundary values (global), or zero where the source cell has no row.
       const int jc = REV ? j0 + 31 : j0, js = REV ? j0 + 32 : j0 - 1;
       const int kc = REV ? k0 + NW - 1 : k0, ks = REV ? k0 + NW : k0 - 1;
-      const int Jsrc = REV ? J + 1 : J - 1, Ksrc = REV ? K + 1 : K - 1;
-      bool jsrc_tile = Jsrc >= 0 && Jsrc < g.NJt && g.tile_active[(size_t)K * g.NJt + Jsrc];
-      bool ksrc_tile = Ksrc >= 0 && Ksrc < g.NKt && g.tile_active[(size_t)Ksrc * g.NJt + J];
-      // j source (row r = lane)
-      Line Ljs = {0, 0, 0, 0}, Ljc = {0, 0, 0, 0};
+      Line Ljs = {0, 0, 0, 0};
       int sj_c = 0, Sj_lo = INF_T, Sj_hi = INT_MIN;
-      const unsigned long long* pj = nullptr;
       {
         const int kr = k0 + lane;
-        if (lane < NW && kr < nk && js >= 0 && js < nj && jsrc_tile) {
-          Ljs = g.lines[(size_t)kr * nj + js];
-          if (jc < nj) Ljc = g.lines[(size_t)kr * nj + jc];
-          pj = &g.prog[(size_t)kr * g.NJt + Jsrc];
-        }
+        if (lane < NW && kr < nk && js >= 0 && js < nj) Ljs = g.lines[(size_t)kr * nj + js];
         sj_c = jc + kr;
         if (Ljs.len > 0) {
-          int a = Ljs.lo + sj_c, b = Ljs.lo + Ljs.len - 1 + sj_c;
+          const int a = Ljs.lo + sj_c, b = Ljs.lo + Ljs.len - 1 + sj_c;
           if (!REV) { Sj_lo = a; Sj_hi = b; } else { Sj_lo = maxT - b; Sj_hi = maxT - a; }
         }
       }
-      // k source (column l = lane)
-      Line Lks = {0, 0, 0, 0}, Lkc = {0, 0, 0, 0};
+      Line Lks = {0, 0, 0, 0};
       int sk_c = 0, Sk_lo = INF_T, Sk_hi = INT_MIN;
-      const unsigned long long* pk = nullptr;
       {
         const int jl = j0 + lane;
-        if (jl < nj && ks >= 0 && ks < nk && ksrc_tile) {
-          Lks = g.lines[(size_t)ks * nj + jl];
-          if (kc < nk) Lkc = g.lines[(size_t)kc * nj + jl];
-          pk = &g.prog[(size_t)ks * g.NJt + J];
-        }
+        if (jl < nj && ks >= 0 && ks < nk) Lks = g.lines[(size_t)ks * nj + jl];
         sk_c = jl + kc;
         if (Lks.len > 0) {
-          int a = Lks.lo + sk_c, b = Lks.lo + Lks.len - 1 + sk_c;
+          const int a = Lks.lo + sk_c, b = Lks.lo + Lks.len - 1 + sk_c;
           if (!REV) { Sk_lo = a; Sk_hi = b; } else { Sk_lo = maxT - b; Sk_hi = maxT - a; }
         }
       }
-      Spin spin;
-      int next = tileLo;
-      while (next <= tileHi) {
-        // how far the producers allow us to go
-        long long lim = (long long)tileHi;
-        if (Sj_lo <= Sj_hi) {
-          unsigned v = prog_value(ld_acquire_u64(pj), gen);
-          long long m = (v >= (unsigned)Sj_hi || v == 0xffffffffu) ? LLONG_MAX : max((long long)v, (long long)Sj_lo - 1);
-          lim = min(lim, m);
-        }
-        if (Sk_lo <= Sk_hi) {
-          unsigned v = prog_value(ld_acquire_u64(pk), gen);
-          long long m = (v >= (unsigned)Sk_hi || v == 0xffffffffu) ? LLONG_MAX : max((long long)v, (long long)Sk_lo - 1);
-          lim = min(lim, m);
-        }
-        // ring space: every compute warp must have finished tau - LRING
-        int minp = INF_T;
-        for (int w = 0; w < NW; ++w) minp = min(minp, (int)s_prog[w]);
-        if (minp != INF_T) lim = min(lim, (long long)minp + LRING);
-        int limit = (int)lim;
-        limit = __reduce_min_sync(XFP_FULL, limit);
-        if (limit < next) {
-          if (!spin.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 4); break; }
-          continue;
-        }
-        spin.n = 0;
-        for (int tau = next; tau <= limit; ++tau) {
-          const int slot = tau & (LRING - 1);
-          if (lane < NW) {
-            R v{};
-            const int i = REV ? (maxT - tau) - sj_c : tau - sj_c;
-            if (tau >= Sj_lo && tau <= Sj_hi) {
-              const long long n = (long long)Ljs.off + (i - Ljs.lo);
-              if constexpr (OP == SWEEP_FWD) {
-                v = ld_relaxed(&d.y[n]);
-              } else if constexpr (OP == SWEEP_BWD) {
-                v = mul_rn(d.ly[n], ld_relaxed(&d.y[n]));
-              } else {
-                if ((unsigned)(i - Ljc.lo) < (unsigned)Ljc.len) {
-                  const long long cc = (long long)Ljc.off + (i - Ljc.lo);
-                  Pair<CT> pr;
-                  pr.a = ld_relaxed(&d.fly[cc]);
-                  pr.b = ld_relaxed(&d.fmy[cc]);
-                  v = pr;
-                }
-              }
-            }
-            jring[(size_t)slot * NW + lane] = v;
+      int cons_min = tileLo - 1;   // cached min progress over the compute warps
+      for (int base = tileLo; base <= tileHi; base += LB) {
+        // ring space for the whole batch: slot of step t last held t-LRING,
+        // read by its consumers at that same step
+        const int need = base + LB - 1 - LRING;
+        if (need > cons_min) {
+          trace_wait(g, 5, base);
+          Spin sp;
+          for (;;) {
+            int m = INF_T;
+            for (int w = 0; w < NW; ++w) m = min(m, (int)s_prog[w]);
+            cons_min = m;
+            if (cons_min >= need) break;
+            if (!sp.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 5, tpos, base, OP, (unsigned long long)(unsigned)cons_min, (unsigned)need); break; }
           }
-          {
-            R v{};
-            const int i = REV ? (maxT - tau) - sk_c : tau - sk_c;
-            if (tau >= Sk_lo && tau <= Sk_hi) {
-              const long long n = (long long)Lks.off + (i - Lks.lo);
-              if constexpr (OP == SWEEP_FWD) {
-                v = ld_relaxed(&d.y[n]);
-              } else if constexpr (OP == SWEEP_BWD) {
-                v = mul_rn(d.lz[n], ld_relaxed(&d.y[n]));
-              } else {
-                if ((unsigned)(i - Lkc.lo) < (unsigned)Lkc.len) {
-                  const long long cc = (long long)Lkc.off + (i - Lkc.lo);
-                  Pair<CT> pr;
-                  pr.a = ld_relaxed(&d.flz[cc]);
-                  pr.b = ld_relaxed(&d.fmz[cc]);
-                  v = pr;
-                }
-              }
+          trace_wait(g, 0, base);
+        }
+        // Wait until the producers have published the LAST step of the batch
+        // this lane needs (they publish in step order), so the whole batch is
+        // fetched with one more round trip instead of one round trip per step.
+        {
+          int lj = INT_MIN, lk = INT_MIN;
+          const int bhi = min(base + LB - 1, tileHi);
+          if (lane < NW && Sj_lo <= Sj_hi) lj = min(bhi, Sj_hi) >= max(base, Sj_lo) ? min(bhi, Sj_hi) : INT_MIN;
+          if (Sk_lo <= Sk_hi) lk = min(bhi, Sk_hi) >= max(base, Sk_lo) ? min(bhi, Sk_hi) : INT_MIN;
+          if (lj != INT_MIN) {
+            const int ij = REV ? (maxT - lj) - sj_c : lj - sj_c;
+            const unsigned long long* a = &d.sy[(size_t)(Ljs.off + (ij - Ljs.lo)) * P + (P - 1)];
+            unsigned long long v = ld_gpu64(a);
+            if ((uint32_t)(v >> 32) != gen) {
+              trace_wait(g, 8, lj);
+              Spin s2;
+              do {
+                if (!s2.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 8, tpos, lj, OP, v, gen); break; }
+                v = ld_gpu64(a);
+              } while ((uint32_t)(v >> 32) != gen);
+              trace_wait(g, 0, lj);
             }
-            kring[(size_t)slot * 32 + lane] = v;
+          }
+          if (lk != INT_MIN) {
+            const int ik = REV ? (maxT - lk) - sk_c : lk - sk_c;
+            const unsigned long long* a = &d.sz[(size_t)(Lks.off + (ik - Lks.lo)) * P + (P - 1)];
+            unsigned long long v = ld_gpu64(a);
+            if ((uint32_t)(v >> 32) != gen) {
+              trace_wait(g, 9, lk);
+              Spin s2;
+              do {
+                if (!s2.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 9, tpos, lk, OP, v, gen); break; }
+                v = ld_gpu64(a);
+              } while ((uint32_t)(v >> 32) != gen);
+              trace_wait(g, 0, lk);
+            }
           }
         }
-        __syncwarp();
-        if (lane == 0) {
-          __threadfence_block();
-          *s_lprog = limit;
+        // issue the batch's loads, then poll until every stamp is current
+        unsigned long long vj[LB][P], vk[LB][P];
+        bool needj[LB], needk[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          const int tau = base + q;
+          needj[q] = lane < NW && tau <= tileHi && tau >= Sj_lo && tau <= Sj_hi;
+          needk[q] = tau <= tileHi && tau >= Sk_lo && tau <= Sk_hi;
+          const int ij = REV ? (maxT - tau) - sj_c : tau - sj_c;
+          const int ik = REV ? (maxT - tau) - sk_c : tau - sk_c;
+          const size_t nj_ = needj[q] ? (size_t)(Ljs.off + (ij - Ljs.lo)) : 0;
+          const size_t nk_ = needk[q] ? (size_t)(Lks.off + (ik - Lks.lo)) : 0;
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            vj[q][p] = needj[q] ? ld_gpu64(&d.sy[nj_ * P + p]) : 0ull;
+            vk[q][p] = needk[q] ? ld_gpu64(&d.sz[nk_ * P + p]) : 0ull;
+          }
         }
-        next = limit + 1;
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          const int tau = base + q;
+          const int ij = REV ? (maxT - tau) - sj_c : tau - sj_c;
+          const int ik = REV ? (maxT - tau) - sk_c : tau - sk_c;
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            if (needj[q] && (uint32_t)(vj[q][p] >> 32) != gen) {
+              trace_wait(g, 6, tau);
+              Spin s2;
+              const size_t n = (size_t)(Ljs.off + (ij - Ljs.lo)) * P + p;
+              do {
+                if (!s2.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 6, tpos, tau, OP, vj[q][p], gen); break; }
+                vj[q][p] = ld_gpu64(&d.sy[n]);
+              } while ((uint32_t)(vj[q][p] >> 32) != gen);
+              trace_wait(g, 0, tau);
+            }
+            if (needk[q] && (uint32_t)(vk[q][p] >> 32) != gen) {
+              trace_wait(g, 7, tau);
+              Spin s2;
+              const size_t n = (size_t)(Lks.off + (ik - Lks.lo)) * P + p;
+              do {
+                if (!s2.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 7, tpos, tau, OP, vk[q][p], gen); break; }
+                vk[q][p] = ld_gpu64(&d.sz[n]);
+              } while ((uint32_t)(vk[q][p] >> 32) != gen);
+              trace_wait(g, 0, tau);
+            }
+          }
+          if (tau <= tileHi) {
+            const uint32_t st = tstamp | tau;
+            const int slot = tau & (LRING - 1);
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+              if (lane < NW)
+                st_vol64(&jring[((size_t)slot * P + p) * NW + lane], stamped(st, needj[q] ? (uint32_t)vj[q][p] : 0u));
+              st_vol64(&kring[((size_t)slot * P + p) * 32 + lane], stamped(st, needk[q] ? (uint32_t)vk[q][p] : 0u));
+            }
+          }
+        }
       }
     }
 
     // ---------------- tile epilogue: dot partial (backward) ----------------
     if (OP == SWEEP_BWD) {
-      double v = std::is_same<VT, float>::value && !std::is_same<IT, double>::value ? (double)dot_acc_f : dot_acc;
-      if (std::is_same<VT, float>::value && !std::is_same<IT, double>::value) {
+      double v;
+      if (DOT32) {
         float f = dot_acc_f;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) f = __fadd_rn(f, __shfl_xor_sync(XFP_FULL, f, o));
         v = f;
       } else {
+        v = dot_acc;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_xor_sync(XFP_FULL, v, o));
       }
@@ -482,7 +691,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
     }
     __syncthreads();
     if (OP == SWEEP_BWD && threadIdx.x == 0) {
-      if (std::is_same<VT, float>::value && !std::is_same<IT, double>::value) {
+      if (DOT32) {
         float t = 0.f;
         for (int w = 0; w < NW; ++w) t = __fadd_rn(t, (float)s_red[w]);
         d.partials[tpos] = t;
@@ -504,95 +713,93 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
     s_last = (t == gridDim.x - 1);
   }
   __syncthreads();
-  if (s_last) {
+  if (s_last && threadIdx.x == 0) {
     __threadfence();
     if (OP == SWEEP_BWD && g.scal != nullptr) {
       // deterministic reduction of the per-tile partials: rho_new = z.r
       double acc = 0.0;
       float accf = 0.f;
-      const bool f32 = std::is_same<VT, float>::value && !std::is_same<IT, double>::value;
-      if (threadIdx.x == 0) {
-        for (int t = 0; t < g.ntiles; ++t) {
-          double pv = ld_relaxed(&d.partials[t]);
-          if (f32) accf = __fadd_rn(accf, (float)pv); else acc = __dadd_rn(acc, pv);
-        }
-        const double rho_new = f32 ? (double)accf : acc;
-        PcgScalars* sc = g.scal;
-        if (g.bwd_mode == 0) {
-          sc->rho = rho_new;
-          if (rho_new == 0.0 || rho_new != rho_new) { sc->status = -5; sc->done = 1; }
-        } else {
-          const double beta = f32 ? (double)__fdiv_rn((float)rho_new, (float)sc->rho) : __ddiv_rn(rho_new, sc->rho);
-          sc->beta = beta;
-          sc->rho = rho_new;
-        }
+      for (int t = 0; t < g.ntiles; ++t) {
+        const double pv = ((volatile double*)d.partials)[t];
+        if (DOT32) accf = __fadd_rn(accf, (float)pv); else acc = __dadd_rn(acc, pv);
+      }
+      const double rho_new = DOT32 ? (double)accf : acc;
+      PcgScalars* sc = g.scal;
+      if (g.bwd_mode == 0) {
+        sc->rho = rho_new;
+        if (rho_new == 0.0 || rho_new != rho_new) { sc->status = -5; sc->done = 1; }
+      } else {
+        sc->beta = DOT32 ? (double)__fdiv_rn((float)rho_new, (float)sc->rho) : __ddiv_rn(rho_new, sc->rho);
+        sc->rho = rho_new;
       }
     }
-    if (threadIdx.x == 0) {
-      g.ctl->finished = 0;
-      __threadfence();
-      atomicExch(&g.ctl->gen, gen + 1);
-    }
+    g.ctl->finished = 0;
+    __threadfence();
+    atomicExch(&g.ctl->gen, gen + 1);
   }
 }
 
-template <int OP, typename VT, typename IT, typename CT>
-static cudaError_t launch_op(const SweepGrid& g, const SweepData<VT, IT, CT>& d, int nw, int grid,
-                             cudaStream_t st) {
-  size_t sm = Smem<OP, VT, IT, CT>::bytes(nw);
-  void* args[] = {(void*)&g, (void*)&d};
+// ---------------------------------------------------------------- host side
+template <int OP, typename VT, typename IT, typename CT, int NW>
+static cudaError_t prepare(int* max_grid) {
+  static int cached = -1;
+  static cudaError_t cached_err = cudaSuccess;
+  if (cached < 0) {
+    const size_t sm = smem_bytes<OP, VT, IT, CT>(NW);
+    auto kfn = sweep_kernel<OP, VT, IT, CT, NW>;
+    cached_err = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int dev = 0, nsm = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cached_err == cudaSuccess)
+      cached_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, (NW + 1) * 32, sm);
+    cached = per * nsm;
+  }
+  *max_grid = cached;
+  return cached_err;
+}
+
+template <int OP, typename VT, typename IT, typename CT, int NW>
+static cudaError_t launch_nw(const SweepGrid& g, const SweepData<VT, IT, CT>& d, int grid, cudaStream_t st) {
+  int maxg = 0;
+  cudaError_t e = prepare<OP, VT, IT, CT, NW>(&maxg);
+  if (e != cudaSuccess) return e;
+  if (grid > maxg) grid = maxg;
+  if (grid <= 0) return cudaErrorInvalidConfiguration;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cfg.gridDim = dim3(grid);
-  cfg.dynamicSmemBytes = sm;
+  cfg.blockDim = dim3((NW + 1) * 32);
+  cfg.dynamicSmemBytes = smem_bytes<OP, VT, IT, CT>(NW);
   cfg.stream = st;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  (void)args;
+  return cudaLaunchKernelEx(&cfg, sweep_kernel<OP, VT, IT, CT, NW>, g, d);
+}
+
+template <int OP, typename VT, typename IT, typename CT>
+static cudaError_t launch_op(const SweepGrid& g, const SweepData<VT, IT, CT>& d, int nw, int grid,
+                             cudaStream_t st) {
   switch (nw) {
-#define XFP_NW_CASE(N)                                                                       \
-  case N: {                                                                                  \
-    auto kfn = sweep_kernel<OP, VT, IT, CT, N>;                                              \
-    cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);         \
-    cfg.blockDim = dim3((N + 1) * 32);                                                       \
-    return cudaLaunchKernelEx(&cfg, kfn, g, d);                                              \
-  }
-    XFP_NW_CASE(8)
-    XFP_NW_CASE(16)
-#undef XFP_NW_CASE
-    default:
-      return cudaErrorInvalidValue;
+    case 8: return launch_nw<OP, VT, IT, CT, 8>(g, d, grid, st);
+    case 16: return launch_nw<OP, VT, IT, CT, 16>(g, d, grid, st);
+    default: return cudaErrorInvalidValue;
   }
 }
 
 template <int OP, typename VT, typename IT, typename CT>
 static int max_grid_op(int nw) {
-  size_t sm = Smem<OP, VT, IT, CT>::bytes(nw);
-  int dev = 0, nsm = 0, per = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  int maxg = 0;
   switch (nw) {
-    case 8: {
-      auto kfn = sweep_kernel<OP, VT, IT, CT, 8>;
-      cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, (8 + 1) * 32, sm);
-      break;
-    }
-    case 16: {
-      auto kfn = sweep_kernel<OP, VT, IT, CT, 16>;
-      cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, (16 + 1) * 32, sm);
-      break;
-    }
-    default:
-      return 0;
+    case 8: prepare<OP, VT, IT, CT, 8>(&maxg); break;
+    case 16: prepare<OP, VT, IT, CT, 16>(&maxg); break;
+    default: break;
   }
-  return per * nsm;
+  return maxg;
 }
 
-// ---- explicit entry points (declared in xfp_kernels.h) ----
 #define XFP_SWEEP_INST(VT, IT, CT)                                                              \
   cudaError_t sweep_launch(int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d, int nw,  \
                            int grid, cudaStream_t st) {                                         \
