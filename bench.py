@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark: 256^3 pressure projections per second on B200.
+
+Workload (the standalone-projection configuration): a 256^3 MAC grid whose fluid
+mask is 32 seeded Gaussian blobs (sigma ~ U[0.03,0.12]) thresholded at 0.5, a
+random box obstacle covering 10% of the volume with fractional face weights, a
+solid border and U[-1,1] FP32 face velocities (xfluid_b200.scenes.blob_scene,
+seed 3).  One step = one projection: layout + assembly, MIC(0) factorisation,
+PCG to |r|_inf <= 1e-6 |b|_inf, pressure scatter and velocity update.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm prints one JSON line whose `value` is device-resident throughput in the
+mixed-precision form (inputs already in HBM, a distinct input copy per step so
+inputs exceed L2), with `e2e` measured through the C ABI from pinned host
+buffers, `roofline` for the dominant kernel (the MIC(0) triangular-solve sweeps,
+timed with CUDA events on the launching stream), the plain FP32 and FP64 GPU
+forms beside it, and the CPU baseline.  The reference arm (--impl reference)
+times xFluid's own CPU solver (oracle/_ref, built from the reference sources;
+the oracle's C port where that build is absent) on the same scene.
+
+Multi-GPU: a single projection does not shard (the lexicographic MIC(0) is one
+global wavefront), so N GPUs run N independent replicas; value = N * K / (max
+over ranks of the timed region).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "256³ projections/s, mixed-prec vs plain GPU MIC(0)-PCG at rel-res 1e-6; HBM GB/s"
+UNIT = "projections/s"
+TOL = 1e-6
+MAXIT = 2000
+SEED = 3
+
+
+def workload_config(n, rows=None, iters=None):
+    cfg = {"workload": f"blob scene {n}^3 (32 Gaussian blobs, 10% box obstacle with fractional faces, "
+                       f"U[-1,1] FP32 faces, seed {SEED}); tol 1e-6 relative inf-norm",
+           "grid": [n, n, n], "tol": TOL, "l2": "inputs larger than L2: a distinct input copy per step"}
+    if rows is not None:
+        cfg["rows"] = rows
+    if iters is not None:
+        cfg["iterations"] = iters
+    return cfg
+
+
+# ---------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms (read-only)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(s[1]) for s in self.samples if num(s[1]) is not None]
+        mx = [num(s[2]) for s in self.samples if num(s[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for s in self.samples for q in range(4)
+                          if len(s) > 5 + q and s[5 + q].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------- CPU baseline
+def cpu_project_seconds(sc):
+    """One projection of the scene by xFluid's own CPU solver when it was built
+    (oracle/_ref), else by the oracle's C port.  Returns (seconds, kind)."""
+    import oracle
+    s64 = sc.astype(np.float64)
+    if oracle.reference_available():
+        R = oracle.Reference()
+        t = time.perf_counter()
+        R.project(s64.reference_mode(), tol=TOL, maxit=MAXIT)
+        return time.perf_counter() - t, "reference"
+    oracle.build_oracle()
+    O = oracle.Oracle()
+    t = time.perf_counter()
+    O.project(s64, tol=TOL, maxit=MAXIT)
+    return time.perf_counter() - t, "port"
+
+
+def _ref_worker(conn, n):
+    from xfluid_b200 import scenes
+    sc = scenes.blob_scene(n, seed=SEED, dtype=np.float32)
+    conn.send("ready")
+    while True:
+        msg = conn.recv()
+        if msg == "stop":
+            break
+        sec, kind = cpu_project_seconds(sc)
+        conn.send((sec, kind))
+
+
+def reference_arm(args, rank, world):
+    """xFluid's CPU solver on every usable host core, one projection per core per step."""
+    import multiprocessing as mp
+    if rank != 0:
+        return
+    cores = min(os.cpu_count() or 1, 16)
+    ctxmp = mp.get_context("spawn")
+    pipes, procs = [], []
+    for _ in range(cores):
+        a, b = ctxmp.Pipe()
+        p = ctxmp.Process(target=_ref_worker, args=(b, args.n), daemon=True)
+        p.start()
+        pipes.append(a)
+        procs.append(p)
+    for a in pipes:
+        a.recv()
+    kinds = set()
+
+    def step():
+        for a in pipes:
+            a.send("go")
+        res = [a.recv() for a in pipes]
+        kinds.update(k for _, k in res)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    el = time.perf_counter() - t0
+    for a in pipes:
+        a.send("stop")
+    for p in procs:
+        p.join(timeout=30)
+    value = cores * args.steps / el
+    kind = "reference" if kinds == {"reference"} else "port"
+    sample = (f"{cores} processes, each one full {args.n}^3 projection per step (assemble + MIC(0)-PCG to "
+              f"1e-6 + applyPressure), same seeded scene without fractional face weights (xFluid has none)")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": workload_config(args.n),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------- our arm
+def sweep_traffic_per_row():
+    """DRAM bytes per unknown row of one sweep launch, from the committed ncu
+    summary (profiles/sweep_traffic.txt); None when absent."""
+    f = ROOT / "profiles" / "sweep_traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("dram_bytes_per_row_per_sweep:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def ours(args, rank, world):
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+    from xfluid_b200 import _lib, scenes
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    stream = torch.cuda.current_stream()
+
+    sc = scenes.blob_scene(args.n, seed=SEED, dtype=np.float32)
+    ni, nj, nk = sc.ni, sc.nj, sc.nk
+
+    def ctx_for(prec, device_pointers):
+        o = _lib.default_options()
+        o.precision = _lib.PREC[prec]
+        o.tol, o.max_iter = TOL, MAXIT
+        o.device = dev
+        o.device_pointers = device_pointers
+        o.stream = C.c_void_p(stream.cuda_stream)
+        return _lib.Context(o)
+
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    mat = t(sc.mat)
+    wts = [t(a) for a in (sc.wu, sc.wv, sc.ww)]
+    nsteps = args.steps + args.warmup
+    vel0 = [t(a) for a in (sc.u, sc.v, sc.w)]
+    copies = [[a.clone() for a in vel0] for _ in range(nsteps)]
+    pres = torch.zeros((nk, nj, ni), dtype=torch.float32, device="cuda")
+    P = lambda x: C.c_void_p(x.data_ptr())
+
+    def project_dev(ctx, vel, p):
+        st = _lib.XfpStats()
+        rc = ctx.lib.xfp_project_f32(ctx.ptr, ni, nj, nk, P(mat), P(vel[0]), P(vel[1]), P(vel[2]),
+                                     *map(P, wts), P(p), C.byref(st))
+        ctx.check(rc)
+        return rc, st.as_dict()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        tt = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    # ---------------- headline: mixed precision, device-resident inputs ----------------
+    ctx = ctx_for("mixed", 1)
+    stats = []
+    for s in range(args.warmup):
+        project_dev(ctx, copies[s], pres)
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        ev0.record(stream)
+        for s in range(args.steps):
+            rc, st = project_dev(ctx, copies[args.warmup + s], pres)
+            stats.append((rc, st))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms)
+    value = world * args.steps / (ms_max / 1000.0)
+    last = stats[-1][1]
+    rows = int(last["rows"])
+    iters = int(last["iterations"])
+    launches = int(sum(s["launches"] for _, s in stats))
+    sweep_ms = sum(s["ms_sweeps"] for _, s in stats)
+    sweeps = sum(s["sweeps"] for _, s in stats)
+    # algorithmic bytes of one sweep launch (mixed: FP32 vectors/L, FP64 invdiag):
+    # forward r 4 + L 12 + invdiag 8 + y 4 = 28 B/row; backward y 4 + L 12 +
+    # invdiag 8 + r 4 + z 4 = 32 B/row; launches alternate -> 30 B/row average
+    bytes_per_launch = 30.0 * rows
+    avg_launch_s = (sweep_ms / max(sweeps, 1)) / 1000.0
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = bytes_per_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else None
+    tr = sweep_traffic_per_row()
+    roofline = {"bound": "hbm", "kernel": "MIC(0) triangular-solve sweeps (sweep_kernel fwd/bwd)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": (tr * rows) if tr is not None else None,
+                "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_launch_s * 1000,
+                "sweep_share_of_step": sweep_ms / ms if ms > 0 else None}
+
+    # ---------------- e2e: through the C ABI from pinned host buffers ----------------
+    ctx_h = ctx_for("mixed", 0)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    hmat = pin(sc.mat)
+    hw = [pin(a) for a in (sc.wu, sc.wv, sc.ww)]
+    hvel0 = [pin(a) for a in (sc.u, sc.v, sc.w)]
+    hp = torch.zeros((nk, nj, ni), dtype=torch.float32).pin_memory()
+    e2e_steps = max(2, min(args.steps, 5))
+    hcopies = [[a.clone().pin_memory() for a in hvel0] for _ in range(e2e_steps + 1)]
+
+    def project_host(vel):
+        st = _lib.XfpStats()
+        rc = ctx_h.lib.xfp_project_f32(ctx_h.ptr, ni, nj, nk, P(hmat), P(vel[0]), P(vel[1]), P(vel[2]),
+                                       *map(P, hw), P(hp), C.byref(st))
+        ctx_h.check(rc)
+
+    project_host(hcopies[0])
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in range(e2e_steps):
+        project_host(hcopies[1 + s])
+    torch.cuda.synchronize()
+    el = max_over_ranks(time.perf_counter() - t0)
+    h2d = sc.mat.nbytes + sum(a.nbytes for a in (sc.u, sc.v, sc.w, sc.wu, sc.wv, sc.ww))
+    d2h = hp.numel() * 4 + sum(a.nbytes for a in (sc.u, sc.v, sc.w))
+    e2e = {"value": world * e2e_steps / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "path": "xfp_project_f32, host pointers (pinned)"}
+
+    # ---------------- plain forms and accuracy against an FP64 solve ----------------
+    forms = {}
+    ref_p = None
+    ctx64 = ctx_for("f64", 1)
+    o = ctx64.opts
+    o.tol = 1e-12
+    ctx64.set_options(o)
+    p64 = torch.zeros((nk, nj, ni), dtype=torch.float32, device="cuda")
+    project_dev(ctx64, [a.clone() for a in vel0], p64)
+    ref_p = p64.double()
+    accs = {}
+
+    def rel(a):
+        return float(torch.linalg.norm(a.double() - ref_p) / torch.linalg.norm(ref_p))
+
+    accs["mixed"] = {"pressure_rel_l2_vs_fp64": rel(pres), "rel_residual": last["rel_residual"],
+                     "iterations": iters, "refinements": int(last["refinements"])}
+    for prec in ("f32", "f64"):
+        c2 = ctx_for(prec, 1)
+        p2 = torch.zeros_like(pres)
+        project_dev(c2, [a.clone() for a in vel0], p2)
+        torch.cuda.synchronize()
+        reps = 2
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        vs = [[a.clone() for a in vel0] for _ in range(reps)]
+        e0.record(stream)
+        for r_ in range(reps):
+            rc2, st2 = project_dev(c2, vs[r_], p2)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        forms["plain_" + prec] = {"value": reps / (e0.elapsed_time(e1) / 1000.0), "unit": UNIT,
+                                  "iterations": int(st2["iterations"]), "rel_residual": st2["rel_residual"],
+                                  "pressure_rel_l2_vs_fp64": rel(p2), "status": rc2}
+        c2.close()
+    forms["mixed_over_plain_f32"] = value / world / forms["plain_f32"]["value"]
+    forms["mixed_over_plain_f64"] = value / world / forms["plain_f64"]["value"]
+
+    # ---------------- CPU baseline (rank 0, N=1 only) ----------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sec, kind = cpu_project_seconds(sc)
+        cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": (f"one full {args.n}^3 projection ({sec:.1f} s): assemble + MIC(0)-PCG to 1e-6 + "
+                          "applyPressure, single-threaded as xFluid's PCG is"
+                          + ("; same scene without fractional face weights (xFluid has none)" if kind == "reference"
+                             else "; oracle C port, same scene"))}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "mixed f32/f64",
+            "data": "synthetic (seeded blob scene)",
+            "config": dict(workload_config(args.n, rows, iters),
+                           parallelism="replicas" if world > 1 else "single GPU"),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk.summary(), "accuracy": accs, "forms": forms}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for c in (ctx, ctx_h, ctx64):
+        c.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+    else:
+        ours(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

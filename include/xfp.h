@@ -85,6 +85,9 @@ typedef struct xfp_stats {
   double ms_apply;       /* pressure scatter + velocity update */
   double ms_total;       /* whole call incl. host<->device copies */
   double bytes;          /* algorithmic bytes moved by the device kernels */
+  double ms_sweeps;      /* device time of the MIC(0) triangular-solve sweeps (CUDA events) */
+  int sweeps;            /* triangular-solve sweep launches timed in ms_sweeps */
+  long long launches;    /* device kernels launched by this call */
 } xfp_stats;
 
 /* Fills opt with defaults: tol 1e-5, max_iter 100, omega 0.97, ratio 0.25 --

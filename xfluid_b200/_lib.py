@@ -57,6 +57,9 @@ class XfpStats(C.Structure):
         ("ms_apply", C.c_double),
         ("ms_total", C.c_double),
         ("bytes", C.c_double),
+        ("ms_sweeps", C.c_double),
+        ("sweeps", C.c_int),
+        ("launches", C.c_longlong),
     ]
 
     def as_dict(self) -> dict:

@@ -83,6 +83,10 @@ struct xfp_ctx {
   int iters = 0, refinements = 0;
   double res = 0, bnorm = 0;
   cudaEvent_t ev[8] = {};
+  // device timing of the triangular-solve sweeps (pairs of events, read at the end)
+  std::vector<cudaEvent_t> sweep_ev;
+  int sweep_ev_used = 0;
+  long long launches = 0;
 };
 
 namespace {
@@ -166,6 +170,7 @@ int ensure_compact(xfp_ctx* ctx, int prec) {
   if (prec == XFP_PREC_F64) {
     XFP_CUDA(ctx, ctx->s64.ensure(M * 8));
     XFP_CUDA(ctx, ctx->z64.ensure(M * 8));
+    XFP_CUDA(ctx, ctx->x32.ensure(M * 4));  // FP32 output staging
   }
   if (prec == XFP_PREC_F32 || prec == XFP_PREC_MIXED) {
     for (auto& b : ctx->A32) XFP_CUDA(ctx, b.ensure(M * 4));
@@ -218,8 +223,29 @@ int run_sweep(xfp_ctx* ctx, int op, const SweepGrid& g, const SweepData<VT, IT, 
   int maxg = sweep_max_grid(op, d, ctx->nw);
   if (maxg <= 0) return fail(ctx, XFP_ERR_CUDA, "sweep kernel cannot be resident");
   int grid = std::min(maxg, g.ntiles);
+  const bool timed = op != SWEEP_FACTOR && ctx->sweep_ev_used + 2 <= (int)ctx->sweep_ev.size();
+  if (timed) cudaEventRecord(ctx->sweep_ev[ctx->sweep_ev_used], ctx->stream);
   XFP_CUDA(ctx, sweep_launch(op, g, d, ctx->nw, grid, ctx->stream));
+  if (timed) {
+    cudaEventRecord(ctx->sweep_ev[ctx->sweep_ev_used + 1], ctx->stream);
+    ctx->sweep_ev_used += 2;
+  }
   return XFP_OK;
+}
+
+// Sum of the timed sweep durations (after the stream has been synchronised).
+double sweep_ms(xfp_ctx* ctx, int* n) {
+  double tot = 0;
+  int cnt = 0;
+  for (int q = 0; q + 1 < ctx->sweep_ev_used; q += 2) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ctx->sweep_ev[q], ctx->sweep_ev[q + 1]) == cudaSuccess) {
+      tot += ms;
+      ++cnt;
+    }
+  }
+  *n = cnt;
+  return tot;
 }
 
 int check_sweep_error(xfp_ctx* ctx) {
@@ -342,6 +368,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
   cudaStream_t st = ctx->stream;
   int rc;
   ev_record(ctx, 0);
+  ctx->sweep_ev_used = 0;
   if ((rc = build_layout(ctx, dmat, ni, nj, nk)) != XFP_OK) return rc;
   if ((rc = ensure_compact(ctx, prec)) != XFP_OK) return rc;
   const Line* lines = ctx->lines.as<Line>();
@@ -517,6 +544,10 @@ void fill_stats(xfp_ctx* ctx, xfp_stats* s, int status, double ms_total) {
   const double cells = (double)ctx->ni * ctx->nj * ctx->nk;
   s->bytes = bytes_per_row_iter(ctx->opt.precision) * (double)ctx->rows * ctx->iters + 33.0 * cells +
              24.0 * (double)ctx->rows + 29.0 * cells;
+  int n = 0;
+  s->ms_sweeps = sweep_ms(ctx, &n);
+  s->sweeps = n;
+  s->launches = g_kernel_launches - ctx->launches;
 }
 
 template <typename IOT>
@@ -530,6 +561,7 @@ int project_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* 
     return fail(ctx, XFP_ERR_ARGS, "face weights: pass all three or none");
   if (!do_apply && !pressure) return fail(ctx, XFP_ERR_ARGS, "pressure output is NULL");
   XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  ctx->launches = g_kernel_launches;
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
@@ -627,6 +659,7 @@ int backward_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, cons
   if ((wu == nullptr) != (wv == nullptr) || (wu == nullptr) != (ww == nullptr))
     return fail(ctx, XFP_ERR_ARGS, "face weights: pass all three or none");
   XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  ctx->launches = g_kernel_launches;
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
@@ -836,6 +869,8 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
     ctx->own_stream = true;
   }
   for (auto& e : ctx->ev) cudaEventCreate(&e);
+  ctx->sweep_ev.resize(2048);
+  for (auto& e : ctx->sweep_ev) cudaEventCreate(&e);
   if (getenv("XFP_TRACE")) {
     ctx->tracing = true;
     ctx->trace.ensure(1024 * 40 * 4 * sizeof(int));
@@ -865,6 +900,8 @@ int xfp_destroy(xfp_ctx* ctx) {
   for (auto& b : ctx->F32) b.release();
   for (auto& b : ctx->L32) b.release();
   for (auto& e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : ctx->sweep_ev)
     if (e) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -10,6 +10,10 @@ namespace xfp {
 
 enum { SWEEP_FACTOR = 0, SWEEP_FWD = 1, SWEEP_BWD = 2 };
 
+// Kernels launched by this library in this process (every launcher adds its
+// launches); a call reports the difference across its own work.
+extern long long g_kernel_launches;
+
 // Static description of one sweep launch (tiles, progress words, control).
 struct SweepGrid {
   int ni, nj, nk, NJt, NKt, ntiles, maxT;

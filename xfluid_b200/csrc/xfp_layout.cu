@@ -142,11 +142,15 @@ cudaError_t layout_build(const uint8_t* mat, int ni, int nj, int nk, int tile_k,
                          cudaStream_t st) {
   const long long nlines = (long long)nj * nk;
   const int wpb = 8;
+  ++g_kernel_launches;
   line_span_kernel<<<(unsigned)((nlines + wpb - 1) / wpb), wpb * 32, 0, st>>>(mat, ni, nj, nk, L.lines,
                                                                               L.line_len_scan);
+  ++g_kernel_launches;
   line_scan_kernel<<<1, 1024, 0, st>>>(L.lines, L.line_len_scan, nlines, L.counters);
   const int NJt = (nj + 31) / 32, NKt = (nk + tile_k - 1) / tile_k;
+  ++g_kernel_launches;
   tile_active_kernel<<<NJt * NKt, 256, 0, st>>>(L.lines, nj, nk, tile_k, NJt, NKt, L.tile_active);
+  ++g_kernel_launches;
   tile_order_kernel<<<1, 32, 0, st>>>(L.tile_active, NJt, NKt, L.tiles, L.counters);
   return cudaGetLastError();
 }

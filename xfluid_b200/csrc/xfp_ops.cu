@@ -15,7 +15,7 @@
 
 namespace xfp {
 
-constexpr int RED_THREADS = 256;
+long long g_kernel_launches = 0;
 
 __device__ __forceinline__ size_t uix(int ni, int nj, int i, int j, int k) {
   return ((size_t)k * nj + j) * (size_t)(ni + 1) + i;
@@ -135,6 +135,7 @@ cudaError_t assemble(const uint8_t* mat, const FT* u, const FT* v, const FT* w, 
   const long long nlines = (long long)nj * nk;
   long long blocks = (nlines + 7) / 8;
   if (blocks > 65535 * 8) blocks = 65535 * 8;
+  ++g_kernel_launches;
   assemble_kernel<FT, AT><<<(unsigned)blocks, 256, 0, st>>>(mat, u, v, w, wu, wv, ww, ni, nj, nk, lines,
                                                           diag, ax, ay, az, b);
   return cudaGetLastError();
@@ -178,6 +179,7 @@ cudaError_t scatter_dense(const T* x, const Line* lines, int ni, int nj, int nk,
                           cudaStream_t st) {
   size_t n = (size_t)ni * nj * nk;
   unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32);
+  ++g_kernel_launches;
   scatter_dense_kernel<T><<<blocks, 256, 0, st>>>(x, lines, ni, nj, nk, dense);
   return cudaGetLastError();
 }
@@ -204,6 +206,7 @@ cudaError_t gather_compact(const T* dense, const Line* lines, int ni, int nj, in
                            cudaStream_t st) {
   const long long nlines = (long long)nj * nk;
   long long blocks = std::min<long long>((nlines + 7) / 8, 65535LL * 8);
+  ++g_kernel_launches;
   gather_compact_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(dense, lines, ni, nj, nk, x);
   return cudaGetLastError();
 }
@@ -274,6 +277,7 @@ cudaError_t apply_pressure(const uint8_t* mat, const FT* wu, const FT* wv, const
   for (int axis = 0; axis < 3; ++axis) {
     size_t n = (size_t)(ni + (axis == 0)) * (nj + (axis == 1)) * (nk + (axis == 2));
     unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32);
+    ++g_kernel_launches;
     apply_kernel<FT, PT><<<blocks, 256, 0, st>>>(mat, axis == 0 ? wu : axis == 1 ? wv : ww, p, ni, nj, nk,
                                                 axis, axis == 0 ? u : axis == 1 ? v : w);
   }
@@ -564,6 +568,7 @@ cudaError_t spmv_dot(const AT* diag, const AT* ax, const AT* ay, const AT* az, c
   (void)M;
   const long long nlines = (long long)nj * nk;
   int blocks = (int)std::min<long long>((nlines + 7) / 8, (long long)nblk_max);
+  ++g_kernel_launches;
   spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(diag, ax, ay, az, s, z, lines, ni, nj, nk, sc,
                                                      partials, mode);
   return cudaGetLastError();
@@ -623,6 +628,7 @@ cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgSc
                       double* partials, int nblk_max, cudaStream_t st) {
   int blocks = (int)std::min<long long>((M + 255) / 256, (long long)nblk_max);
   if (blocks < 1) blocks = 1;
+  ++g_kernel_launches;
   update_xr_kernel<VT><<<blocks, 256, 0, st>>>(x, r, s, z, M, sc, partials);
   return cudaGetLastError();
 }
@@ -646,6 +652,7 @@ template <typename VT>
 cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st) {
   int blocks = (int)std::min<long long>((M + 255) / 256, 148LL * 16);
   if (blocks < 1) blocks = 1;
+  ++g_kernel_launches;
   update_s_kernel<VT><<<blocks, 256, 0, st>>>(s, z, M, sc);
   return cudaGetLastError();
 }
@@ -681,6 +688,7 @@ cudaError_t absmax_init(const VT* b, long long M, PcgScalars* sc, double* partia
                         double tol, int maxit, cudaStream_t st) {
   int blocks = (int)std::min<long long>((M + 255) / 256, (long long)nblk_max);
   if (blocks < 1) blocks = 1;
+  ++g_kernel_launches;
   absmax_init_kernel<VT><<<blocks, 256, 0, st>>>(b, M, sc, partials, tol, maxit);
   return cudaGetLastError();
 }
@@ -698,6 +706,7 @@ template <typename A, typename B>
 cudaError_t convert(const A* in, B* out, long long n, cudaStream_t st) {
   int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
   if (blocks < 1) blocks = 1;
+  ++g_kernel_launches;
   convert_kernel<A, B><<<blocks, 256, 0, st>>>(in, out, n);
   return cudaGetLastError();
 }
@@ -772,6 +781,7 @@ cudaError_t residual64(const double* diag, const double* ax, const double* ay, c
   (void)M;
   const long long nlines = (long long)nj * nk;
   int blocks = (int)std::min<long long>((nlines + 7) / 8, (long long)nblk_max);
+  ++g_kernel_launches;
   residual64_kernel<<<blocks, 256, 0, st>>>(diag, ax, ay, az, b, x, r, lines, ni, nj, nk, sc, partials);
   return cudaGetLastError();
 }
@@ -783,6 +793,7 @@ __global__ void refine_update_kernel(double* __restrict__ x64, const float* __re
 cudaError_t refine_update(double* x64, const float* e32, long long M, cudaStream_t st) {
   int blocks = (int)std::min<long long>((M + 255) / 256, 148LL * 16);
   if (blocks < 1) blocks = 1;
+  ++g_kernel_launches;
   refine_update_kernel<<<blocks, 256, 0, st>>>(x64, e32, M);
   return cudaGetLastError();
 }

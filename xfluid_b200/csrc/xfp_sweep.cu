@@ -776,6 +776,7 @@ static cudaError_t launch_nw(const SweepGrid& g, const SweepData<VT, IT, CT>& d,
   cfg.stream = st;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  ++g_kernel_launches;
   return cudaLaunchKernelEx(&cfg, sweep_kernel<OP, VT, IT, CT, NW>, g, d);
 }
 
