@@ -65,7 +65,7 @@ typedef struct xfp_options {
   double timeout_ms;     /* bound on any device-side wait (0: 2000 ms) */
   int max_refine;        /* mixed: iterative-refinement cycles (0: 20) */
   double inner_tol;      /* mixed: relative residual reduction per cycle (0: 1e-4) */
-  int tile_k;            /* sweep tile height in k-lines (0: default) */
+  int tile_k;            /* sweep tile height in k-lines: 8 or 16 (0: 8) */
   void* stream;          /* cudaStream_t to run on; NULL: the context's own stream */
 } xfp_options;
 

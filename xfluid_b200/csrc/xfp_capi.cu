@@ -75,7 +75,7 @@ struct xfp_ctx {
   DevBuf ctl, scal, scal2, partials, tpartials, sy, sz, trace;
   bool tracing = false;
   // sizes of the current layout
-  int ni = 0, nj = 0, nk = 0, NJt = 0, NKt = 0, nw = 16;
+  int ni = 0, nj = 0, nk = 0, NJt = 0, NKt = 0, nw = 8;
   long long M = 0, rows = 0, nlines_act = 0, ntiles = 0;
   PcgScalars host_sc{};
   // stats
@@ -825,7 +825,7 @@ void xfp_default_options(xfp_options* o) {
   o->timeout_ms = 2000.0;
   o->max_refine = 20;
   o->inner_tol = 1e-6;
-  o->tile_k = 16;
+  o->tile_k = 8;
   o->stream = nullptr;
 }
 
@@ -848,7 +848,7 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
   if (rc) { delete ctx; return rc; }
   ctx->opt = o;
   ctx->device = o.device;
-  ctx->nw = o.tile_k ? o.tile_k : 16;
+  ctx->nw = o.tile_k ? o.tile_k : 8;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     delete ctx;
@@ -916,7 +916,7 @@ int xfp_set_options(xfp_ctx* ctx, const xfp_options* opt) {
   void* keep_stream = ctx->opt.stream;
   ctx->opt = *opt;
   ctx->opt.stream = keep_stream;
-  int nw = opt->tile_k ? opt->tile_k : 16;
+  int nw = opt->tile_k ? opt->tile_k : 8;
   ctx->nw = nw;
   return XFP_OK;
 }
