@@ -168,6 +168,31 @@ int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* materi
                      double* b, double* inv, double* lx, double* ly, double* lz,
                      double* y, double* z, double* q);
 
+/* |b|_inf of the pressure system's right-hand side -- the same value
+ * xfp_solve_f64 reports as stats.b_inf -- computed without allocating any
+ * device memory.  This entry point has no counterpart in the reference.  It is
+ * for callers that must not call cudaMalloc/cudaFree: a real-time loop that
+ * cannot afford cudaFree's device-wide synchronisation, or an application
+ * whose own allocator has reserved the device's memory.  No context is
+ * needed.
+ *
+ * All arrays, including the output b_inf (one double), are device (or managed)
+ * memory on the current device; host pointers are rejected.  The kernel runs
+ * asynchronously on `stream` (NULL: the default stream); *b_inf is ready when
+ * the stream's work completes.  Its only scratch is one fixed 128 KiB
+ * __device__ array per GPU (held from the moment the library's device code is
+ * loaded on that GPU until the process exits), so grids above 268,435,456
+ * cells are rejected with XFP_ERR_ARGS.  Calls share that array: calls whose
+ * kernels may overlap on the GPU (different streams or threads) race and must
+ * be serialised by the caller.  The first call on a device looks up the
+ * array's device address and clears it synchronously; make that first call
+ * before any stream capture begins.  On error a message goes to err (up to
+ * err_len bytes, may be NULL). */
+int xfp_rhs_inf_noalloc_f64(int ni, int nj, int nk, const uint8_t* material,
+                            const double* u, const double* v, const double* w,
+                            const double* wu, const double* wv, const double* ww,
+                            double* b_inf, void* stream, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,7 +73,7 @@ EXPORTS = [
     "xfp_default_options", "xfp_create", "xfp_destroy", "xfp_set_options", "xfp_last_error",
     "xfp_version", "xfp_solve_f64", "xfp_solve_f32", "xfp_apply_pressure_f64",
     "xfp_apply_pressure_f32", "xfp_project_f64", "xfp_project_f32", "xfp_project_backward_f64",
-    "xfp_project_backward_f32", "xfp_debug_stages",
+    "xfp_project_backward_f32", "xfp_debug_stages", "xfp_rhs_inf_noalloc_f64",
 ]
 
 
@@ -105,6 +105,7 @@ def load() -> C.CDLL:
     L.xfp_project_backward_f64.argtypes = dims + [vp] * 9 + [C.POINTER(XfpStats)]
     L.xfp_project_backward_f32.argtypes = dims + [vp] * 9 + [C.POINTER(XfpStats)]
     L.xfp_debug_stages.argtypes = dims + [vp] * 19
+    L.xfp_rhs_inf_noalloc_f64.argtypes = [C.c_int] * 3 + [vp] * 9 + [C.c_char_p, C.c_size_t]
     for name in EXPORTS:
         f = getattr(L, name)
         if name not in ("xfp_default_options", "xfp_last_error", "xfp_version"):
