@@ -116,9 +116,6 @@ __device__ __forceinline__ void st_gpu64(unsigned long long* p, unsigned long lo
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v));
 }
 
-__device__ __forceinline__ void prefetch_l2(const void* p) {
-  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
 
 struct Spin {
   long long n = 0;
@@ -183,8 +180,8 @@ struct OpTraits {
   static constexpr int P = Words<X>::P;
   static constexpr int RING = 32 / P;   // intra-CTA ring depth (steps)
   static constexpr int LRING = 64 / P;  // loader ring depth (steps)
-  static constexpr int LB = 16 / P;     // loader batch (steps fetched per round trip)
-  static constexpr int PF = (sizeof(VT) == 4 && OP != SWEEP_FACTOR) ? 8 : 4;  // cell prefetch depth (steps)
+  static constexpr int LB = 8 / P;      // loader batch (steps polled together)
+  static constexpr int PF = 4;  // cell prefetch depth (steps)
   static_assert(RING > QPUB, "ring must be deeper than the progress interval");
   static_assert(LRING >= LB + QPUB - 1, "loader ring too shallow");
 };
@@ -197,8 +194,16 @@ __host__ __device__ constexpr size_t smem_bytes(int nw) {
          sizeof(int) * (4 * (size_t)nw + 8) + sizeof(double) * (nw + 2);
 }
 
+// Two CTAs per SM where the register budget allows it (tile height 8): a
+// 256^3 grid has more tiles than SMs, and a second co-resident CTA also gives
+// each scheduler more warps to hide the step's dependency chain.
+template <int NW>
+struct SweepOcc {
+  static constexpr int MIN_BLOCKS = NW <= 8 ? 2 : 1;
+};
+
 template <int OP, typename VT, typename IT, typename CT, int NW>
-__global__ void __launch_bounds__((NW + 1) * 32, 1)
+__global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
     sweep_kernel(SweepGrid g, SweepData<VT, IT, CT> d) {
   using TR = OpTraits<OP, VT, IT, CT>;
   using X = typename TR::X;
@@ -316,25 +321,11 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
         cd.inv = IT(0);
         cd.dg = cd.upx = cd.upy = cd.upz = CT(0);
         cd.cyup = cd.czup = -1;
-        // L2 prefetch of the lane's line data LOOK steps further on: the lines
-        // are then L2-resident when the register pipeline loads them.
-        constexpr int LOOK = 32;
-        const int ip = i + LOOK * di;
-        const bool inp = (unsigned)(ip - L.lo) < (unsigned)L.len;
-        const int cp = inp ? L.off + (ip - L.lo) : 0;
         if constexpr (OP == SWEEP_FWD) {
           cd.r = d.r[c]; cd.lx = d.lx[c]; cd.ly = d.ly[c]; cd.lz = d.lz[c]; cd.inv = d.inv[c];
-          if (inp) {
-            prefetch_l2(d.r + cp); prefetch_l2(d.lx + cp); prefetch_l2(d.ly + cp);
-            prefetch_l2(d.lz + cp); prefetch_l2(d.inv + cp);
-          }
         } else if constexpr (OP == SWEEP_BWD) {
           cd.r = d.y[c]; cd.lx = d.lx[c]; cd.ly = d.ly[c]; cd.lz = d.lz[c]; cd.inv = d.inv[c];
           cd.rr = d.r[c];
-          if (inp) {
-            prefetch_l2(d.y + cp); prefetch_l2(d.lx + cp); prefetch_l2(d.ly + cp);
-            prefetch_l2(d.lz + cp); prefetch_l2(d.inv + cp); prefetch_l2(d.r + cp);
-          }
         } else {
           cd.dg = d.diag[c];
           const bool hx = in && (i + 1 - L.lo < L.len);
@@ -577,100 +568,81 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
           }
           trace_wait(g, 0, base);
         }
-        // Wait until the producers have published the LAST step of the batch
-        // this lane needs (they publish in step order), so the whole batch is
-        // fetched with one more round trip instead of one round trip per step.
-        {
-          int lj = INT_MIN, lk = INT_MIN;
-          const int bhi = min(base + LB - 1, tileHi);
-          if (lane < NW && Sj_lo <= Sj_hi) lj = min(bhi, Sj_hi) >= max(base, Sj_lo) ? min(bhi, Sj_hi) : INT_MIN;
-          if (Sk_lo <= Sk_hi) lk = min(bhi, Sk_hi) >= max(base, Sk_lo) ? min(bhi, Sk_hi) : INT_MIN;
-          if (lj != INT_MIN) {
-            const int ij = REV ? (maxT - lj) - sj_c : lj - sj_c;
-            const unsigned long long* a = &d.sy[(size_t)(Ljs.off + (ij - Ljs.lo)) * P + (P - 1)];
-            unsigned long long v = ld_gpu64(a);
-            if ((uint32_t)(v >> 32) != gen) {
-              trace_wait(g, 8, lj);
-              Spin s2;
-              do {
-                if (!s2.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 8, tpos, lj, OP, v, gen); break; }
-                v = ld_gpu64(a);
-              } while ((uint32_t)(v >> 32) != gen);
-              trace_wait(g, 0, lj);
-            }
-          }
-          if (lk != INT_MIN) {
-            const int ik = REV ? (maxT - lk) - sk_c : lk - sk_c;
-            const unsigned long long* a = &d.sz[(size_t)(Lks.off + (ik - Lks.lo)) * P + (P - 1)];
-            unsigned long long v = ld_gpu64(a);
-            if ((uint32_t)(v >> 32) != gen) {
-              trace_wait(g, 9, lk);
-              Spin s2;
-              do {
-                if (!s2.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 9, tpos, lk, OP, v, gen); break; }
-                v = ld_gpu64(a);
-              } while ((uint32_t)(v >> 32) != gen);
-              trace_wait(g, 0, lk);
-            }
-          }
-        }
-        // issue the batch's loads, then poll until every stamp is current
+        // Issue the whole batch's loads, then forward every step to the rings
+        // as soon as its stamps are current: each poll round re-issues the
+        // loads of all steps still missing (all in flight together) and
+        // forwards the ready prefix, so a step reaches the compute warps one
+        // round trip after its producer published it, and a round trip can
+        // deliver a whole batch.  The source cell of step base+q lies q cells
+        // further along the source line (backward: q cells back).
+        const int ij0 = REV ? (maxT - base) - sj_c : base - sj_c;
+        const int ik0 = REV ? (maxT - base) - sk_c : base - sk_c;
+        const int cj0 = Ljs.off + (ij0 - Ljs.lo), ck0 = Lks.off + (ik0 - Lks.lo);
+        auto needj = [&](int q) {
+          const int tau = base + q;
+          return lane < NW && tau <= tileHi && tau >= Sj_lo && tau <= Sj_hi;
+        };
+        auto needk = [&](int q) {
+          const int tau = base + q;
+          return tau <= tileHi && tau >= Sk_lo && tau <= Sk_hi;
+        };
+        auto oj = [&](int q) { return (size_t)(REV ? cj0 - q : cj0 + q) * P; };
+        auto ok_ = [&](int q) { return (size_t)(REV ? ck0 - q : ck0 + q) * P; };
         unsigned long long vj[LB][P], vk[LB][P];
-        bool needj[LB], needk[LB];
 #pragma unroll
         for (int q = 0; q < LB; ++q) {
-          const int tau = base + q;
-          needj[q] = lane < NW && tau <= tileHi && tau >= Sj_lo && tau <= Sj_hi;
-          needk[q] = tau <= tileHi && tau >= Sk_lo && tau <= Sk_hi;
-          const int ij = REV ? (maxT - tau) - sj_c : tau - sj_c;
-          const int ik = REV ? (maxT - tau) - sk_c : tau - sk_c;
-          const size_t nj_ = needj[q] ? (size_t)(Ljs.off + (ij - Ljs.lo)) : 0;
-          const size_t nk_ = needk[q] ? (size_t)(Lks.off + (ik - Lks.lo)) : 0;
 #pragma unroll
           for (int p = 0; p < P; ++p) {
-            vj[q][p] = needj[q] ? ld_gpu64(&d.sy[nj_ * P + p]) : 0ull;
-            vk[q][p] = needk[q] ? ld_gpu64(&d.sz[nk_ * P + p]) : 0ull;
+            vj[q][p] = needj(q) ? ld_gpu64(&d.sy[oj(q) + p]) : 0ull;
+            vk[q][p] = needk(q) ? ld_gpu64(&d.sz[ok_(q) + p]) : 0ull;
           }
         }
+        const int nsteps = min(LB, tileHi - base + 1);
+        int fwd = 0;   // steps of this batch already forwarded (a prefix)
+        Spin s2;
+        for (;;) {
 #pragma unroll
-        for (int q = 0; q < LB; ++q) {
-          const int tau = base + q;
-          const int ij = REV ? (maxT - tau) - sj_c : tau - sj_c;
-          const int ik = REV ? (maxT - tau) - sk_c : tau - sk_c;
+          for (int q = 0; q < LB; ++q) {
+            if (q == fwd && q < nsteps) {
+              bool rdy = true;
 #pragma unroll
-          for (int p = 0; p < P; ++p) {
-            if (needj[q] && (uint32_t)(vj[q][p] >> 32) != gen) {
-              trace_wait(g, 6, tau);
-              Spin s2;
-              const size_t n = (size_t)(Ljs.off + (ij - Ljs.lo)) * P + p;
-              do {
-                if (!s2.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 6, tpos, tau, OP, vj[q][p], gen); break; }
-                vj[q][p] = ld_gpu64(&d.sy[n]);
-              } while ((uint32_t)(vj[q][p] >> 32) != gen);
-              trace_wait(g, 0, tau);
-            }
-            if (needk[q] && (uint32_t)(vk[q][p] >> 32) != gen) {
-              trace_wait(g, 7, tau);
-              Spin s2;
-              const size_t n = (size_t)(Lks.off + (ik - Lks.lo)) * P + p;
-              do {
-                if (!s2.step(g.ctl, g.spin_limit)) { raise_timeout(g.ctl, 7, tpos, tau, OP, vk[q][p], gen); break; }
-                vk[q][p] = ld_gpu64(&d.sz[n]);
-              } while ((uint32_t)(vk[q][p] >> 32) != gen);
-              trace_wait(g, 0, tau);
+              for (int p = 0; p < P; ++p) {
+                rdy &= !needj(q) || (uint32_t)(vj[q][p] >> 32) == gen;
+                rdy &= !needk(q) || (uint32_t)(vk[q][p] >> 32) == gen;
+              }
+              if (rdy) {
+                const uint32_t st = tstamp | (base + q);
+                const int slot = (base + q) & (LRING - 1);
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                  if (lane < NW)
+                    st_vol64(&jring[((size_t)slot * P + p) * NW + lane],
+                             stamped(st, needj(q) ? (uint32_t)vj[q][p] : 0u));
+                  st_vol64(&kring[((size_t)slot * P + p) * 32 + lane],
+                           stamped(st, needk(q) ? (uint32_t)vk[q][p] : 0u));
+                }
+                fwd = q + 1;
+              }
             }
           }
-          if (tau <= tileHi) {
-            const uint32_t st = tstamp | tau;
-            const int slot = tau & (LRING - 1);
+          if (fwd >= nsteps) break;
+          if (!s2.step(g.ctl, g.spin_limit)) {
+            raise_timeout(g.ctl, 6, tpos, base + fwd, OP, 0ull, gen);
+            break;
+          }
+          trace_wait(g, 6, base + fwd);
 #pragma unroll
-            for (int p = 0; p < P; ++p) {
-              if (lane < NW)
-                st_vol64(&jring[((size_t)slot * P + p) * NW + lane], stamped(st, needj[q] ? (uint32_t)vj[q][p] : 0u));
-              st_vol64(&kring[((size_t)slot * P + p) * 32 + lane], stamped(st, needk[q] ? (uint32_t)vk[q][p] : 0u));
+          for (int q = 0; q < LB; ++q) {
+            if (q >= fwd) {
+#pragma unroll
+              for (int p = 0; p < P; ++p) {
+                if (needj(q) && (uint32_t)(vj[q][p] >> 32) != gen) vj[q][p] = ld_gpu64(&d.sy[oj(q) + p]);
+                if (needk(q) && (uint32_t)(vk[q][p] >> 32) != gen) vk[q][p] = ld_gpu64(&d.sz[ok_(q) + p]);
+              }
             }
           }
         }
+        trace_wait(g, 0, base + fwd);
       }
     }
 
