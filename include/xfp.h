@@ -65,7 +65,7 @@ typedef struct xfp_options {
   double timeout_ms;     /* bound on any device-side wait (0: 2000 ms) */
   int max_refine;        /* mixed: iterative-refinement cycles (0: 20) */
   double inner_tol;      /* mixed: relative residual reduction per cycle (0: 1e-4) */
-  int tile_k;            /* sweep tile height in k-lines: 8 or 16 (0: 8) */
+  int tile_k;            /* sweep tile height in k-lines: 8 or 16 (0: 8 for one scene, timed per batch shape for batches) */
   void* stream;          /* cudaStream_t to run on; NULL: the context's own stream */
 } xfp_options;
 
@@ -88,6 +88,7 @@ typedef struct xfp_stats {
   double ms_sweeps;      /* device time of the MIC(0) triangular-solve sweeps (CUDA events) */
   int sweeps;            /* triangular-solve sweep launches timed in ms_sweeps */
   long long launches;    /* device kernels launched by this call */
+  int tile_k;            /* sweep tile height the call used (k-lines) */
 } xfp_stats;
 
 /* Fills opt with defaults: tol 1e-5, max_iter 100, omega 0.97, ratio 0.25 --
@@ -149,6 +150,34 @@ int xfp_project_backward_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t
                              const float* wu, const float* wv, const float* ww,
                              const float* gu, const float* gv, const float* gw,
                              float* du, float* dv, float* dw, xfp_stats* stats);
+
+/* One scene of a batch.  Arrays have the shapes and layout described at the top
+ * of this header; the element type is float for xfp_project_batch_f32 and
+ * double for xfp_project_batch_f64.  u, v, w are updated in place; wu/wv/ww
+ * are optional (all three or none); pressure is optional output. */
+typedef struct xfp_scene {
+  int ni, nj, nk;
+  const uint8_t* material;
+  void* u;
+  void* v;
+  void* w;
+  const void* wu;
+  const void* wv;
+  const void* ww;
+  void* pressure;
+} xfp_scene;
+
+/* Projects n independent scenes of (possibly) different sizes together: each
+ * scene is solved exactly as xfp_project_* solves it alone (its own
+ * tolerance test, iteration count and PCG scalars), but the MIC(0) sweeps of
+ * all scenes run in one persistent launch and the PCG iteration is replayed
+ * as a CUDA graph.  No reference counterpart: xFluid projects one grid per
+ * call (FluidSimulator.cpp:501-509).  With options.tile_k == 0 the sweep tile
+ * height is picked per batch shape by timing both heights on the first call
+ * (cached in the context).  stats, if not NULL, receives n entries.  Returns
+ * XFP_OK when every scene converged, XFP_NOT_CONVERGED when one did not. */
+int xfp_project_batch_f32(xfp_ctx* ctx, int n, const xfp_scene* scenes, xfp_stats* stats);
+int xfp_project_batch_f64(xfp_ctx* ctx, int n, const xfp_scene* scenes, xfp_stats* stats);
 
 /* Diagnostics: runs the internal stages on one scene and returns them on the
  * dense grid (ni*nj*nk doubles each; any output may be NULL), in the

@@ -40,6 +40,17 @@ class XfpOptions(C.Structure):
     ]
 
 
+class XfpScene(C.Structure):
+    """xfp_scene: one scene of xfp_project_batch_{f32,f64}."""
+    _fields_ = [
+        ("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int),
+        ("material", C.c_void_p),
+        ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p),
+        ("wu", C.c_void_p), ("wv", C.c_void_p), ("ww", C.c_void_p),
+        ("pressure", C.c_void_p),
+    ]
+
+
 class XfpStats(C.Structure):
     _fields_ = [
         ("status", C.c_int),
@@ -60,6 +71,7 @@ class XfpStats(C.Structure):
         ("ms_sweeps", C.c_double),
         ("sweeps", C.c_int),
         ("launches", C.c_longlong),
+        ("tile_k", C.c_int),
     ]
 
     def as_dict(self) -> dict:
@@ -74,6 +86,7 @@ EXPORTS = [
     "xfp_version", "xfp_solve_f64", "xfp_solve_f32", "xfp_apply_pressure_f64",
     "xfp_apply_pressure_f32", "xfp_project_f64", "xfp_project_f32", "xfp_project_backward_f64",
     "xfp_project_backward_f32", "xfp_debug_stages", "xfp_rhs_inf_noalloc_f64",
+    "xfp_project_batch_f32", "xfp_project_batch_f64",
 ]
 
 
@@ -105,6 +118,8 @@ def load() -> C.CDLL:
     L.xfp_project_backward_f64.argtypes = dims + [vp] * 9 + [C.POINTER(XfpStats)]
     L.xfp_project_backward_f32.argtypes = dims + [vp] * 9 + [C.POINTER(XfpStats)]
     L.xfp_debug_stages.argtypes = dims + [vp] * 19
+    L.xfp_project_batch_f32.argtypes = [vp, C.c_int, C.POINTER(XfpScene), C.POINTER(XfpStats)]
+    L.xfp_project_batch_f64.argtypes = [vp, C.c_int, C.POINTER(XfpScene), C.POINTER(XfpStats)]
     L.xfp_rhs_inf_noalloc_f64.argtypes = [C.c_int] * 3 + [vp] * 9 + [C.c_char_p, C.c_size_t]
     for name in EXPORTS:
         f = getattr(L, name)

@@ -18,92 +18,12 @@
 
 #include "../../include/xfp.h"
 #include "xfp_common.cuh"
+#include "xfp_context.h"
 #include "xfp_kernels.h"
 
 using namespace xfp;
 
-namespace {
-
-constexpr int NBLK_MAX = 148 * 8;   // blocks of the reduction kernels (partials slots)
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t cap = 0;
-  cudaError_t ensure(size_t bytes) {
-    if (bytes <= cap && p) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-    size_t want = std::max<size_t>(bytes, 256);
-    cudaError_t e = cudaMalloc(&p, want);
-    if (e == cudaSuccess) cap = want;
-    return e;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-  }
-  template <typename T>
-  T* as() const { return reinterpret_cast<T*>(p); }
-};
-
-struct Timer {
-  cudaEvent_t ev[6] = {};
-};
-
-}  // namespace
-
-struct xfp_ctx {
-  xfp_options opt;
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  std::string err;
-  int nsm = 148;
-  // I/O staging (host-pointer mode)
-  DevBuf io_mat, io_u, io_v, io_w, io_wu, io_wv, io_ww, io_p, io_gu, io_gv, io_gw;
-  // layout
-  DevBuf lines, lens, tile_active, tiles, counters;
-  // compact arrays
-  DevBuf A64[5];                  // diag, ax, ay, az, b (FP64)
-  DevBuf A32[5];                  // same in FP32
-  DevBuf F64[6], F32[6];          // factor scratch: L and missing per direction
-  DevBuf inv64, inv32, L32[3];
-  DevBuf x64, r64, x32, r32, s32, z32, s64, z64, dense;
-  // control
-  DevBuf ctl, scal, scal2, partials, tpartials, sy, sz, trace;
-  bool tracing = false;
-  // sizes of the current layout
-  int ni = 0, nj = 0, nk = 0, NJt = 0, NKt = 0, nw = 8;
-  long long M = 0, rows = 0, nlines_act = 0, ntiles = 0;
-  PcgScalars host_sc{};
-  // stats
-  double ms_setup = 0, ms_factor = 0, ms_solve = 0, ms_apply = 0;
-  int iters = 0, refinements = 0;
-  double res = 0, bnorm = 0;
-  cudaEvent_t ev[8] = {};
-  // device timing of the triangular-solve sweeps (pairs of events, read at the end)
-  std::vector<cudaEvent_t> sweep_ev;
-  int sweep_ev_used = 0;
-  long long launches = 0;
-};
-
-namespace {
-
-int fail(xfp_ctx* ctx, int code, const std::string& msg) {
-  if (ctx) ctx->err = msg;
-  return code;
-}
-
-#define XFP_CUDA(ctx, call)                                                                    \
-  do {                                                                                         \
-    cudaError_t _e = (call);                                                                   \
-    if (_e != cudaSuccess) {                                                                   \
-      return fail(ctx, _e == cudaErrorMemoryAllocation ? XFP_ERR_NOMEM : XFP_ERR_CUDA,         \
-                  std::string(#call) + ": " + cudaGetErrorString(_e));                         \
-    }                                                                                          \
-  } while (0)
+namespace xfp_host {
 
 size_t ncells(int ni, int nj, int nk) { return (size_t)ni * nj * nk; }
 size_t nu(int ni, int nj, int nk) { return (size_t)(ni + 1) * nj * nk; }
@@ -115,16 +35,6 @@ long long spin_limit(const xfp_ctx* ctx) {
   return (long long)std::max(1e4, ms * 4000.0);  // ~250 ns per backed-off poll
 }
 
-// Stage an input array on the device (or use it in place).
-template <typename T>
-int stage_in(xfp_ctx* ctx, DevBuf& buf, const T* src, size_t n, const T** dev) {
-  if (src == nullptr) { *dev = nullptr; return XFP_OK; }
-  if (ctx->opt.device_pointers) { *dev = src; return XFP_OK; }
-  XFP_CUDA(ctx, buf.ensure(n * sizeof(T)));
-  XFP_CUDA(ctx, cudaMemcpyAsync(buf.p, src, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
-  *dev = buf.as<T>();
-  return XFP_OK;
-}
 
 int check_dims(xfp_ctx* ctx, int ni, int nj, int nk, const void* mat) {
   if (!ctx) return XFP_ERR_ARGS;
@@ -548,6 +458,7 @@ void fill_stats(xfp_ctx* ctx, xfp_stats* s, int status, double ms_total) {
   s->ms_sweeps = sweep_ms(ctx, &n);
   s->sweeps = n;
   s->launches = g_kernel_launches - ctx->launches;
+  s->tile_k = ctx->nw;
 }
 
 template <typename IOT>
@@ -804,7 +715,9 @@ int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* c
   return XFP_OK;
 }
 
-}  // namespace
+}  // namespace xfp_host
+
+using namespace xfp_host;
 
 // ============================================================================ C ABI
 extern "C" {
@@ -825,7 +738,7 @@ void xfp_default_options(xfp_options* o) {
   o->timeout_ms = 2000.0;
   o->max_refine = 20;
   o->inner_tol = 1e-6;
-  o->tile_k = 8;
+  o->tile_k = 0;
   o->stream = nullptr;
 }
 
@@ -894,6 +807,8 @@ int xfp_destroy(xfp_ctx* ctx) {
                    &ctx->r64, &ctx->x32, &ctx->r32, &ctx->s32, &ctx->z32, &ctx->s64, &ctx->z64, &ctx->dense,
                    &ctx->sy, &ctx->sz, &ctx->ctl, &ctx->scal, &ctx->scal2, &ctx->partials, &ctx->tpartials};
   for (DevBuf* b : all) b->release();
+  batch_state_free(ctx->batch);
+  ctx->batch = nullptr;
   for (auto& b : ctx->A64) b.release();
   for (auto& b : ctx->A32) b.release();
   for (auto& b : ctx->F64) b.release();

@@ -37,6 +37,19 @@ struct SweepCtl {
   unsigned int err_expect, err_pad;
 };
 
+// One scene of a batch: its grid, its slice [base, base+M) of the compact
+// arrays, its line table (offsets already global) and the blocks the vector
+// kernels give it (line-based and cell-based grids, consecutive per scene).
+struct BatchSeg {
+  int ni, nj, nk;
+  int blk_lines, blk_lines_start;   // line-based kernels (SpMV)
+  int blk_cells, blk_cells_start;   // cell-based kernels (updates, norms)
+  int pad;
+  long long base, M;
+  const Line* lines;
+  double* partials;                 // this scene's reduction slots
+};
+
 // Scalars of one PCG solve, resident on the device.
 struct PcgScalars {
   double rho, alpha, beta, res, tolabs, bnorm, dot_tmp;

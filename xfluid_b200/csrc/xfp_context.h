@@ -1,0 +1,117 @@
+// xfp_context.h -- the context behind xfp_ctx* and the host helpers shared by
+// the single-scene driver (xfp_capi.cu) and the batch driver (xfp_batch.cu).
+// Internal to libxfp.
+#pragma once
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/xfp.h"
+#include "xfp_common.cuh"
+#include "xfp_kernels.h"
+
+namespace xfp_host {
+
+constexpr int NBLK_MAX = 148 * 8;   // blocks of the reduction kernels (partials slots)
+
+// A device allocation that only grows.
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct BatchState;                      // xfp_batch.cu
+void batch_state_free(BatchState* b);
+
+}  // namespace xfp_host
+
+struct xfp_ctx {
+  xfp_options opt;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  int nsm = 148;
+  using DevBuf = xfp_host::DevBuf;
+  // I/O staging (host-pointer mode)
+  DevBuf io_mat, io_u, io_v, io_w, io_wu, io_wv, io_ww, io_p, io_gu, io_gv, io_gw;
+  // layout
+  DevBuf lines, lens, tile_active, tiles, counters;
+  // compact arrays
+  DevBuf A64[5];                  // diag, ax, ay, az, b (FP64)
+  DevBuf A32[5];                  // same in FP32
+  DevBuf F64[6], F32[6];          // factor scratch: L and missing per direction
+  DevBuf inv64, inv32, L32[3];
+  DevBuf x64, r64, x32, r32, s32, z32, s64, z64, dense;
+  // control
+  DevBuf ctl, scal, scal2, partials, tpartials, sy, sz, trace;
+  bool tracing = false;
+  // sizes of the current layout
+  int ni = 0, nj = 0, nk = 0, NJt = 0, NKt = 0, nw = 8;
+  long long M = 0, rows = 0, nlines_act = 0, ntiles = 0;
+  xfp::PcgScalars host_sc{};
+  // stats
+  double ms_setup = 0, ms_factor = 0, ms_solve = 0, ms_apply = 0;
+  int iters = 0, refinements = 0;
+  double res = 0, bnorm = 0;
+  cudaEvent_t ev[8] = {};
+  // device timing of the triangular-solve sweeps (pairs of events, read at the end)
+  std::vector<cudaEvent_t> sweep_ev;
+  int sweep_ev_used = 0;
+  long long launches = 0;
+  // batched scenes (xfp_project_batch_*): buffers, tables and tuning cache
+  xfp_host::BatchState* batch = nullptr;
+};
+
+namespace xfp_host {
+
+inline int fail(xfp_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+#define XFP_CUDA(ctx, call)                                                                    \
+  do {                                                                                         \
+    cudaError_t _e = (call);                                                                   \
+    if (_e != cudaSuccess) {                                                                   \
+      return ::xfp_host::fail(ctx, _e == cudaErrorMemoryAllocation ? XFP_ERR_NOMEM : XFP_ERR_CUDA, \
+                              std::string(#call) + ": " + cudaGetErrorString(_e));             \
+    }                                                                                          \
+  } while (0)
+
+// Stage an input array on the device (or use it in place).
+template <typename T>
+int stage_in(xfp_ctx* ctx, DevBuf& buf, const T* src, size_t n, const T** dev) {
+  if (src == nullptr) { *dev = nullptr; return XFP_OK; }
+  if (ctx->opt.device_pointers) { *dev = src; return XFP_OK; }
+  XFP_CUDA(ctx, buf.ensure(n * sizeof(T)));
+  XFP_CUDA(ctx, cudaMemcpyAsync(buf.p, src, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  *dev = buf.as<T>();
+  return XFP_OK;
+}
+
+// xfp_capi.cu
+long long spin_limit(const xfp_ctx* ctx);
+int check_dims(xfp_ctx* ctx, int ni, int nj, int nk, const void* mat);
+int ensure_compact(xfp_ctx* ctx, int prec);
+int check_sweep_error(xfp_ctx* ctx);
+
+}  // namespace xfp_host

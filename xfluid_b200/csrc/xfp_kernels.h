@@ -24,6 +24,12 @@ struct SweepGrid {
   long long spin_limit;
   PcgScalars* scal;             // forward/backward: skip when done; backward: rho/beta
   int* trace;                   // optional: per (block, warp) {site, step, progress, tile} while waiting
+  // Batch of scenes (null for one scene): scene of each tile, per-scene
+  // geometry and scalars.  Tiles of a converged scene are skipped, and the
+  // backward dot partials are reduced per scene by batch_bwd_reduce.
+  const int* tile_scene = nullptr;
+  const BatchSeg* segs = nullptr;
+  PcgScalars* scal_batch = nullptr;
 };
 
 // Arrays of one sweep.  VT: vector/L type of the solves, IT: invdiag type,
@@ -116,6 +122,34 @@ cudaError_t gather_compact(const T* dense, const Line* lines, int ni, int nj, in
                            cudaStream_t st);
 template <typename T>
 cudaError_t copy_vec(const T* in, T* out, long long n, cudaStream_t st);
+
+// ---- batch forms: one launch covers every scene of a batch (BatchSeg table,
+// nseg scenes, per-scene scalars sc[nseg]); grid = the table's total blocks ----
+template <typename VT, typename AT, typename DT>
+cudaError_t batch_spmv_dot(const BatchSeg* segs, int nseg, int blocks, const AT* diag, const AT* ax,
+                           const AT* ay, const AT* az, const VT* s, VT* z, PcgScalars* sc, int mode,
+                           cudaStream_t st);
+template <typename VT>
+cudaError_t batch_update_xr(const BatchSeg* segs, int nseg, int blocks, VT* x, VT* r, const VT* s,
+                            const VT* z, PcgScalars* sc, cudaStream_t st);
+template <typename VT>
+cudaError_t batch_update_s(const BatchSeg* segs, int nseg, int blocks, VT* s, const VT* z, PcgScalars* sc,
+                           cudaStream_t st);
+// tols/maxits: optional per-scene tolerance and iteration cap (else tol, maxit)
+template <typename VT>
+cudaError_t batch_absmax_init(const BatchSeg* segs, int nseg, int blocks, const VT* b, PcgScalars* sc,
+                              double tol, int maxit, const double* tols, const int* maxits, cudaStream_t st);
+cudaError_t batch_residual64(const BatchSeg* segs, int nseg, int blocks, const double* diag, const double* ax,
+                             const double* ay, const double* az, const double* b, const double* x, double* r,
+                             PcgScalars* sc, cudaStream_t st);
+// Per-scene z.r from the backward sweep's per-tile partials, summed in each
+// scene's own tile order; mode 0: rho, mode 1: beta and rho (the single-scene
+// backward epilogue).  scene_tiles lists tile positions scene by scene.
+template <typename DT>
+cudaError_t batch_bwd_reduce(int nseg, const int* scene_tile_start, const int* scene_tiles,
+                             const double* tpartials, PcgScalars* sc, int mode, cudaStream_t st);
+// Adds base[s] to the offsets of scene s's line table.
+cudaError_t offset_lines(Line* lines, long long nlines, long long base, cudaStream_t st);
 
 // Mixed precision: r64 = b64 - A64 x64, |r|_inf and r32 = (float) r64 / scale.
 cudaError_t residual64(const double* diag, const double* ax, const double* ay, const double* az,

@@ -480,17 +480,37 @@ __device__ __forceinline__ double block_max(double v, double* sh) {
   __syncthreads();
   return t;
 }
-// Returns true in thread 0 of the last block to finish.
-__device__ __forceinline__ bool last_block(PcgScalars* sc) {
+// Returns true in thread 0 of the last of nblk blocks to finish (a batch runs
+// one such group of blocks per scene, each with its own counter).
+__device__ __forceinline__ bool last_block(PcgScalars* sc, unsigned nblk) {
   __shared__ bool s_last;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     unsigned t = atomicAdd(&sc->red_count, 1u);
-    s_last = (t == gridDim.x - 1);
+    s_last = (t == nblk - 1);
   }
   __syncthreads();
   return s_last;
+}
+
+// Batch of scenes in one launch: block b belongs to the scene whose range of
+// blocks [start, start + count) holds it; the scene's blocks then run exactly
+// the decomposition a single-scene launch of `count` blocks would.
+__device__ __forceinline__ int batch_scene_of(const BatchSeg* __restrict__ segs, int nseg, bool by_lines) {
+  __shared__ int s_seg;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = nseg - 1;
+    const int b = (int)blockIdx.x;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      const int start = by_lines ? segs[mid].blk_lines_start : segs[mid].blk_cells_start;
+      if (start <= b) lo = mid; else hi = mid - 1;
+    }
+    s_seg = lo;
+  }
+  __syncthreads();
+  return s_seg;
 }
 
 // ---------------------------------------------------------------------------
@@ -500,9 +520,9 @@ __device__ __forceinline__ bool last_block(PcgScalars* sc) {
 // One warp per x-line; the warp's lanes walk the line span.
 // ---------------------------------------------------------------------------
 template <typename VT, typename AT, typename DT>
-__global__ void __launch_bounds__(256) spmv_dot_kernel(
-    const AT* __restrict__ diag, const AT* __restrict__ ax, const AT* __restrict__ ay,
-    const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
+__device__ __forceinline__ void spmv_dot_body(
+    unsigned bid, unsigned nblk, const AT* __restrict__ diag, const AT* __restrict__ ax,
+    const AT* __restrict__ ay, const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
     const Line* __restrict__ lines, int ni, int nj, int nk, PcgScalars* sc,
     DT* __restrict__ partials, int mode) {
   __shared__ DT sh[32];
@@ -510,8 +530,8 @@ __global__ void __launch_bounds__(256) spmv_dot_kernel(
   const int lane = threadIdx.x & 31;
   const long long nlines = (long long)nj * nk;
   DT acc = DT(0);
-  for (long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
-       line += (long long)gridDim.x * (blockDim.x >> 5)) {
+  for (long long line = (long long)bid * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
+       line += (long long)nblk * (blockDim.x >> 5)) {
     const Line L = lines[line];
     if (L.len == 0) continue;
     const int j = (int)(line % nj), k = (int)(line / nj);
@@ -550,16 +570,34 @@ __global__ void __launch_bounds__(256) spmv_dot_kernel(
   }
   if (mode != 0) return;
   DT t = block_sum(acc, sh);
-  if (threadIdx.x == 0) partials[blockIdx.x] = t;
-  if (last_block(sc) && threadIdx.x == 0) {
+  if (threadIdx.x == 0) partials[bid] = t;
+  if (last_block(sc, nblk) && threadIdx.x == 0) {
     DT tot = DT(0);
-    for (unsigned b = 0; b < gridDim.x; ++b) tot = add_rn(tot, ((volatile DT*)partials)[b]);
+    for (unsigned b = 0; b < nblk; ++b) tot = add_rn(tot, ((volatile DT*)partials)[b]);
     if (std::is_same<DT, float>::value)
       sc->alpha = (double)__fdiv_rn((float)sc->rho, (float)tot);
     else
       sc->alpha = __ddiv_rn(sc->rho, (double)tot);
     sc->red_count = 0;
   }
+}
+template <typename VT, typename AT, typename DT>
+__global__ void __launch_bounds__(256) spmv_dot_kernel(
+    const AT* __restrict__ diag, const AT* __restrict__ ax, const AT* __restrict__ ay,
+    const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
+    const Line* __restrict__ lines, int ni, int nj, int nk, PcgScalars* sc,
+    DT* __restrict__ partials, int mode) {
+  spmv_dot_body<VT, AT, DT>(blockIdx.x, gridDim.x, diag, ax, ay, az, s, z, lines, ni, nj, nk, sc, partials, mode);
+}
+template <typename VT, typename AT, typename DT>
+__global__ void __launch_bounds__(256) batch_spmv_dot_kernel(
+    const BatchSeg* __restrict__ segs, int nseg, const AT* __restrict__ diag, const AT* __restrict__ ax,
+    const AT* __restrict__ ay, const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
+    PcgScalars* sc, int mode) {
+  const int q = batch_scene_of(segs, nseg, true);
+  const BatchSeg& S = segs[q];
+  spmv_dot_body<VT, AT, DT>(blockIdx.x - S.blk_lines_start, S.blk_lines, diag, ax, ay, az, s, z, S.lines, S.ni,
+                            S.nj, S.nk, sc + q, reinterpret_cast<DT*>(S.partials), mode);
 }
 template <typename VT, typename AT, typename DT>
 cudaError_t spmv_dot(const AT* diag, const AT* ax, const AT* ay, const AT* az, const VT* s, VT* z,
@@ -591,26 +629,26 @@ template cudaError_t spmv_dot<float, float, double>(const float*, const float*, 
 // block decides convergence: |r|_inf <= tol*|b|_inf, or the iteration cap.
 // ---------------------------------------------------------------------------
 template <typename VT>
-__global__ void __launch_bounds__(256) update_xr_kernel(VT* __restrict__ x, VT* __restrict__ r,
-                                                        const VT* __restrict__ s,
-                                                        const VT* __restrict__ z, long long M,
-                                                        PcgScalars* sc, double* __restrict__ partials) {
+__device__ __forceinline__ void update_xr_body(unsigned bid, unsigned nblk, VT* __restrict__ x,
+                                               VT* __restrict__ r, const VT* __restrict__ s,
+                                               const VT* __restrict__ z, long long M, PcgScalars* sc,
+                                               double* __restrict__ partials) {
   __shared__ double sh[32];
   if (*(volatile int*)&sc->done) return;
   const VT alpha = (VT)sc->alpha;
   const VT nalpha = -alpha;
   double m = 0.0;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x) {
+  for (long long c = (long long)bid * blockDim.x + threadIdx.x; c < M; c += (long long)nblk * blockDim.x) {
     x[c] = add_rn(x[c], mul_rn(alpha, s[c]));
     const VT rv = add_rn(r[c], mul_rn(nalpha, z[c]));
     r[c] = rv;
     m = fmax(m, (double)fabs(rv));
   }
   double t = block_max(m, sh);
-  if (threadIdx.x == 0) partials[blockIdx.x] = t;
-  if (last_block(sc) && threadIdx.x == 0) {
+  if (threadIdx.x == 0) partials[bid] = t;
+  if (last_block(sc, nblk) && threadIdx.x == 0) {
     double tot = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) tot = fmax(tot, ((volatile double*)partials)[b]);
+    for (unsigned b = 0; b < nblk; ++b) tot = fmax(tot, ((volatile double*)partials)[b]);
     sc->res = tot;
     sc->iters += 1;
     if (tot <= sc->tolabs) {
@@ -622,6 +660,23 @@ __global__ void __launch_bounds__(256) update_xr_kernel(VT* __restrict__ x, VT* 
     }
     sc->red_count = 0;
   }
+}
+template <typename VT>
+__global__ void __launch_bounds__(256) update_xr_kernel(VT* __restrict__ x, VT* __restrict__ r,
+                                                        const VT* __restrict__ s,
+                                                        const VT* __restrict__ z, long long M,
+                                                        PcgScalars* sc, double* __restrict__ partials) {
+  update_xr_body<VT>(blockIdx.x, gridDim.x, x, r, s, z, M, sc, partials);
+}
+template <typename VT>
+__global__ void __launch_bounds__(256) batch_update_xr_kernel(const BatchSeg* __restrict__ segs, int nseg,
+                                                              VT* __restrict__ x, VT* __restrict__ r,
+                                                              const VT* __restrict__ s, const VT* __restrict__ z,
+                                                              PcgScalars* sc) {
+  const int q = batch_scene_of(segs, nseg, false);
+  const BatchSeg& S = segs[q];
+  update_xr_body<VT>(blockIdx.x - S.blk_cells_start, S.blk_cells, x + S.base, r + S.base, s + S.base,
+                     z + S.base, S.M, sc + q, S.partials);
 }
 template <typename VT, typename DT>
 cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgScalars* sc,
@@ -641,12 +696,24 @@ template cudaError_t update_xr<float, double>(float*, float*, const float*, cons
 
 // s = z + beta s  (add_scaled(beta, s, z) then swap, pcg_solver.h:280)
 template <typename VT>
-__global__ void update_s_kernel(VT* __restrict__ s, const VT* __restrict__ z, long long M,
-                                PcgScalars* sc) {
+__device__ __forceinline__ void update_s_body(unsigned bid, unsigned nblk, VT* __restrict__ s,
+                                              const VT* __restrict__ z, long long M, PcgScalars* sc) {
   if (*(volatile int*)&sc->done) return;
   const VT beta = (VT)sc->beta;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x)
+  for (long long c = (long long)bid * blockDim.x + threadIdx.x; c < M; c += (long long)nblk * blockDim.x)
     s[c] = add_rn(z[c], mul_rn(beta, s[c]));
+}
+template <typename VT>
+__global__ void update_s_kernel(VT* __restrict__ s, const VT* __restrict__ z, long long M,
+                                PcgScalars* sc) {
+  update_s_body<VT>(blockIdx.x, gridDim.x, s, z, M, sc);
+}
+template <typename VT>
+__global__ void batch_update_s_kernel(const BatchSeg* __restrict__ segs, int nseg, VT* __restrict__ s,
+                                      const VT* __restrict__ z, PcgScalars* sc) {
+  const int q = batch_scene_of(segs, nseg, false);
+  const BatchSeg& S = segs[q];
+  update_s_body<VT>(blockIdx.x - S.blk_cells_start, S.blk_cells, s + S.base, z + S.base, S.M, sc + q);
 }
 template <typename VT>
 cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st) {
@@ -661,17 +728,18 @@ template cudaError_t update_s<float>(float*, const float*, long long, PcgScalars
 
 // |b|_inf, tolerance and loop state at the start of a solve (pcg_solver.h:247-254).
 template <typename VT>
-__global__ void absmax_init_kernel(const VT* __restrict__ b, long long M, PcgScalars* sc,
-                                   double* __restrict__ partials, double tol, int maxit) {
+__device__ __forceinline__ void absmax_init_body(unsigned bid, unsigned nblk, const VT* __restrict__ b,
+                                                 long long M, PcgScalars* sc, double* __restrict__ partials,
+                                                 double tol, int maxit) {
   __shared__ double sh[32];
   double m = 0.0;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x)
+  for (long long c = (long long)bid * blockDim.x + threadIdx.x; c < M; c += (long long)nblk * blockDim.x)
     m = fmax(m, (double)fabs(b[c]));
   double t = block_max(m, sh);
-  if (threadIdx.x == 0) partials[blockIdx.x] = t;
-  if (last_block(sc) && threadIdx.x == 0) {
+  if (threadIdx.x == 0) partials[bid] = t;
+  if (last_block(sc, nblk) && threadIdx.x == 0) {
     double tot = 0.0;
-    for (unsigned q = 0; q < gridDim.x; ++q) tot = fmax(tot, ((volatile double*)partials)[q]);
+    for (unsigned q = 0; q < nblk; ++q) tot = fmax(tot, ((volatile double*)partials)[q]);
     sc->bnorm = tot;
     sc->res = tot;
     sc->tolabs = tol * tot;
@@ -682,6 +750,20 @@ __global__ void absmax_init_kernel(const VT* __restrict__ b, long long M, PcgSca
     if (tot != 0.0 && maxit <= 0) sc->status = 1;
     sc->red_count = 0;
   }
+}
+template <typename VT>
+__global__ void absmax_init_kernel(const VT* __restrict__ b, long long M, PcgScalars* sc,
+                                   double* __restrict__ partials, double tol, int maxit) {
+  absmax_init_body<VT>(blockIdx.x, gridDim.x, b, M, sc, partials, tol, maxit);
+}
+template <typename VT>
+__global__ void batch_absmax_init_kernel(const BatchSeg* __restrict__ segs, int nseg, const VT* __restrict__ b,
+                                         PcgScalars* sc, double tol, int maxit, const double* __restrict__ tols,
+                                         const int* __restrict__ maxits) {
+  const int q = batch_scene_of(segs, nseg, false);
+  const BatchSeg& S = segs[q];
+  absmax_init_body<VT>(blockIdx.x - S.blk_cells_start, S.blk_cells, b + S.base, S.M, sc + q, S.partials,
+                       tols ? tols[q] : tol, maxits ? maxits[q] : maxit);
 }
 template <typename VT>
 cudaError_t absmax_init(const VT* b, long long M, PcgScalars* sc, double* partials, int nblk_max,
@@ -724,17 +806,17 @@ template cudaError_t copy_vec<float>(const float*, float*, long long, cudaStream
 // Mixed precision: FP64 residual r = b - A x with |r|_inf (into sc->res), on
 // the FP64 copy of A; and x64 += e32 after each FP32 inner solve.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) residual64_kernel(
-    const double* __restrict__ diag, const double* __restrict__ ax, const double* __restrict__ ay,
-    const double* __restrict__ az, const double* __restrict__ b, const double* __restrict__ x,
-    double* __restrict__ r, const Line* __restrict__ lines, int ni, int nj, int nk, PcgScalars* sc,
-    double* __restrict__ partials) {
+__device__ __forceinline__ void residual64_body(
+    unsigned bid, unsigned nblk, const double* __restrict__ diag, const double* __restrict__ ax,
+    const double* __restrict__ ay, const double* __restrict__ az, const double* __restrict__ b,
+    const double* __restrict__ x, double* __restrict__ r, const Line* __restrict__ lines, int ni, int nj,
+    int nk, PcgScalars* sc, double* __restrict__ partials) {
   __shared__ double sh[32];
   const int lane = threadIdx.x & 31;
   const long long nlines = (long long)nj * nk;
   double m = 0.0;
-  for (long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
-       line += (long long)gridDim.x * (blockDim.x >> 5)) {
+  for (long long line = (long long)bid * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
+       line += (long long)nblk * (blockDim.x >> 5)) {
     const Line L = lines[line];
     if (L.len == 0) continue;
     const int j = (int)(line % nj), k = (int)(line / nj);
@@ -766,13 +848,36 @@ __global__ void __launch_bounds__(256) residual64_kernel(
     }
   }
   double t = block_max(m, sh);
-  if (threadIdx.x == 0) partials[blockIdx.x] = t;
-  if (last_block(sc) && threadIdx.x == 0) {
+  if (threadIdx.x == 0) partials[bid] = t;
+  if (last_block(sc, nblk) && threadIdx.x == 0) {
     double tot = 0.0;
-    for (unsigned q = 0; q < gridDim.x; ++q) tot = fmax(tot, ((volatile double*)partials)[q]);
+    for (unsigned q = 0; q < nblk; ++q) tot = fmax(tot, ((volatile double*)partials)[q]);
     sc->res = tot;
     sc->red_count = 0;
   }
+}
+__global__ void __launch_bounds__(256) residual64_kernel(
+    const double* __restrict__ diag, const double* __restrict__ ax, const double* __restrict__ ay,
+    const double* __restrict__ az, const double* __restrict__ b, const double* __restrict__ x,
+    double* __restrict__ r, const Line* __restrict__ lines, int ni, int nj, int nk, PcgScalars* sc,
+    double* __restrict__ partials) {
+  residual64_body(blockIdx.x, gridDim.x, diag, ax, ay, az, b, x, r, lines, ni, nj, nk, sc, partials);
+}
+__global__ void __launch_bounds__(256) batch_residual64_kernel(
+    const BatchSeg* __restrict__ segs, int nseg, const double* __restrict__ diag, const double* __restrict__ ax,
+    const double* __restrict__ ay, const double* __restrict__ az, const double* __restrict__ b,
+    const double* __restrict__ x, double* __restrict__ r, PcgScalars* sc) {
+  const int q = batch_scene_of(segs, nseg, true);
+  const BatchSeg& S = segs[q];
+  residual64_body(blockIdx.x - S.blk_lines_start, S.blk_lines, diag, ax, ay, az, b, x, r, S.lines, S.ni, S.nj,
+                  S.nk, sc + q, S.partials);
+}
+cudaError_t batch_residual64(const BatchSeg* segs, int nseg, int blocks, const double* diag, const double* ax,
+                             const double* ay, const double* az, const double* b, const double* x, double* r,
+                             PcgScalars* sc, cudaStream_t st) {
+  ++g_kernel_launches;
+  batch_residual64_kernel<<<blocks, 256, 0, st>>>(segs, nseg, diag, ax, ay, az, b, x, r, sc);
+  return cudaGetLastError();
 }
 cudaError_t residual64(const double* diag, const double* ax, const double* ay, const double* az,
                        const double* b, const double* x, double* r, const Line* lines, int ni,
@@ -783,6 +888,115 @@ cudaError_t residual64(const double* diag, const double* ax, const double* ay, c
   int blocks = (int)std::min<long long>((nlines + 7) / 8, (long long)nblk_max);
   ++g_kernel_launches;
   residual64_kernel<<<blocks, 256, 0, st>>>(diag, ax, ay, az, b, x, r, lines, ni, nj, nk, sc, partials);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Batch launchers and the per-scene reductions of a batch.
+// ---------------------------------------------------------------------------
+template <typename VT, typename AT, typename DT>
+cudaError_t batch_spmv_dot(const BatchSeg* segs, int nseg, int blocks, const AT* diag, const AT* ax,
+                           const AT* ay, const AT* az, const VT* s, VT* z, PcgScalars* sc, int mode,
+                           cudaStream_t st) {
+  ++g_kernel_launches;
+  batch_spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(segs, nseg, diag, ax, ay, az, s, z, sc, mode);
+  return cudaGetLastError();
+}
+template cudaError_t batch_spmv_dot<double, double, double>(const BatchSeg*, int, int, const double*,
+                                                            const double*, const double*, const double*,
+                                                            const double*, double*, PcgScalars*, int,
+                                                            cudaStream_t);
+template cudaError_t batch_spmv_dot<float, float, float>(const BatchSeg*, int, int, const float*, const float*,
+                                                         const float*, const float*, const float*, float*,
+                                                         PcgScalars*, int, cudaStream_t);
+template cudaError_t batch_spmv_dot<float, float, double>(const BatchSeg*, int, int, const float*, const float*,
+                                                          const float*, const float*, const float*, float*,
+                                                          PcgScalars*, int, cudaStream_t);
+
+template <typename VT>
+cudaError_t batch_update_xr(const BatchSeg* segs, int nseg, int blocks, VT* x, VT* r, const VT* s,
+                            const VT* z, PcgScalars* sc, cudaStream_t st) {
+  ++g_kernel_launches;
+  batch_update_xr_kernel<VT><<<blocks, 256, 0, st>>>(segs, nseg, x, r, s, z, sc);
+  return cudaGetLastError();
+}
+template cudaError_t batch_update_xr<double>(const BatchSeg*, int, int, double*, double*, const double*,
+                                             const double*, PcgScalars*, cudaStream_t);
+template cudaError_t batch_update_xr<float>(const BatchSeg*, int, int, float*, float*, const float*,
+                                            const float*, PcgScalars*, cudaStream_t);
+
+template <typename VT>
+cudaError_t batch_update_s(const BatchSeg* segs, int nseg, int blocks, VT* s, const VT* z, PcgScalars* sc,
+                           cudaStream_t st) {
+  ++g_kernel_launches;
+  batch_update_s_kernel<VT><<<blocks, 256, 0, st>>>(segs, nseg, s, z, sc);
+  return cudaGetLastError();
+}
+template cudaError_t batch_update_s<double>(const BatchSeg*, int, int, double*, const double*, PcgScalars*,
+                                            cudaStream_t);
+template cudaError_t batch_update_s<float>(const BatchSeg*, int, int, float*, const float*, PcgScalars*,
+                                           cudaStream_t);
+
+template <typename VT>
+cudaError_t batch_absmax_init(const BatchSeg* segs, int nseg, int blocks, const VT* b, PcgScalars* sc,
+                              double tol, int maxit, const double* tols, const int* maxits, cudaStream_t st) {
+  ++g_kernel_launches;
+  batch_absmax_init_kernel<VT><<<blocks, 256, 0, st>>>(segs, nseg, b, sc, tol, maxit, tols, maxits);
+  return cudaGetLastError();
+}
+template cudaError_t batch_absmax_init<double>(const BatchSeg*, int, int, const double*, PcgScalars*, double,
+                                               int, const double*, const int*, cudaStream_t);
+template cudaError_t batch_absmax_init<float>(const BatchSeg*, int, int, const float*, PcgScalars*, double, int,
+                                              const double*, const int*, cudaStream_t);
+
+// One thread per scene: the same sequential sum over the scene's tiles, in
+// its own tile order, that the single-scene backward sweep's last CTA does.
+template <typename DT>
+__global__ void batch_bwd_reduce_kernel(int nseg, const int* __restrict__ start, const int* __restrict__ tiles,
+                                        const double* __restrict__ tpartials, PcgScalars* sc, int mode) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nseg) return;
+  PcgScalars* S = sc + q;
+  if (S->done) return;
+  double acc = 0.0;
+  float accf = 0.f;
+  for (int t = start[q]; t < start[q + 1]; ++t) {
+    const double pv = tpartials[tiles[t]];
+    if (std::is_same<DT, float>::value) accf = __fadd_rn(accf, (float)pv); else acc = __dadd_rn(acc, pv);
+  }
+  const double rho_new = std::is_same<DT, float>::value ? (double)accf : acc;
+  if (mode == 0) {
+    S->rho = rho_new;
+    if (rho_new == 0.0 || rho_new != rho_new) { S->status = -5; S->done = 1; }
+  } else {
+    S->beta = std::is_same<DT, float>::value ? (double)__fdiv_rn((float)rho_new, (float)S->rho)
+                                             : __ddiv_rn(rho_new, S->rho);
+    S->rho = rho_new;
+  }
+}
+template <typename DT>
+cudaError_t batch_bwd_reduce(int nseg, const int* scene_tile_start, const int* scene_tiles,
+                             const double* tpartials, PcgScalars* sc, int mode, cudaStream_t st) {
+  ++g_kernel_launches;
+  batch_bwd_reduce_kernel<DT><<<(nseg + 63) / 64, 64, 0, st>>>(nseg, scene_tile_start, scene_tiles, tpartials, sc,
+                                                               mode);
+  return cudaGetLastError();
+}
+template cudaError_t batch_bwd_reduce<double>(int, const int*, const int*, const double*, PcgScalars*, int,
+                                              cudaStream_t);
+template cudaError_t batch_bwd_reduce<float>(int, const int*, const int*, const double*, PcgScalars*, int,
+                                             cudaStream_t);
+
+__global__ void offset_lines_kernel(Line* __restrict__ lines, long long nlines, long long base) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nlines;
+       q += (long long)gridDim.x * blockDim.x)
+    lines[q].off += (int)base;
+}
+cudaError_t offset_lines(Line* lines, long long nlines, long long base, cudaStream_t st) {
+  if (base == 0 || nlines <= 0) return cudaSuccess;
+  ++g_kernel_launches;
+  offset_lines_kernel<<<(unsigned)std::min<long long>((nlines + 255) / 256, 148LL * 8), 256, 0, st>>>(lines, nlines,
+                                                                                                   base);
   return cudaGetLastError();
 }
 

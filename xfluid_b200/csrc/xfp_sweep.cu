@@ -222,7 +222,6 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned gen = ld_volatile_u32(&g.ctl->gen);
-  const int nj = g.nj, nk = g.nk, maxT = g.maxT;
 
   if (OP != SWEEP_FACTOR && g.scal != nullptr && *(volatile int*)&g.scal->done != 0) return;
 
@@ -235,6 +234,20 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
 
   for (int pos = blockIdx.x, seq = 0; pos < g.ntiles; pos += gridDim.x, ++seq) {
     const int tpos = REV ? g.ntiles - 1 - pos : pos;
+    // the tile's grid: the launch's one scene, or its scene of the batch
+    int nj = g.nj, nk = g.nk, maxT = g.maxT;
+    const Line* lines = g.lines;
+    if (g.tile_scene != nullptr) {
+      const int sid = g.tile_scene[tpos];
+      const BatchSeg& S = g.segs[sid];
+      // a converged scene's tiles are skipped (its scalars only change between
+      // launches, so every CTA of this launch decides the same way)
+      if (OP != SWEEP_FACTOR && g.scal_batch != nullptr && *(volatile int*)&g.scal_batch[sid].done != 0) continue;
+      nj = S.nj;
+      nk = S.nk;
+      maxT = S.ni + S.nj + S.nk;
+      lines = S.lines;
+    }
     const int packed = g.tiles[tpos];
     const int J = packed & 0xffff, K = packed >> 16;
     const int j0 = J * 32, k0 = K * NW;
@@ -245,7 +258,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
     int s = 0;
     if (warp < NW) {
       const int j = j0 + lane, k = k0 + warp;
-      if (j < nj && k < nk) L = g.lines[(size_t)k * nj + j];
+      if (j < nj && k < nk) L = lines[(size_t)k * nj + j];
       s = j + k;
       int tl = INF_T, th = INT_MIN;
       if (L.len > 0) {
@@ -297,8 +310,8 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
       Line Ly = {0, 0, 0, 0}, Lz = {0, 0, 0, 0};
       if (OP == SWEEP_FACTOR) {
         const int j = j0 + lane;
-        if (j + 1 < nj && k < nk) Ly = g.lines[(size_t)k * nj + j + 1];
-        if (j < nj && k + 1 < nk) Lz = g.lines[(size_t)(k + 1) * nj + j];
+        if (j + 1 < nj && k < nk) Ly = lines[(size_t)k * nj + j + 1];
+        if (j < nj && k + 1 < nk) Lz = lines[(size_t)(k + 1) * nj + j];
       }
 
       // Cell data of the next PF steps is kept in flight in a rotating register
@@ -533,7 +546,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
       int sj_c = 0, Sj_lo = INF_T, Sj_hi = INT_MIN;
       {
         const int kr = k0 + lane;
-        if (lane < NW && kr < nk && js >= 0 && js < nj) Ljs = g.lines[(size_t)kr * nj + js];
+        if (lane < NW && kr < nk && js >= 0 && js < nj) Ljs = lines[(size_t)kr * nj + js];
         sj_c = jc + kr;
         if (Ljs.len > 0) {
           const int a = Ljs.lo + sj_c, b = Ljs.lo + Ljs.len - 1 + sj_c;
@@ -544,7 +557,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
       int sk_c = 0, Sk_lo = INF_T, Sk_hi = INT_MIN;
       {
         const int jl = j0 + lane;
-        if (jl < nj && ks >= 0 && ks < nk) Lks = g.lines[(size_t)ks * nj + jl];
+        if (jl < nj && ks >= 0 && ks < nk) Lks = lines[(size_t)ks * nj + jl];
         sk_c = jl + kc;
         if (Lks.len > 0) {
           const int a = Lks.lo + sk_c, b = Lks.lo + Lks.len - 1 + sk_c;
