@@ -179,6 +179,35 @@ typedef struct xfp_scene {
 int xfp_project_batch_f32(xfp_ctx* ctx, int n, const xfp_scene* scenes, xfp_stats* stats);
 int xfp_project_batch_f64(xfp_ctx* ctx, int n, const xfp_scene* scenes, xfp_stats* stats);
 
+/* Differentiable rollouts (advect -> project, repeated; no reference
+ * counterpart: xFluid moves velocity with particles, FluidSimulator.cpp:652-1085).
+ * Semi-Lagrangian self-advection of the MAC velocity: each face value is
+ * re-sampled (trilinear, lattice coordinates clamped to the grid) at its
+ * departure point x_f - dt_over_dx * vel(x_f), vel sampled from u, v, w at
+ * the face.  The backward form writes the exact adjoint (both the sampling
+ * weights and the departure point's dependence on the velocity) of that map
+ * at state (u,v,w): (du,dv,dw) = J^T (gu,gv,gw).  The box loss is the sum of
+ * squared face values whose unit-cube position ((i,j+.5,k+.5)/(ni,nj,nk) for
+ * u, etc.) lies in box = {x0,x1,y0,y1,z0,z1}; its gradient (2*value inside,
+ * 0 outside) is written when gu/gv/gw are given; loss is a host double.
+ * These entry points take device arrays only (options.device_pointers = 1);
+ * box is host memory. */
+int xfp_advect_f64(xfp_ctx* ctx, int ni, int nj, int nk, const double* u, const double* v,
+                   const double* w, double* ou, double* ov, double* ow, double dt_over_dx);
+int xfp_advect_f32(xfp_ctx* ctx, int ni, int nj, int nk, const float* u, const float* v,
+                   const float* w, float* ou, float* ov, float* ow, double dt_over_dx);
+int xfp_advect_backward_f64(xfp_ctx* ctx, int ni, int nj, int nk, const double* u, const double* v,
+                            const double* w, const double* gu, const double* gv, const double* gw,
+                            double* du, double* dv, double* dw, double dt_over_dx);
+int xfp_advect_backward_f32(xfp_ctx* ctx, int ni, int nj, int nk, const float* u, const float* v,
+                            const float* w, const float* gu, const float* gv, const float* gw,
+                            float* du, float* dv, float* dw, double dt_over_dx);
+int xfp_box_loss_f64(xfp_ctx* ctx, int ni, int nj, int nk, const double* u, const double* v,
+                     const double* w, const double* box, double* loss, double* gu, double* gv,
+                     double* gw);
+int xfp_box_loss_f32(xfp_ctx* ctx, int ni, int nj, int nk, const float* u, const float* v,
+                     const float* w, const double* box, double* loss, float* gu, float* gv, float* gw);
+
 /* Diagnostics: runs the internal stages on one scene and returns them on the
  * dense grid (ni*nj*nk doubles each; any output may be NULL), in the
  * context's precision.  Exposes, for verification against the reference:

@@ -148,6 +148,17 @@ cudaError_t batch_residual64(const BatchSeg* segs, int nseg, int blocks, const d
 template <typename DT>
 cudaError_t batch_bwd_reduce(int nseg, const int* scene_tile_start, const int* scene_tiles,
                              const double* tpartials, PcgScalars* sc, int mode, cudaStream_t st);
+// ---- semi-Lagrangian MAC self-advection and its adjoint (xfp_advect.cu) ----
+template <typename T>
+cudaError_t advect(const T* u, const T* v, const T* w, T* ou, T* ov, T* ow, int ni, int nj, int nk, T c,
+                   cudaStream_t st);
+template <typename T>
+cudaError_t advect_adjoint(const T* u, const T* v, const T* w, const T* gu, const T* gv, const T* gw, T* du,
+                           T* dv, T* dw, int ni, int nj, int nk, T c, cudaStream_t st);
+template <typename T>
+cudaError_t box_loss(const T* u, const T* v, const T* w, T* gu, T* gv, T* gw, int ni, int nj, int nk,
+                     const double box[6], double* loss, cudaStream_t st);
+
 // Adds base[s] to the offsets of scene s's line table.
 cudaError_t offset_lines(Line* lines, long long nlines, long long base, cudaStream_t st);
 
