@@ -16,6 +16,7 @@ HERE = Path(__file__).resolve().parent
 ORACLE_SRC = HERE / "xfp_oracle.c"
 ORACLE_LIB = HERE / "_build" / "libxfp_oracle.so"
 REF_LIB = HERE / "_ref" / "libxfref.so"
+SIM_LIB = HERE / "_ref" / "libxfsim.so"
 
 _dp = C.POINTER(C.c_double)
 _u8 = C.POINTER(C.c_uint8)
@@ -43,7 +44,13 @@ def build_reference(ref_root: str | None = None) -> Path | None:
         return None
     subprocess.check_call(["bash", str(HERE / "build_ref.sh")], env=env,
                           stdout=subprocess.DEVNULL)
+    subprocess.check_call(["bash", str(HERE / "build_sim.sh")], env=env,
+                          stdout=subprocess.DEVNULL)
     return REF_LIB
+
+
+def sim_available() -> bool:
+    return SIM_LIB.exists()
 
 
 def oracle_available() -> bool:
@@ -256,3 +263,56 @@ class Reference(_Lib):
         self.lib.xfref_divergence(sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(_f64(u)),
                                   _p(_f64(v)), _p(_f64(w)), _p(d))
         return d
+
+
+class RefSim(_Lib):
+    """xFluid's own FluidSimulator on the dam-break scene (oracle/_ref/libxfsim.so,
+    oracle/sim_harness.cpp), stepped up to and through the projection."""
+
+    def __init__(self, n=64, cfl=5.0, gravity=-9.8, tol=1e-6, maxit=200):
+        super().__init__(SIM_LIB)
+        L = self.lib
+        L.xfsim_create_dam.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int]
+        L.xfsim_create_dam.restype = C.c_void_p
+        L.xfsim_destroy.argtypes = [C.c_void_p]
+        L.xfsim_begin_step.argtypes = [C.c_void_p, C.c_double, _u8, _dp, _dp, _dp]
+        L.xfsim_begin_step.restype = C.c_double
+        L.xfsim_project.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.POINTER(C.c_int)]
+        L.xfsim_project.restype = C.c_int
+        L.xfsim_end_step.argtypes = [C.c_void_p]
+        L.xfsim_fluid_cells.argtypes = [C.c_void_p]
+        L.xfsim_fluid_cells.restype = C.c_int
+        self.n = n
+        self.h = L.xfsim_create_dam(n, cfl, gravity, tol, maxit)
+
+    def close(self):
+        if self.h:
+            self.lib.xfsim_destroy(self.h)
+            self.h = None
+
+    def _shapes(self):
+        n = self.n
+        return (n, n, n), (n, n, n + 1), (n, n + 1, n), (n + 1, n, n)
+
+    def begin_step(self, max_dt=1.0 / 30.0):
+        """Runs the step up to the projection; returns (dt, mat, u, v, w)."""
+        sm, su, sv, sw = self._shapes()
+        mat = np.zeros(sm, np.uint8)
+        u, v, w = np.zeros(su), np.zeros(sv), np.zeros(sw)
+        dt = self.lib.xfsim_begin_step(self.h, max_dt, _p(mat), _p(u), _p(v), _p(w))
+        return dt, mat, u, v, w
+
+    def project(self):
+        """The reference's own projection: (ok, pressure, u, v, w, iterations)."""
+        sm, su, sv, sw = self._shapes()
+        p = np.zeros(sm)
+        u, v, w = np.zeros(su), np.zeros(sv), np.zeros(sw)
+        it = C.c_int(0)
+        ok = self.lib.xfsim_project(self.h, _p(p), _p(u), _p(v), _p(w), C.byref(it))
+        return bool(ok), p, u, v, w, it.value
+
+    def end_step(self):
+        self.lib.xfsim_end_step(self.h)
+
+    def fluid_cells(self):
+        return self.lib.xfsim_fluid_cells(self.h)

@@ -1,0 +1,146 @@
+// sim_harness.cpp -- TEST INFRASTRUCTURE ONLY (part of the oracle).
+//
+// Drives xFluid's own FluidSimulator (compiled from the reference sources by
+// oracle/build_sim.sh) one time step at a time, stopping just before the
+// pressure projection so a test can hand the very same (material, u, v, w)
+// snapshot to the CUDA path and compare.  The simulator then continues with
+// its own projection, so every step's snapshot is the reference's.
+//
+// A step follows FluidSimulator::timeStep (xFluid/xFluid/FluidSimulator.cpp:
+// 265-335) with the mesh output left out:
+//   xfsim_begin_step  dt as frameStep picks it (:228-253, capped at max_dt),
+//                     distance field + surface + material update (:274-277),
+//                     _saveVelocity (:286), _applyForces (:310)
+//   xfsim_project     _solvePressure (:501-509): setDt, solve, applyPressure
+//   xfsim_end_step    _expolateVelocity (:322), _advectParticles (:328)
+// The scene is the dam break of the plain CPU-runnable configuration:
+// FluidSimulator(n,n,n), setCellWidth(1/n), addCubicFluid((0,0,0),(0.4,0.5,1))
+// (:123-140), gravity (0,g,0) (:142-150), init (:186-222, solid border and 8
+// jittered particles per fluid cell, :168-184 and :347-370).
+//
+// Private members (CFL number, pressure solver, grids) are reached by mapping
+// private/protected to public around the reference header.  std::cout is muted
+// around every call (the reference prints timings each step).
+
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#define private public
+#define protected public
+#include "FluidSimulator.h"
+#undef private
+#undef protected
+
+namespace {
+
+struct MuteCout {
+  std::streambuf* saved;
+  std::ostringstream sink;
+  MuteCout() : saved(std::cout.rdbuf(sink.rdbuf())) {}
+  ~MuteCout() { std::cout.rdbuf(saved); }
+};
+
+struct Sim {
+  FluidSimulator fs;
+  double dt = 0.0;
+  int iters = 0;
+  explicit Sim(int n) : fs(n, n, n) {}
+};
+
+template <typename T>
+void dump(Array3d<T>& a, T* dst) {
+  for (int k = 0; k < a.sizek(); ++k)
+    for (int j = 0; j < a.sizej(); ++j)
+      for (int i = 0; i < a.sizei(); ++i)
+        dst[(size_t)k * a.sizei() * a.sizej() + (size_t)j * a.sizei() + i] = a(i, j, k);
+}
+
+}  // namespace
+
+extern "C" {
+
+void* xfsim_create_dam(int n, double cfl, double gravity, double tol, int maxit) {
+  MuteCout mute;
+  Sim* s = new Sim(n);
+  s->fs.setCellWidth(1.0 / n);
+  s->fs.addCubicFluid(Vec3d(0.0, 0.0, 0.0), Vec3d(0.4, 0.5, 1.0));
+  s->fs.addConstantForce(0.0, gravity, 0.0);
+  s->fs._CFLnumber = cfl;
+  s->fs.init();
+  s->fs._pressureSolver.solver.set_solver_parameters(tol, maxit);
+  return s;
+}
+
+void xfsim_destroy(void* h) { delete static_cast<Sim*>(h); }
+
+// Everything before the projection; writes the snapshot the projection sees.
+double xfsim_begin_step(void* h, double max_dt, uint8_t* mat, double* u, double* v, double* w) {
+  MuteCout mute;
+  Sim* s = static_cast<Sim*>(h);
+  FluidSimulator& f = s->fs;
+  const double maxv = f._maxVelocity();
+  double dt = maxv == 0.0 ? f._maxStepTime : f._CFLnumber * f._dx / maxv;
+  dt = dt < f._maxStepTime ? dt : f._maxStepTime;
+  dt = dt < max_dt ? dt : max_dt;
+  s->dt = dt;
+  f._dis_field.updateFeild();
+  f._dis_field.updateSurfaceInfo(f._material);
+  f._updateMaterial();
+  f._saveVelocity();
+  f._applyForces(dt);
+  for (int k = 0; k < f._material.sizek(); ++k)
+    for (int j = 0; j < f._material.sizej(); ++j)
+      for (int i = 0; i < f._material.sizei(); ++i)
+        mat[(size_t)k * f._ni * f._nj + (size_t)j * f._ni + i] = static_cast<uint8_t>(f._material(i, j, k));
+  dump(f._u, u);
+  dump(f._v, v);
+  dump(f._w, w);
+  return dt;
+}
+
+// The reference's own projection of the snapshot; writes its pressure (when
+// the solve succeeded) and the projected velocities.  Returns 1 on success.
+int xfsim_project(void* h, double* p, double* u, double* v, double* w, int* iters) {
+  MuteCout mute;
+  Sim* s = static_cast<Sim*>(h);
+  FluidSimulator& f = s->fs;
+  // iterations: the same PCG rerun on the same system (solve() does not report them)
+  if (iters) {
+    SparseMatrix<double> A;
+    std::vector<double> b;
+    f._pressureSolver._calculate_coefficient(A, b);
+    std::vector<double> x(b.size(), 0.0);
+    double res = 0.0;
+    int it = 0;
+    PCGSolver<double> pcg;
+    pcg.set_solver_parameters(f._pressureSolver.solver.tolerance_factor, f._pressureSolver.solver.max_iterations);
+    pcg.solve(A, b, x, res, it);
+    *iters = it;
+  }
+  Array3d<double> pressure;
+  f._pressureSolver.setDt(s->dt);
+  const bool ok = f._pressureSolver.solve(pressure);
+  f._pressureSolver.applyPressure(pressure);
+  if (ok && p) dump(pressure, p);
+  dump(f._u, u);
+  dump(f._v, v);
+  dump(f._w, w);
+  return ok ? 1 : 0;
+}
+
+void xfsim_end_step(void* h) {
+  MuteCout mute;
+  Sim* s = static_cast<Sim*>(h);
+  s->fs._expolateVelocity();
+  s->fs._advectParticles(s->dt);
+}
+
+int xfsim_fluid_cells(void* h) { return static_cast<Sim*>(h)->fs._countFluidCell(); }
+
+}  // extern "C"

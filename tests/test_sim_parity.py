@@ -1,0 +1,85 @@
+"""Parity inside xFluid's own simulation loop (the plain CPU-runnable
+configuration): a 64^3 dam break (dx = 1/64, solid border, fluid x < 0.4,
+y < 0.5, 8 jittered particles per fluid cell, gravity -9.8, CFL 5) stepped 30
+times by the reference FluidSimulator built from its sources (oracle/_ref).
+Before each projection the simulator's own (material, u, v, w) snapshot goes
+to the CUDA path -- FP64, and mixed precision with FP32 velocities -- and to
+the reference projection of the same snapshot (MIC(0)-PCG, tol 1e-6, at most
+200 iterations); the simulator then continues with the reference result.
+
+Bars per step: pressure relative L2 <= 1e-5 (FP64) and <= 1e-4 (mixed, FP32
+inputs), projected velocities likewise, FP64 iteration count within 5% of the
+reference's, and the post-projection weighted divergence (the residual the
+solve drives to tol * |b|_inf) no larger than the reference's own by more than
+the tolerance allows."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 30
+
+
+def _rel(a, b):
+    d = np.linalg.norm(b)
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / (d if d > 0 else 1.0))
+
+
+def _project(ctx, mat, u, v, w, dtype):
+    import ctypes as C
+    from xfluid_b200 import _lib
+    n = mat.shape[0]
+    uu, vv, ww = (np.array(a, dtype) for a in (u, v, w))
+    p = np.zeros(mat.shape, dtype)
+    st = _lib.XfpStats()
+    fn = ctx.lib.xfp_project_f64 if dtype == np.float64 else ctx.lib.xfp_project_f32
+    P = lambda a: C.c_void_p(a.ctypes.data)
+    rc = ctx.check(fn(ctx.ptr, n, n, n, P(np.ascontiguousarray(mat)), P(uu), P(vv), P(ww), None, None, None, P(p),
+                      C.byref(st)))
+    return rc, p, uu, vv, ww, st.as_dict()
+
+
+@pytest.mark.skipif(not oracle.sim_available(), reason="reference simulator not built (oracle/_ref/libxfsim.so)")
+def test_dam_break_30_steps_inside_reference_simulator():
+    from gpu_util import make_ctx
+    O = oracle.Oracle()
+    sim = oracle.RefSim(64, cfl=5.0, gravity=-9.8, tol=1e-6, maxit=200)
+    c64 = make_ctx("f64", tol=1e-6, max_iter=200)
+    cmx = make_ctx("mixed", tol=1e-6, max_iter=200)
+    rows = []
+    try:
+        for step in range(STEPS):
+            dt, mat, u, v, w = sim.begin_step()
+            rc64, p64, u64, v64, w64, s64 = _project(c64, mat, u, v, w, np.float64)
+            rcm, pm, um, vm, wm, sm = _project(cmx, mat, u, v, w, np.float32)
+            ok, pr, ur, vr, wr, itr = sim.project()
+            sim.end_step()
+            assert ok and rc64 == 0 and rcm == 0, (step, ok, rc64, rcm)
+            from xfluid_b200.scenes import Scene
+            sc = Scene(64, 64, 64, mat, u, v, w)
+            div_ref = np.abs(O.weighted_divergence(sc, ur, vr, wr)).max()
+            div_64 = np.abs(O.weighted_divergence(sc, u64, v64, w64)).max()
+            div_mx = np.abs(O.weighted_divergence(sc, *(a.astype(np.float64) for a in (um, vm, wm)))).max()
+            rows.append(dict(step=step, dt=dt, fluid=int((mat == 1).sum()), it_ref=itr, it64=s64["iterations"],
+                             itmx=sm["iterations"], p64=_rel(p64, pr), pmx=_rel(pm, pr),
+                             u64=max(_rel(u64, ur), _rel(v64, vr), _rel(w64, wr)),
+                             umx=max(_rel(um, ur), _rel(vm, vr), _rel(wm, wr)),
+                             div_ref=div_ref, div64=div_64, divmx=div_mx, b_inf=s64["b_inf"]))
+    finally:
+        sim.close()
+        c64.close()
+        cmx.close()
+    import json
+    import os
+    if os.environ.get("XFP_SIM_REPORT"):
+        with open(os.environ["XFP_SIM_REPORT"], "w") as f:
+            json.dump(rows, f, indent=1, default=float)
+    for r in rows:
+        msg = str(r)
+        assert r["p64"] <= 1e-5 and r["u64"] <= 1e-5, msg
+        assert abs(r["it64"] - r["it_ref"]) <= max(1, int(np.ceil(0.05 * r["it_ref"]))), msg
+        assert r["pmx"] <= 1e-4 and r["umx"] <= 1e-4, msg
+        # the solve stops at |r|_inf <= 1e-6 |b|_inf; both residuals sit below it
+        assert r["div64"] <= max(2 * r["div_ref"], 1e-6 * r["b_inf"] * 1.01), msg
