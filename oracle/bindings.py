@@ -269,11 +269,16 @@ class RefSim(_Lib):
     """xFluid's own FluidSimulator on the dam-break scene (oracle/_ref/libxfsim.so,
     oracle/sim_harness.cpp), stepped up to and through the projection."""
 
-    def __init__(self, n=64, cfl=5.0, gravity=-9.8, tol=1e-6, maxit=200):
+    def __init__(self, n=64, cfl=5.0, gravity=-9.8, tol=1e-6, maxit=200, boxes=None, spheres=()):
+        """boxes: fluid boxes ((x0,y0,z0),(x1,y1,z1)) (default: the dam break);
+        spheres: fluid spheres ((cx,cy,cz), r); unit-cube coordinates."""
         super().__init__(SIM_LIB)
         L = self.lib
-        L.xfsim_create_dam.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int]
-        L.xfsim_create_dam.restype = C.c_void_p
+        L.xfsim_create.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int]
+        L.xfsim_create.restype = C.c_void_p
+        L.xfsim_add_box.argtypes = [C.c_void_p] + [C.c_double] * 6
+        L.xfsim_add_sphere.argtypes = [C.c_void_p] + [C.c_double] * 4
+        L.xfsim_init.argtypes = [C.c_void_p]
         L.xfsim_destroy.argtypes = [C.c_void_p]
         L.xfsim_begin_step.argtypes = [C.c_void_p, C.c_double, _u8, _dp, _dp, _dp]
         L.xfsim_begin_step.restype = C.c_double
@@ -283,7 +288,12 @@ class RefSim(_Lib):
         L.xfsim_fluid_cells.argtypes = [C.c_void_p]
         L.xfsim_fluid_cells.restype = C.c_int
         self.n = n
-        self.h = L.xfsim_create_dam(n, cfl, gravity, tol, maxit)
+        self.h = L.xfsim_create(n, cfl, gravity, tol, maxit)
+        for lo, hi in (boxes if boxes is not None else [((0.0, 0.0, 0.0), (0.4, 0.5, 1.0))]):
+            L.xfsim_add_box(self.h, *lo, *hi)
+        for c, r in spheres:
+            L.xfsim_add_sphere(self.h, *c, r)
+        L.xfsim_init(self.h)
 
     def close(self):
         if self.h:
@@ -302,13 +312,14 @@ class RefSim(_Lib):
         dt = self.lib.xfsim_begin_step(self.h, max_dt, _p(mat), _p(u), _p(v), _p(w))
         return dt, mat, u, v, w
 
-    def project(self):
-        """The reference's own projection: (ok, pressure, u, v, w, iterations)."""
+    def project(self, iterations=True):
+        """The reference's own projection: (ok, pressure, u, v, w, iterations);
+        iterations (a rerun of the same PCG) is -1 when not asked for."""
         sm, su, sv, sw = self._shapes()
         p = np.zeros(sm)
         u, v, w = np.zeros(su), np.zeros(sv), np.zeros(sw)
-        it = C.c_int(0)
-        ok = self.lib.xfsim_project(self.h, _p(p), _p(u), _p(v), _p(w), C.byref(it))
+        it = C.c_int(-1)
+        ok = self.lib.xfsim_project(self.h, _p(p), _p(u), _p(v), _p(w), C.byref(it) if iterations else None)
         return bool(ok), p, u, v, w, it.value
 
     def end_step(self):

@@ -13,10 +13,11 @@
 //                     _saveVelocity (:286), _applyForces (:310)
 //   xfsim_project     _solvePressure (:501-509): setDt, solve, applyPressure
 //   xfsim_end_step    _expolateVelocity (:322), _advectParticles (:328)
-// The scene is the dam break of the plain CPU-runnable configuration:
-// FluidSimulator(n,n,n), setCellWidth(1/n), addCubicFluid((0,0,0),(0.4,0.5,1))
-// (:123-140), gravity (0,g,0) (:142-150), init (:186-222, solid border and 8
-// jittered particles per fluid cell, :168-184 and :347-370).
+// Scenes: FluidSimulator(n,n,n), setCellWidth(1/n), gravity (0,g,0)
+// (:142-150), fluid from addCubicFluid (:123-140) and addSpereFluid (:98-121),
+// then init (:186-222: solid border, 8 jittered particles per fluid cell,
+// :168-184 and :347-370).  xfsim_create_dam builds the dam break of the plain
+// CPU-runnable configuration: fluid box (0,0,0)-(0.4,0.5,1).
 //
 // Private members (CFL number, pressure solver, grids) are reached by mapping
 // private/protected to public around the reference header.  std::cout is muted
@@ -65,16 +66,37 @@ void dump(Array3d<T>& a, T* dst) {
 
 extern "C" {
 
-void* xfsim_create_dam(int n, double cfl, double gravity, double tol, int maxit) {
+// An n^3 simulator with cell width 1/n (unit cube); add fluid, then init.
+void* xfsim_create(int n, double cfl, double gravity, double tol, int maxit) {
   MuteCout mute;
   Sim* s = new Sim(n);
   s->fs.setCellWidth(1.0 / n);
-  s->fs.addCubicFluid(Vec3d(0.0, 0.0, 0.0), Vec3d(0.4, 0.5, 1.0));
   s->fs.addConstantForce(0.0, gravity, 0.0);
   s->fs._CFLnumber = cfl;
-  s->fs.init();
   s->fs._pressureSolver.solver.set_solver_parameters(tol, maxit);
   return s;
+}
+// addCubicFluid (FluidSimulator.cpp:123-140): cells whose centre lies in the box
+void xfsim_add_box(void* h, double x0, double y0, double z0, double x1, double y1, double z1) {
+  static_cast<Sim*>(h)->fs.addCubicFluid(Vec3d(x0, y0, z0), Vec3d(x1, y1, z1));
+}
+// addSpereFluid (FluidSimulator.cpp:98-121)
+void xfsim_add_sphere(void* h, double cx, double cy, double cz, double r) {
+  static_cast<Sim*>(h)->fs.addSpereFluid(cx, cy, cz, r);
+}
+// init (FluidSimulator.cpp:186-222): solid border, particles, distance field, solver wiring
+void xfsim_init(void* h) {
+  MuteCout mute;
+  Sim* s = static_cast<Sim*>(h);
+  s->fs.init();
+  // init() does not touch the PCG parameters set at creation
+}
+// The dam break: fluid box (0,0,0)-(0.4,0.5,1).
+void* xfsim_create_dam(int n, double cfl, double gravity, double tol, int maxit) {
+  void* h = xfsim_create(n, cfl, gravity, tol, maxit);
+  xfsim_add_box(h, 0.0, 0.0, 0.0, 0.4, 0.5, 1.0);
+  xfsim_init(h);
+  return h;
 }
 
 void xfsim_destroy(void* h) { delete static_cast<Sim*>(h); }

@@ -83,3 +83,74 @@ def test_dam_break_30_steps_inside_reference_simulator():
         assert r["pmx"] <= 1e-4 and r["umx"] <= 1e-4, msg
         # the solve stops at |r|_inf <= 1e-6 |b|_inf; both residuals sit below it
         assert r["div64"] <= max(2 * r["div_ref"], 1e-6 * r["b_inf"] * 1.01), msg
+
+
+POOL_STEPS = 3
+
+
+@pytest.mark.skipif(not oracle.sim_available(), reason="reference simulator not built (oracle/_ref/libxfsim.so)")
+def test_pool_drop_128_mixed_vs_fp64_oracle_per_step():
+    """Drop into a pool at 128^3: the reference simulator steps a pool (y < 0.3)
+    plus a fluid sphere (r 0.15 at (0.5,0.7,0.5)), ~5M particles.  Each
+    pre-projection snapshot gets the static solid sphere (r 0.1 at
+    (0.3,0.2,0.5)): its cells solid, its cut faces fractional open weights
+    (xFluid's simulator has no fractional solids, so the obstacle is added to
+    the snapshot, not simulated).  The mixed-precision CUDA path (FP32 fields,
+    FP64 dots/pivots/refinement) is checked per step against the FP64 oracle at
+    the same tolerance (1e-6) and at a tight one (1e-12)."""
+    from gpu_util import make_ctx
+    from xfluid_b200 import scenes
+    n = 128
+    O = oracle.Oracle()
+    sim = oracle.RefSim(n, cfl=5.0, gravity=-9.8, tol=1e-6, maxit=200,
+                        boxes=[((0.0, 0.0, 0.0), (1.0, 0.3, 1.0))], spheres=[((0.5, 0.7, 0.5), 0.15)])
+    c = (np.arange(n) + 0.5) / n
+    X, Y, Z = c[None, None, :], c[None, :, None], c[:, None, None]
+    obstacle = np.broadcast_to((X - 0.3) ** 2 + (Y - 0.2) ** 2 + (Z - 0.5) ** 2 < 0.1 ** 2, (n, n, n))
+    wts = scenes._sphere_face_fractions(n, n, n, (0.3, 0.2, 0.5), 0.1)
+    cmx = make_ctx("mixed", tol=1e-6, max_iter=400)
+    rows = []
+    try:
+        for step in range(POOL_STEPS):
+            dt, mat, u, v, w = sim.begin_step()
+            mat = mat.copy()
+            mat[obstacle] = scenes.SOLID
+            sc = scenes.Scene(n, n, n, mat, u, v, w, *wts)
+            import ctypes as C
+            from xfluid_b200 import _lib
+            f32 = lambda a: np.ascontiguousarray(a, np.float32)
+            uu, vv, ww = f32(u), f32(v), f32(w)
+            p = np.zeros((n, n, n), np.float32)
+            st = _lib.XfpStats()
+            P = lambda a: C.c_void_p(a.ctypes.data)
+            wf = [f32(a) for a in wts]
+            rc = cmx.check(cmx.lib.xfp_project_f32(cmx.ptr, n, n, n, P(mat), P(uu), P(vv), P(ww), *map(P, wf), P(p),
+                                                   C.byref(st)))
+            ref6 = O.project(sc, tol=1e-6, maxit=2000)
+            ref12 = O.project(sc, tol=1e-12, maxit=20000)
+            sim.project(iterations=False)
+            sim.end_step()
+            div = np.abs(O.weighted_divergence(sc, *(a.astype(np.float64) for a in (uu, vv, ww)))).max()
+            rows.append(dict(step=step, dt=dt, rc=rc, it=st.iterations, refinements=st.refinements,
+                             it_oracle=int(ref6.get("iters", -1)), p_vs_oracle=_rel(p, ref6["p"]),
+                             p_vs_exact=_rel(p, ref12["p"]), oracle_vs_exact=_rel(ref6["p"], ref12["p"]),
+                             u_vs_oracle=max(_rel(uu, ref6["u"]), _rel(vv, ref6["v"]), _rel(ww, ref6["w"])),
+                             div=div, b_inf=st.b_inf, umax=float(max(np.abs(a).max() for a in (uu, vv, ww)))))
+    finally:
+        sim.close()
+        cmx.close()
+    import json
+    import os
+    if os.environ.get("XFP_SIM_REPORT"):
+        with open(os.environ["XFP_SIM_REPORT"] + ".pool", "w") as f:
+            json.dump(rows, f, indent=1, default=float)
+    for r in rows:
+        msg = str(r)
+        assert r["rc"] == 0, msg
+        # FP32 fields and FP64 refinement vs the FP64 solve at the same tolerance
+        assert r["p_vs_oracle"] <= 1e-4 and r["u_vs_oracle"] <= 1e-4, msg
+        # no worse against the exact solution than the FP64 solve itself, to within 2x
+        assert r["p_vs_exact"] <= max(2 * r["oracle_vs_exact"], 1e-5), msg
+        # the refined residual meets the tolerance, up to the rounding of the
+        # FP32 output faces (six faces per cell, half an ulp each)
+        assert r["div"] <= 1.01e-6 * r["b_inf"] + 6 * 2.0 ** -24 * r["umax"], msg
