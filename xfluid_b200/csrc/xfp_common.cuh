@@ -1,13 +1,17 @@
 // xfp_common.cuh -- shared device helpers and layout structures for libxfp.
 //
 // Storage layout ("line-compacted"): the grid is cut into x-lines, one per
-// (j,k).  Each line that holds an unknown stores the cells of its active span
-// [lo, lo+len) contiguously, lo rounded down and len rounded up to a multiple
-// of XFP_ALIGN cells, at offset `off` in every per-cell array.  Because off and
-// lo are both multiples of XFP_ALIGN, cell i of ANY line sits at an address
-// congruent to i modulo XFP_ALIGN, so aligned vector loads of neighbour lines
-// stay aligned.  Cells inside a span that are not unknowns (air, uncoupled
-// solid) are padding: zero coefficients, zero vectors, null rows.
+// (j,k).  Each line that holds an unknown stores the cells [lo, lo+len)
+// contiguously at offset `off` in every per-cell array: lo is the first
+// unknown moved down by 0..3 cells so that lo + j + k = 0 (mod XFP_ALIGN), len
+// is rounded up to a multiple of XFP_ALIGN, and off is a multiple of
+// XFP_ALIGN.  Cell (i,j,k) therefore sits at an address = i + j + k (mod
+// XFP_ALIGN): every cell of one wavefront hyperplane i+j+k = t has the same
+// position inside its aligned group of XFP_ALIGN cells, which is what lets
+// the triangular-solve sweeps move whole groups with one vector access.  lo
+// may be negative and lo+len may pass ni; cells inside a span that are not
+// unknowns (air, uncoupled solid, outside the grid) are padding: zero
+// coefficients, zero vectors, null rows.
 #pragma once
 
 #include <cstdint>

@@ -3,7 +3,8 @@
 // Unknown rows are xFluid's: fluid cells and solid cells with a fluid
 // neighbour (variational_pressuresolver.cpp:245-321: only fluid cells assemble,
 // and each solid neighbour of a fluid cell receives a row).  Every (j,k) x-line
-// stores its active span [lo, lo+len) rounded out to XFP_ALIGN cells.
+// stores its active span, rounded out to whole groups of XFP_ALIGN cells that
+// are aligned to the wavefront (see xfp_common.cuh).
 #include <climits>
 
 #include "xfp_common.cuh"
@@ -48,7 +49,9 @@ __global__ void line_span_kernel(const uint8_t* __restrict__ mat, int ni, int nj
   if (lane == 0) {
     Line L = {0, 0, 0, 0};
     if (cnt > 0) {
-      L.lo = lo & ~(XFP_ALIGN - 1);
+      // first stored cell S <= lo with S + j + k = 0 (mod XFP_ALIGN): cell i
+      // then sits at an address = i + j + k (mod XFP_ALIGN); S may be < 0
+      L.lo = lo - ((lo + j + k) & (XFP_ALIGN - 1));
       L.len = ((hi + 1 - L.lo) + XFP_ALIGN - 1) & ~(XFP_ALIGN - 1);
       L.nrows = cnt;
     }

@@ -58,7 +58,7 @@ __global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __res
       const size_t c = (size_t)k * nn + (size_t)j * ni + i;
       const size_t o = (size_t)L.off + q;
       AT d = AT(0), bb = AT(0), ox = AT(0), oy = AT(0), oz = AT(0);
-      const uint8_t m = i < ni ? mat[c] : MAT_AIR;
+      const uint8_t m = (i >= 0 && i < ni) ? mat[c] : MAT_AIR;
       if (m == MAT_FLUID || m == MAT_SOLID) {
         // neighbour (di,dj,dk), face value, weight, vsign
         auto face = [&](int nb, AT& uf, AT& mf, AT& vs, int& ii, int& jj, int& kk) -> bool {
@@ -197,7 +197,7 @@ __global__ void gather_compact_kernel(const T* __restrict__ dense, const Line* _
     const Line L = lines[line];
     for (int q = lane; q < L.len; q += 32) {
       const int i = L.lo + q;
-      x[(size_t)L.off + q] = i < ni ? dense[(size_t)line * ni + i] : T(0);
+      x[(size_t)L.off + q] = (i >= 0 && i < ni) ? dense[(size_t)line * ni + i] : T(0);
     }
   }
 }
@@ -311,7 +311,7 @@ __global__ void apply_T_kernel(const uint8_t* __restrict__ mat, const FT* __rest
     for (int qq = lane; qq < L.len; qq += 32) {
       const int i = L.lo + qq;
       PT acc = PT(0);
-      if (i < ni) {
+      if (i >= 0 && i < ni) {
         const uint8_t mc = mat[(size_t)k * nn + (size_t)j * ni + i];
         if (mc == MAT_FLUID || mc == MAT_SOLID) {
           // faces: low/high per axis; c is the right cell of its low face and

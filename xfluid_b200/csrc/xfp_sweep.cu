@@ -117,6 +117,24 @@ __device__ __forceinline__ void st_gpu64(unsigned long long* p, unsigned long lo
 }
 
 
+// Four consecutive cells of an array, from/to a 4-cell-aligned index:
+// one 16-byte access (FP32) or two (FP64).
+__device__ __forceinline__ void ld4(float (&v)[4], const float* p) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ld4(double (&v)[4], const double* p) {
+  const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
 struct Spin {
   long long n = 0;
   __device__ __forceinline__ bool step(const SweepCtl* ctl, long long limit) {
@@ -355,27 +373,13 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
         }
         return cd;
       };
-      const int i0 = REV ? (maxT - Tlo) - s : Tlo - s;
-      // pf[q] holds the data of step base+q; it is refilled for step base+q+PF
-      // right after use and first read again PF steps later (static indices,
-      // no register moves, so the load latency stays hidden).
-      CellData pf[PF];
-#pragma unroll
-      for (int q = 0; q < PF; ++q) pf[q] = load_cell(i0 + q * di);
-
       X out_x{}, out_y{};
       int cons_seen = zdst_in ? (int)s_prog[zdst] : INF_T;   // cached consumer progress
-      for (int base = Tlo; base <= Thi; base += PF) {
-#pragma unroll
-      for (int q = 0; q < PF; ++q) {
-        const int tau = base + q;
-        if (tau > Thi) break;
-        const int i = i0 + (tau - Tlo) * di;
-        const CellData cd = pf[q];
-        pf[q] = load_cell(i + PF * di);
-        const bool in = (unsigned)(i - L.lo) < (unsigned)L.len;
-        const int c = L.off + (i - L.lo);
 
+      // One wavefront step of this lane's line: wait for the values produced
+      // at the previous step, compute the cell and hand its outputs on.  The
+      // forward/backward result goes to yout; the caller stores it.
+      auto step = [&](const int tau, const CellData& cd, const bool in, const int c, VT& yout) {
         // ---- neighbour values produced at the previous step ----
         // z: previous warp (ring) or the loader (kring); j boundary: loader
         // (jring, one word per warp, read by all lanes as a broadcast).
@@ -402,66 +406,120 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
           }
           return ok;
         };
-        fetch();
-        if (!__all_sync(XFP_FULL, ready())) {
-          trace_wait(g, kb ? 2 : 1, tau);
-          Spin sp;
-          do {
-            if (!sp.step(g.ctl, g.spin_limit)) {
-              raise_timeout(g.ctl, kb ? 2 : 1, tpos, tau, OP, wz[0], ez);
-              break;
-            }
-            fetch();
-          } while (!__all_sync(XFP_FULL, ready()));
-          trace_wait(g, 0, tau);
-        }
-        X vz{};
-        if (zneed) {
-          uint32_t w[P];
+        auto wait_inputs = [&]() {
+          fetch();
+          if (!__all_sync(XFP_FULL, ready())) {
+            trace_wait(g, kb ? 2 : 1, tau);
+            Spin sp;
+            do {
+              if (!sp.step(g.ctl, g.spin_limit)) {
+                raise_timeout(g.ctl, kb ? 2 : 1, tpos, tau, OP, wz[0], ez);
+                break;
+              }
+              fetch();
+            } while (!__all_sync(XFP_FULL, ready()));
+            trace_wait(g, 0, tau);
+          }
+        };
+        auto take_z = [&]() -> X {
+          X vz{};
+          if (zneed) {
+            uint32_t w[P];
 #pragma unroll
-          for (int p = 0; p < P; ++p) w[p] = (uint32_t)wz[p];
-          vz = from_words<X>(w);
-        }
-        X vy = REV ? shfl_down_any(out_y) : shfl_up_any(out_y);
-        if (jb) {
+            for (int p = 0; p < P; ++p) w[p] = (uint32_t)wz[p];
+            vz = from_words<X>(w);
+          }
+          return vz;
+        };
+        auto take_j = [&]() -> X {
           uint32_t w[P];
 #pragma unroll
           for (int p = 0; p < P; ++p) w[p] = (uint32_t)wj[p];
-          vy = from_words<X>(w);
-        }
+          return from_words<X>(w);
+        };
+        // ring back-pressure: slot tau%RING last held step tau-RING, which the
+        // consumer reads at step tau-RING+1; its progress is published every
+        // QPUB steps.  Checked before the inputs arrive, off the critical path.
+        auto ring_space = [&]() {
+          if (!zdst_in) return;
+          const int need = tau - RING + 1;
+          if (need > cons_seen && need >= zdst_lo && need <= zdst_hi) {
+            trace_wait(g, 4, tau);
+            Spin sp;
+            while ((cons_seen = s_prog[zdst]) < need) {
+              if (!sp.step(g.ctl, g.spin_limit)) {
+                raise_timeout(g.ctl, 4, tpos, tau, OP, (unsigned long long)(unsigned)cons_seen, (unsigned)need);
+                break;
+              }
+            }
+            trace_wait(g, 0, tau);
+          }
+        };
+        auto ring_put = [&](const X& oz) {
+          if (!zdst_in) return;
+          uint32_t w[P];
+          to_words(oz, w);
+          unsigned long long* slot = myring + (size_t)(tau & (RING - 1)) * P * 32 + lane;
+#pragma unroll
+          for (int p = 0; p < P; ++p) st_vol64(slot + (size_t)p * 32, stamped(tstamp | tau, w[p]));
+        };
 
-        // ---- the cell itself ----
         X o_x{}, o_y{}, o_z{};
         if constexpr (OP == SWEEP_FWD) {
           // solve_lower: columns c-nn, c-ni, c-1 scatter into row c in that
-          // order, then result[c] *= invdiag[c]  (pcg_solver.h:198-203)
-          VT t = cd.r;
-          t = sub_rn(t, mul_rn(cd.lz, vz));
-          t = sub_rn(t, mul_rn(cd.ly, vy));
-          t = sub_rn(t, mul_rn(cd.lx, out_x));
+          // order, then result[c] *= invdiag[c]  (pcg_solver.h:198-203).
+          // Everything that does not need the z value is done before waiting
+          // for it; after it arrives only the dependent chain and the hand-off
+          // to the next warp remain (same roundings, same order).
+          const X vy_sh = REV ? shfl_down_any(out_y) : shfl_up_any(out_y);
+          const VT px = mul_rn(cd.lx, out_x);
+          const VT py_sh = mul_rn(cd.ly, vy_sh);
+          ring_space();
+          wait_inputs();
+          const X vz = take_z();
+          VT py = py_sh;
+          if (jb) py = mul_rn(cd.ly, take_j());
+          VT t = sub_rn(cd.r, mul_rn(cd.lz, vz));
+          t = sub_rn(t, py);
+          t = sub_rn(t, px);
           const VT y = in ? VT(mul_rn((IT)t, cd.inv)) : VT(0);
-          if (in) d.y[c] = y;
+          ring_put(y);
+          yout = y;
           o_x = y; o_y = y; o_z = y;
         } else if constexpr (OP == SWEEP_BWD) {
           // solve_lower_transpose_in_place: x[c] -= L(m,c) x[m] for m = c+1,
           // c+ni, c+nn in that order, then x[c] *= invdiag[c]  (:215-218).
-          // The products L(m,c) x[m] arrive ready-made from the producers.
-          VT t = cd.r;
-          t = sub_rn(t, out_x);
-          t = sub_rn(t, vy);
-          t = sub_rn(t, vz);
+          // The products L(m,c) x[m] arrive ready-made from the producers;
+          // the x and y terms are subtracted before waiting for z.
+          const X vy_sh = REV ? shfl_down_any(out_y) : shfl_up_any(out_y);
+          const VT t1 = sub_rn(cd.r, out_x);
+          const VT t2_sh = sub_rn(t1, vy_sh);
+          ring_space();
+          wait_inputs();
+          const X vz = take_z();
+          VT t2 = t2_sh;
+          if (jb) t2 = sub_rn(t1, take_j());
+          const VT t = sub_rn(t2, vz);
           const VT z = in ? VT(mul_rn((IT)t, cd.inv)) : VT(0);
-          if (in) d.y[c] = z;
+          o_z = mul_rn(in ? cd.lz : VT(0), z);
+          ring_put(o_z);
+          yout = z;
           const VT rr = in ? cd.rr : VT(0);
           if (DOT32) dot_acc_f = __fadd_rn(dot_acc_f, __fmul_rn((float)z, (float)rr));
           else dot_acc = __dadd_rn(dot_acc, __dmul_rn((double)z, (double)rr));
           o_x = mul_rn(in ? cd.lx : VT(0), z);
           o_y = mul_rn(in ? cd.ly : VT(0), z);
-          o_z = mul_rn(in ? cd.lz : VT(0), z);
         } else {
           // factor_modified_incomplete_cholesky0 for column c: updates from
           // columns c-nn, c-ni, c-1 in that order (:137-184), each
           // d -= L*L then d -= omega*L*missing; pivot safeguard (:126-131).
+          // the shuffle runs on every lane (full mask); the j-boundary lane
+          // then takes its value from the loader instead
+          const X vy_sh = REV ? shfl_down_any(out_y) : shfl_up_any(out_y);
+          wait_inputs();
+          const X vz = take_z();
+          X vy = vy_sh;
+          if (jb) vy = take_j();
           const bool act = in && cd.dg != CT(0);
           CT dd = cd.dg;
           const X src[3] = {vz, vy, out_x};
@@ -477,6 +535,8 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
           o_x = {px, add_rn(py, pz)};
           o_y = {py, add_rn(px, pz)};
           o_z = {pz, add_rn(px, py)};
+          ring_space();
+          ring_put(o_z);
           if (act && cd.upx != CT(0)) d.flx[c + 1] = px;
           if (act && cd.cyup >= 0) d.fly[cd.cyup] = py;
           if (act && cd.czup >= 0) d.flz[cd.czup] = pz;
@@ -496,29 +556,6 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
 #pragma unroll
           for (int p = 0; p < P; ++p) st_gpu64(&d.sz[(size_t)c * P + p], stamped(gen, w[p]));
         }
-
-        // ---- hand the z value to the consumer warp (ring back-pressure) ----
-        if (zdst_in) {
-          // slot tau%RING last held step tau-RING, which the consumer reads at
-          // step tau-RING+1; its progress is published every QPUB steps
-          const int need = tau - RING + 1;
-          if (need > cons_seen && need >= zdst_lo && need <= zdst_hi) {
-            trace_wait(g, 4, tau);
-            Spin sp;
-            while ((cons_seen = s_prog[zdst]) < need) {
-              if (!sp.step(g.ctl, g.spin_limit)) {
-                raise_timeout(g.ctl, 4, tpos, tau, OP, (unsigned long long)(unsigned)cons_seen, (unsigned)need);
-                break;
-              }
-            }
-            trace_wait(g, 0, tau);
-          }
-          uint32_t w[P];
-          to_words(o_z, w);
-          unsigned long long* slot = myring + (size_t)(tau & (RING - 1)) * P * 32 + lane;
-#pragma unroll
-          for (int p = 0; p < P; ++p) st_vol64(slot + (size_t)p * 32, stamped(tstamp | tau, w[p]));
-        }
         out_x = o_x;
         out_y = o_y;
         // Progress is published only once every lane has finished the step
@@ -531,7 +568,95 @@ __global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
               *(volatile int*)&g.trace[((size_t)blockIdx.x * (NW + 1) + warp) * 4 + 2] = tau;
           }
         }
-      }
+      };
+
+      if constexpr (OP == SWEEP_FACTOR) {
+        // pf[q] holds the data of step base+q; it is refilled for step
+        // base+q+PF right after use and first read again PF steps later
+        // (static indices, no register moves, so the load latency stays hidden).
+        const int i0 = REV ? (maxT - Tlo) - s : Tlo - s;
+        CellData pf[PF];
+#pragma unroll
+        for (int q = 0; q < PF; ++q) pf[q] = load_cell(i0 + q * di);
+        for (int base = Tlo; base <= Thi; base += PF) {
+#pragma unroll
+          for (int q = 0; q < PF; ++q) {
+            const int tau = base + q;
+            if (tau > Thi) break;
+            const int i = i0 + (tau - Tlo) * di;
+            const CellData cd = pf[q];
+            pf[q] = load_cell(i + PF * di);
+            const bool in = (unsigned)(i - L.lo) < (unsigned)L.len;
+            VT unused;
+            step(tau, cd, in, L.off + (i - L.lo), unused);
+          }
+        }
+      } else {
+        // Grouped access.  A line is stored so that cell (i,j,k) sits at an
+        // address = i+j+k (mod 4): at every wavefront step all lanes of the
+        // warp are at the same position within an aligned group of 4 cells.
+        // Each lane therefore loads the next 4 cells of each array with one
+        // 16-byte (FP32) or 32-byte (FP64) access and stores 4 results at once,
+        // instead of touching one 32-byte sector per array per step.  The group
+        // covering steps t0..t0+3 is loaded 4 steps before use, into the
+        // buffer the previous group has just released (two static buffers, no
+        // register moves).  A group lies entirely inside or outside the span.
+        struct Grp {
+          VT r[4], lx[4], ly[4], lz[4], rr[4];
+          IT inv[4];
+        };
+        // forward: address phase of step t is t mod 4 (increasing cells);
+        // backward: (maxT - t) mod 4, cells decreasing
+        const int a = REV ? ((maxT + 1) & 3) : 0;
+        const int base0 = Tlo - ((Tlo - a) & 3);
+        auto group_c4 = [&](int t0) -> int {
+          const int ilow = REV ? (maxT - (t0 + 3)) - s : t0 - s;
+          const int rel = ilow - L.lo;
+          return (unsigned)rel < (unsigned)L.len ? L.off + rel : -1;
+        };
+        auto load_grp = [&](Grp& G, int c4) {
+          const int cc = c4 >= 0 ? c4 : 0;
+          if constexpr (OP == SWEEP_FWD) {
+            ld4(G.r, d.r + cc);
+          } else {
+            ld4(G.r, d.y + cc);
+            ld4(G.rr, d.r + cc);
+          }
+          ld4(G.lx, d.lx + cc);
+          ld4(G.ly, d.ly + cc);
+          ld4(G.lz, d.lz + cc);
+          ld4(G.inv, d.inv + cc);
+        };
+        auto run_group = [&](int t0, const Grp& G, int c4) {
+          VT yb[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int tau = t0 + q;
+            const int e = REV ? 3 - q : q;
+            yb[e] = VT(0);
+            if (tau >= Tlo && tau <= Thi) {
+              CellData cd;
+              cd.r = G.r[e]; cd.lx = G.lx[e]; cd.ly = G.ly[e]; cd.lz = G.lz[e]; cd.inv = G.inv[e];
+              cd.rr = (OP == SWEEP_BWD) ? G.rr[e] : VT(0);
+              const bool in = c4 >= 0;
+              step(tau, cd, in, (in ? c4 : 0) + e, yb[e]);
+            }
+          }
+          if (c4 >= 0) st4(d.y + c4, yb);
+        };
+        Grp GA, GB;
+        int cA = group_c4(base0);
+        load_grp(GA, cA);
+        for (int gb = base0; gb <= Thi; gb += 8) {
+          const int cB = group_c4(gb + 4);
+          load_grp(GB, cB);
+          run_group(gb, GA, cA);
+          if (gb + 4 > Thi) break;
+          const int cA2 = group_c4(gb + 8);
+          load_grp(GA, cA2);
+          run_group(gb + 4, GB, cB);
+          cA = cA2;
+        }
       }
       __syncwarp();
       if (lane == 0) s_prog[warp] = INF_T;
