@@ -131,7 +131,11 @@ template <typename VT, typename IT, typename CT>
 int run_sweep(xfp_ctx* ctx, int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d) {
   if (g.ntiles <= 0) return XFP_OK;
   int maxg = sweep_max_grid(op, d, ctx->nw);
-  if (maxg <= 0) return fail(ctx, XFP_ERR_CUDA, "sweep kernel cannot be resident");
+  if (maxg <= 0) {
+    const cudaError_t e = cudaGetLastError();
+    return fail(ctx, XFP_ERR_CUDA, std::string("sweep kernel cannot be resident (op ") + std::to_string(op) +
+                                       ", tile height " + std::to_string(ctx->nw) + "): " + cudaGetErrorString(e));
+  }
   int grid = std::min(maxg, g.ntiles);
   const bool timed = op != SWEEP_FACTOR && ctx->sweep_ev_used + 2 <= (int)ctx->sweep_ev.size();
   if (timed) cudaEventRecord(ctx->sweep_ev[ctx->sweep_ev_used], ctx->stream);

@@ -212,16 +212,13 @@ __host__ __device__ constexpr size_t smem_bytes(int nw) {
          sizeof(int) * (4 * (size_t)nw + 8) + sizeof(double) * (nw + 2);
 }
 
-// Two CTAs per SM where the register budget allows it (tile height 8): a
-// 256^3 grid has more tiles than SMs, and a second co-resident CTA also gives
-// each scheduler more warps to hide the step's dependency chain.
-template <int NW>
-struct SweepOcc {
-  static constexpr int MIN_BLOCKS = NW <= 8 ? 2 : 1;
-};
-
+// One CTA per SM is all the bound asks for.  Asking for two made the
+// compiler settle at 96 registers and spill inside the step loop, which cost
+// more than the second CTA gained; with this bound the FP32/mixed sweeps take
+// 104-118 registers without spilling (those at or under 112 still get two
+// CTAs per SM from the occupancy query).
 template <int OP, typename VT, typename IT, typename CT, int NW>
-__global__ void __launch_bounds__((NW + 1) * 32, SweepOcc<NW>::MIN_BLOCKS)
+__global__ void __launch_bounds__((NW + 1) * 32, 1)
     sweep_kernel(SweepGrid g, SweepData<VT, IT, CT> d) {
   using TR = OpTraits<OP, VT, IT, CT>;
   using X = typename TR::X;
