@@ -117,24 +117,25 @@ __device__ __forceinline__ void st_gpu64(unsigned long long* p, unsigned long lo
 }
 
 
-// Four consecutive cells of an array, from/to a 4-cell-aligned index:
-// one 16-byte access (FP32) or two (FP64).
-__device__ __forceinline__ void ld4(float (&v)[4], const float* p) {
+// One group of XFP_ALIGN (4) consecutive cells of an array, from/to a
+// group-aligned index: one 16-byte access (FP32) or two (FP64).  Groups of 8
+// with 32-byte accesses were measured too: faster on long full lines, slower
+// on the 256^3 blob scene (more padding steps, more registers).
+__device__ __forceinline__ void ldg(float (&v)[4], const float* p) {
   const float4 t = *reinterpret_cast<const float4*>(p);
   v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
 }
-__device__ __forceinline__ void ld4(double (&v)[4], const double* p) {
+__device__ __forceinline__ void ldg(double (&v)[4], const double* p) {
   const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
   v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
-__device__ __forceinline__ void st4(float* p, const float (&v)[4]) {
+__device__ __forceinline__ void stg(float* p, const float (&v)[4]) {
   *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
-__device__ __forceinline__ void st4(double* p, const double (&v)[4]) {
+__device__ __forceinline__ void stg(double* p, const double (&v)[4]) {
   reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
   reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
 }
-
 struct Spin {
   long long n = 0;
   __device__ __forceinline__ bool step(const SweepCtl* ctl, long long limit) {
@@ -590,46 +591,48 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
         }
       } else {
         // Grouped access.  A line is stored so that cell (i,j,k) sits at an
-        // address = i+j+k (mod 4): at every wavefront step all lanes of the
-        // warp are at the same position within an aligned group of 4 cells.
-        // Each lane therefore loads the next 4 cells of each array with one
-        // 16-byte (FP32) or 32-byte (FP64) access and stores 4 results at once,
-        // instead of touching one 32-byte sector per array per step.  The group
-        // covering steps t0..t0+3 is loaded 4 steps before use, into the
-        // buffer the previous group has just released (two static buffers, no
-        // register moves).  A group lies entirely inside or outside the span.
+        // address = i+j+k (mod GS): at every wavefront step all lanes of the
+        // warp are at the same position within an aligned group of GS cells.
+        // Each lane therefore loads the next GS cells of each array with
+        // vector accesses and stores GS results at once, instead of touching
+        // one 32-byte sector per array per step.  The group covering steps
+        // t0..t0+GS-1 is loaded GS steps before use, into the buffer the
+        // previous group has just released (two static buffers, no register
+        // moves).  A group lies entirely inside or outside the span.
+        constexpr int GS = XFP_ALIGN;
+        static_assert(GS == 4, "group load/store helpers cover 4-cell groups");
         struct Grp {
-          VT r[4], lx[4], ly[4], lz[4], rr[4];
-          IT inv[4];
+          VT r[GS], lx[GS], ly[GS], lz[GS], rr[GS];
+          IT inv[GS];
         };
-        // forward: address phase of step t is t mod 4 (increasing cells);
-        // backward: (maxT - t) mod 4, cells decreasing
-        const int a = REV ? ((maxT + 1) & 3) : 0;
-        const int base0 = Tlo - ((Tlo - a) & 3);
+        // forward: address phase of step t is t mod GS (increasing cells);
+        // backward: (maxT - t) mod GS, cells decreasing
+        const int a = REV ? ((maxT + 1) & (GS - 1)) : 0;
+        const int base0 = Tlo - ((Tlo - a) & (GS - 1));
         auto group_c4 = [&](int t0) -> int {
-          const int ilow = REV ? (maxT - (t0 + 3)) - s : t0 - s;
+          const int ilow = REV ? (maxT - (t0 + GS - 1)) - s : t0 - s;
           const int rel = ilow - L.lo;
           return (unsigned)rel < (unsigned)L.len ? L.off + rel : -1;
         };
         auto load_grp = [&](Grp& G, int c4) {
           const int cc = c4 >= 0 ? c4 : 0;
           if constexpr (OP == SWEEP_FWD) {
-            ld4(G.r, d.r + cc);
+            ldg(G.r, d.r + cc);
           } else {
-            ld4(G.r, d.y + cc);
-            ld4(G.rr, d.r + cc);
+            ldg(G.r, d.y + cc);
+            ldg(G.rr, d.r + cc);
           }
-          ld4(G.lx, d.lx + cc);
-          ld4(G.ly, d.ly + cc);
-          ld4(G.lz, d.lz + cc);
-          ld4(G.inv, d.inv + cc);
+          ldg(G.lx, d.lx + cc);
+          ldg(G.ly, d.ly + cc);
+          ldg(G.lz, d.lz + cc);
+          ldg(G.inv, d.inv + cc);
         };
         auto run_group = [&](int t0, const Grp& G, int c4) {
-          VT yb[4];
+          VT yb[GS];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
+          for (int q = 0; q < GS; ++q) {
             const int tau = t0 + q;
-            const int e = REV ? 3 - q : q;
+            const int e = REV ? GS - 1 - q : q;
             yb[e] = VT(0);
             if (tau >= Tlo && tau <= Thi) {
               CellData cd;
@@ -639,19 +642,19 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
               step(tau, cd, in, (in ? c4 : 0) + e, yb[e]);
             }
           }
-          if (c4 >= 0) st4(d.y + c4, yb);
+          if (c4 >= 0) stg(d.y + c4, yb);
         };
         Grp GA, GB;
         int cA = group_c4(base0);
         load_grp(GA, cA);
-        for (int gb = base0; gb <= Thi; gb += 8) {
-          const int cB = group_c4(gb + 4);
+        for (int gb = base0; gb <= Thi; gb += 2 * GS) {
+          const int cB = group_c4(gb + GS);
           load_grp(GB, cB);
           run_group(gb, GA, cA);
-          if (gb + 4 > Thi) break;
-          const int cA2 = group_c4(gb + 8);
+          if (gb + GS > Thi) break;
+          const int cA2 = group_c4(gb + 2 * GS);
           load_grp(GA, cA2);
-          run_group(gb + 4, GB, cB);
+          run_group(gb + GS, GB, cB);
           cA = cA2;
         }
       }
