@@ -65,7 +65,7 @@ typedef struct xfp_options {
   double timeout_ms;     /* bound on any device-side wait (0: 2000 ms) */
   int max_refine;        /* mixed: iterative-refinement cycles (0: 20) */
   double inner_tol;      /* mixed: relative residual reduction per cycle (0: 1e-4) */
-  int tile_k;            /* sweep tile height in k-lines: 8 or 16 (0: 8 for one scene, timed per batch shape for batches) */
+  int tile_k;            /* sweep tile height in k-lines: 8, 15 or 16; 0: timed on the first call per grid (or batch) shape and cached */
   void* stream;          /* cudaStream_t to run on; NULL: the context's own stream */
 } xfp_options;
 
@@ -173,8 +173,8 @@ typedef struct xfp_scene {
  * all scenes run in one persistent launch and the PCG iteration is replayed
  * as a CUDA graph.  No reference counterpart: xFluid projects one grid per
  * call (FluidSimulator.cpp:501-509).  With options.tile_k == 0 the sweep tile
- * height is picked per batch shape by timing both heights on the first call
- * (cached in the context).  stats, if not NULL, receives n entries.  Returns
+ * height is picked per batch shape by timing the candidate heights on the
+ * first call (cached in the context).  stats, if not NULL, receives n entries.  Returns
  * XFP_OK when every scene converged, XFP_NOT_CONVERGED when one did not. */
 int xfp_project_batch_f32(xfp_ctx* ctx, int n, const xfp_scene* scenes, xfp_stats* stats);
 int xfp_project_batch_f64(xfp_ctx* ctx, int n, const xfp_scene* scenes, xfp_stats* stats);

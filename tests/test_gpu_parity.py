@@ -255,3 +255,25 @@ def test_full_size_blob_projection_properties(lib_built, oracle_lib):
     b = oracle_lib.assemble(s64)["b"]
     # FP32 output velocities: round-off of the stored faces adds ~1e-7 relative
     assert np.abs(d).max() <= 1e-6 * np.abs(b).max() + 4e-7 * 6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,dtype", [("f64", np.float64), ("mixed", np.float32)])
+def test_results_do_not_depend_on_tile_height(prec, dtype):
+    """The sweep tile height (8, 15, 16 or autotuned) changes only the schedule:
+    cell arithmetic is per line and the z.r reduction runs over lines in a fixed
+    order, so every height gives the same bits."""
+    sc = scenes.blob_scene(dims=(70, 45, 53), seed=9, dtype=dtype)
+    out = {}
+    for tk in (8, 15, 16, 0):
+        ctx = make_ctx(prec, tile_k=tk, tol=1e-8, max_iter=1000)
+        try:
+            rc, p, u, v, w, st = project(ctx, sc, dtype=dtype)
+        finally:
+            ctx.close()
+        assert rc == 0
+        out[tk] = (p, u, st["iterations"], st["tile_k"])
+    assert out[0][3] in (8, 15, 16)
+    for tk in (15, 16, 0):
+        assert out[tk][2] == out[8][2], tk
+        assert np.array_equal(out[tk][0], out[8][0]) and np.array_equal(out[tk][1], out[8][1]), tk

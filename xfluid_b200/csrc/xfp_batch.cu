@@ -14,8 +14,8 @@
 //   * the PCG iteration is captured once as a CUDA graph (check_every
 //     iterations: SpMV+dot, x/r update, forward, backward, rho/beta, s update)
 //     and replayed until every scene has converged or hit its cap.
-//   * the sweep tile height: with options.tile_k == 0 both heights are timed
-//     on the first call for a batch shape and the faster one is cached.
+//   * the sweep tile height: with options.tile_k == 0 the heights 8, 15 and 16
+//     are timed on the first call for a batch shape and the fastest is cached.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -33,7 +33,7 @@ namespace xfp_host {
 
 struct BatchState {
   DevBuf lines, lens, tile_active, scene_tile_lists, counters;
-  DevBuf segs, tiles, tile_scene, tstart, tlist, scal, scal2, part, tols, maxits;
+  DevBuf segs, tiles, tile_scene, scal, scal2, part, tols, maxits;
   DevBuf io, pdense;
   std::vector<BatchSeg> hsegs;
   std::vector<long long> line_base, rows, nlines_act;
@@ -47,7 +47,7 @@ struct BatchState {
 void batch_state_free(BatchState* b) {
   if (!b) return;
   DevBuf* all[] = {&b->lines, &b->lens, &b->tile_active, &b->scene_tile_lists, &b->counters, &b->segs,
-                   &b->tiles, &b->tile_scene, &b->tstart, &b->tlist, &b->scal, &b->scal2, &b->part,
+                   &b->tiles, &b->tile_scene, &b->scal, &b->scal2, &b->part,
                    &b->tols, &b->maxits, &b->io, &b->pdense};
   for (DevBuf* d : all) d->release();
   delete b;
@@ -133,17 +133,10 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
     return a.level != b.level ? a.level < b.level : a.scene != b.scene ? a.scene < b.scene : a.idx < b.idx;
   });
   const int nt = (int)items.size();
-  std::vector<int> tiles(std::max(nt, 1)), tscene(std::max(nt, 1)), tstart(n + 1, 0), tlist(std::max(nt, 1));
+  std::vector<int> tiles(std::max(nt, 1)), tscene(std::max(nt, 1));
   for (int t = 0; t < nt; ++t) {
     tiles[t] = items[t].packed;
     tscene[t] = items[t].scene;
-    tstart[items[t].scene + 1]++;
-  }
-  for (int s = 0; s < n; ++s) tstart[s + 1] += tstart[s];
-  {
-    std::vector<int> fill(tstart.begin(), tstart.end() - 1);
-    // positions in the merged list, in each scene's own order (the merge kept it)
-    for (int t = 0; t < nt; ++t) tlist[fill[tscene[t]]++] = t;
   }
   // per-scene block decomposition of the vector kernels (as a single launch)
   B->hsegs.assign(n, BatchSeg{});
@@ -162,6 +155,7 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
     g.M = Ms;
     g.lines = lines + B->line_base[s];
     g.partials = B->part.as<double>() + (size_t)s * NBLK_MAX;
+    g.line_base = B->line_base[s];
     bl += g.blk_lines;
     bc += g.blk_cells;
   }
@@ -170,15 +164,10 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
   XFP_CUDA(ctx, B->segs.ensure(n * sizeof(BatchSeg)));
   XFP_CUDA(ctx, B->tiles.ensure(tiles.size() * sizeof(int)));
   XFP_CUDA(ctx, B->tile_scene.ensure(tscene.size() * sizeof(int)));
-  XFP_CUDA(ctx, B->tstart.ensure(tstart.size() * sizeof(int)));
-  XFP_CUDA(ctx, B->tlist.ensure(tlist.size() * sizeof(int)));
   XFP_CUDA(ctx, cudaMemcpyAsync(B->segs.p, B->hsegs.data(), n * sizeof(BatchSeg), cudaMemcpyHostToDevice, st));
   XFP_CUDA(ctx, cudaMemcpyAsync(B->tiles.p, tiles.data(), tiles.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   XFP_CUDA(ctx, cudaMemcpyAsync(B->tile_scene.p, tscene.data(), tscene.size() * sizeof(int),
                                 cudaMemcpyHostToDevice, st));
-  XFP_CUDA(ctx, cudaMemcpyAsync(B->tstart.p, tstart.data(), tstart.size() * sizeof(int), cudaMemcpyHostToDevice,
-                                st));
-  XFP_CUDA(ctx, cudaMemcpyAsync(B->tlist.p, tlist.data(), tlist.size() * sizeof(int), cudaMemcpyHostToDevice, st));
   // the host vectors above go out of scope: make the copies complete first
   XFP_CUDA(ctx, cudaStreamSynchronize(st));
   B->n = n;
@@ -188,6 +177,7 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
   ctx->nw = nw;
   ctx->M = B->M;
   ctx->ntiles = nt;
+  ctx->nlines_all = nlines;
   return XFP_OK;
 }
 
@@ -261,12 +251,12 @@ int batch_pcg(xfp_ctx* ctx, BatchState* B, const VT* const A[4], const VT* b, VT
   d.sy = ctx->sy.as<unsigned long long>();
   d.sz = ctx->sz.as<unsigned long long>();
   const SweepGrid g = batch_grid(ctx, B, dsc);
-  const int* tstart = B->tstart.as<int>();
-  const int* tlist = B->tlist.as<int>();
-  const double* tpart = ctx->tpartials.as<double>();
+  const double* lpart = ctx->tpartials.as<double>();
+  // lines of inactive tiles are never written: their partials stay zero
+  XFP_CUDA(ctx, cudaMemsetAsync(ctx->tpartials.p, 0, std::max<long long>(ctx->nlines_all, 1) * sizeof(double), st));
   XFP_CUDA(ctx, (batch_sweep<VT, IT, DT>(ctx, B, SWEEP_FWD, g, d)));
   XFP_CUDA(ctx, (batch_sweep<VT, IT, DT>(ctx, B, SWEEP_BWD, g, d)));
-  XFP_CUDA(ctx, batch_bwd_reduce<DT>(n, tstart, tlist, tpart, dsc, 0, st));
+  XFP_CUDA(ctx, batch_bwd_reduce<DT>(segs, n, lpart, dsc, 0, st));
   XFP_CUDA(ctx, copy_vec<VT>(z, s, (long long)M, st));
   auto iteration = [&]() -> cudaError_t {
     cudaError_t e;
@@ -274,7 +264,7 @@ int batch_pcg(xfp_ctx* ctx, BatchState* B, const VT* const A[4], const VT* b, VT
     if ((e = batch_update_xr<VT>(segs, n, B->blocks_cells, x, r, s, z, dsc, st))) return e;
     if ((e = batch_sweep<VT, IT, DT>(ctx, B, SWEEP_FWD, g, d))) return e;
     if ((e = batch_sweep<VT, IT, DT>(ctx, B, SWEEP_BWD, g, d))) return e;
-    if ((e = batch_bwd_reduce<DT>(n, tstart, tlist, tpart, dsc, 1, st))) return e;
+    if ((e = batch_bwd_reduce<DT>(segs, n, lpart, dsc, 1, st))) return e;
     return batch_update_s<VT>(segs, n, B->blocks_cells, s, z, dsc, st);
   };
   const int K = ctx->opt.check_every > 0 ? ctx->opt.check_every : 8;
@@ -623,7 +613,7 @@ int project_batch(xfp_ctx* ctx, int n, const xfp_scene* scenes, xfp_stats* stats
     } else {
       float best = 0;
       int best_nw = 8;
-      for (int cand : {8, 16}) {
+      for (int cand : {8, 15, 16}) {
         if ((rc = batch_layout<IOT>(ctx, B, S, cand))) return rc;
         if ((rc = ensure_compact(ctx, XFP_PREC_F32))) return rc;
         float ms = 0;

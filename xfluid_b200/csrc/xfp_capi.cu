@@ -65,6 +65,7 @@ int build_layout(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk) {
   ctx->ni = ni; ctx->nj = nj; ctx->nk = nk;
   ctx->NJt = NJt; ctx->NKt = NKt;
   ctx->M = cnt[0]; ctx->rows = cnt[1]; ctx->nlines_act = cnt[2]; ctx->ntiles = cnt[3];
+  ctx->nlines_all = nlines;
   return XFP_OK;
 }
 
@@ -98,7 +99,8 @@ int ensure_compact(xfp_ctx* ctx, int prec) {
   XFP_CUDA(ctx, ctx->scal.ensure(sizeof(PcgScalars)));
   XFP_CUDA(ctx, ctx->scal2.ensure(sizeof(PcgScalars)));
   XFP_CUDA(ctx, ctx->partials.ensure(NBLK_MAX * sizeof(double)));
-  XFP_CUDA(ctx, ctx->tpartials.ensure(std::max<long long>(ctx->ntiles, 1) * sizeof(double)));
+  // z.r partials: one per x-line
+  XFP_CUDA(ctx, ctx->tpartials.ensure(std::max<long long>(ctx->nlines_all, 1) * sizeof(double)));
   // stamped tile-boundary words: 4 per cell; zeroed when (re)allocated so no
   // stale word can carry a live generation
   const size_t sbytes = M * 4 * sizeof(unsigned long long);
@@ -231,6 +233,8 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   XFP_CUDA(ctx, cudaMemsetAsync(dsc, 0, sizeof(PcgScalars), st));
   XFP_CUDA(ctx, copy_vec<VT>(b, r, M, st));
   XFP_CUDA(ctx, absmax_init<VT>(r, M, dsc, ctx->partials.as<double>(), NBLK_MAX, tol, maxit, st));
+  // lines of inactive tiles are never written: their z.r partials stay zero
+  XFP_CUDA(ctx, cudaMemsetAsync(ctx->tpartials.p, 0, std::max<long long>(ctx->nlines_all, 1) * sizeof(double), st));
   SweepData<VT, IT, DT> d;
   d.r = r; d.y = z; d.lx = L[0]; d.ly = L[1]; d.lz = L[2]; d.inv = inv;
   d.partials = ctx->tpartials.as<double>();
@@ -274,6 +278,76 @@ float ev_ms(xfp_ctx* ctx, int a, int b) {
 // Assembles, factors and solves.  On return the solution is in x64 (F64,
 // MIXED) or x32 (F32) in compact layout.  rhs_from_adjoint: when non-null, the
 // assembled b is replaced by G^T g (backward pass) before solving.
+//
+// Tile height (options.tile_k == 0): the first solve of a grid shape builds
+// the layout at each candidate height, assembles and factors in FP32 and
+// times two forward+backward sweep pairs; the fastest height is cached in the
+// context for that shape and precision.
+template <typename IOT>
+int tune_tile_height(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const IOT* du_, const IOT* dv,
+                     const IOT* dw, const IOT* dwu, const IOT* dwv, const IOT* dww) {
+  if (ctx->opt.tile_k != 0) {
+    ctx->nw = ctx->opt.tile_k;
+    return XFP_OK;
+  }
+  const std::string key = std::to_string(ni) + "x" + std::to_string(nj) + "x" + std::to_string(nk) + ":" +
+                          std::to_string(ctx->opt.precision);
+  auto it = ctx->tuned_nw.find(key);
+  if (it != ctx->tuned_nw.end()) {
+    ctx->nw = it->second;
+    return XFP_OK;
+  }
+  cudaStream_t st = ctx->stream;
+  float best = 0.f;
+  int best_nw = 8;
+  cudaEvent_t e0, e1;
+  XFP_CUDA(ctx, cudaEventCreate(&e0));
+  XFP_CUDA(ctx, cudaEventCreate(&e1));
+  int rc = XFP_OK;
+  for (int cand : {8, 15, 16}) {
+    ctx->nw = cand;
+    if ((rc = build_layout(ctx, dmat, ni, nj, nk)) != XFP_OK) break;
+    if ((rc = ensure_compact(ctx, XFP_PREC_F32)) != XFP_OK) break;
+    if (ctx->ntiles == 0) { best_nw = 8; break; }
+    float* A[5];
+    for (int q = 0; q < 5; ++q) A[q] = ctx->A32[q].as<float>();
+    if (assemble<IOT, float>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, ctx->lines.as<Line>(), A[0], A[1], A[2],
+                             A[3], A[4], st) != cudaSuccess) { rc = fail(ctx, XFP_ERR_CUDA, "assembly failed"); break; }
+    float* F[6];
+    for (int q = 0; q < 6; ++q) F[q] = ctx->F32[q].as<float>();
+    const float* Ac[4] = {A[0], A[1], A[2], A[3]};
+    if ((rc = factor<float, float, float>(ctx, Ac, F, ctx->inv32.as<float>(), 0.97f, 0.25f)) != XFP_OK) break;
+    SweepData<float, float, float> d;
+    d.r = A[4]; d.y = ctx->z32.as<float>(); d.lx = F[0]; d.ly = F[1]; d.lz = F[2]; d.inv = ctx->inv32.as<float>();
+    d.partials = ctx->tpartials.as<double>();
+    d.sy = ctx->sy.as<unsigned long long>();
+    d.sz = ctx->sz.as<unsigned long long>();
+    const SweepGrid g = make_grid(ctx, nullptr, 0);
+    const int maxg = sweep_max_grid(SWEEP_FWD, d, cand);
+    if (maxg <= 0) continue;
+    const int grid = std::min(maxg, (int)ctx->ntiles);
+    cudaError_t e = sweep_launch(SWEEP_FWD, g, d, cand, grid, st);   // warm-up
+    if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+    for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
+      e = sweep_launch(SWEEP_FWD, g, d, cand, grid, st);
+      if (e == cudaSuccess) e = sweep_launch(SWEEP_BWD, g, d, cand, grid, st);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { rc = fail(ctx, XFP_ERR_CUDA, std::string("tile height timing: ") + cudaGetErrorString(e)); break; }
+    if ((rc = check_sweep_error(ctx)) != XFP_OK) break;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (cand == 8 || ms < best) { best = ms; best_nw = cand; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != XFP_OK) return rc;
+  ctx->tuned_nw[key] = best_nw;
+  ctx->nw = best_nw;
+  return XFP_OK;
+}
+
 template <typename IOT>
 int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const IOT* du_,
                const IOT* dv, const IOT* dw, const IOT* dwu, const IOT* dwv, const IOT* dww,
@@ -282,6 +356,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
   cudaStream_t st = ctx->stream;
   int rc;
   ev_record(ctx, 0);
+  if ((rc = tune_tile_height<IOT>(ctx, ni, nj, nk, dmat, du_, dv, dw, dwu, dwv, dww)) != XFP_OK) return rc;
   ctx->sweep_ev_used = 0;
   if ((rc = build_layout(ctx, dmat, ni, nj, nk)) != XFP_OK) return rc;
   if ((rc = ensure_compact(ctx, prec)) != XFP_OK) return rc;
@@ -750,7 +825,8 @@ static int validate_options(xfp_ctx* ctx, const xfp_options* o) {
   if (o->precision < XFP_PREC_F64 || o->precision > XFP_PREC_MIXED) return fail(ctx, XFP_ERR_ARGS, "bad precision");
   if (!(o->omega >= 0.0 && o->omega <= 1.0)) return fail(ctx, XFP_ERR_ARGS, "omega must be in [0,1]");
   if (!(o->min_diag_ratio >= 0.0)) return fail(ctx, XFP_ERR_ARGS, "min_diag_ratio must be >= 0");
-  if (o->tile_k != 0 && o->tile_k != 8 && o->tile_k != 16) return fail(ctx, XFP_ERR_ARGS, "tile_k must be 8 or 16");
+  if (o->tile_k != 0 && o->tile_k != 8 && o->tile_k != 15 && o->tile_k != 16)
+    return fail(ctx, XFP_ERR_ARGS, "tile_k must be 0, 8, 15 or 16");
   return XFP_OK;
 }
 

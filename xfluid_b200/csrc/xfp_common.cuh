@@ -52,7 +52,35 @@ struct BatchSeg {
   long long base, M;
   const Line* lines;
   double* partials;                 // this scene's reduction slots
+  long long line_base;              // first line of this scene in the batch's line table
 };
+
+// z.r from one partial per x-line, in an order that depends only on the
+// number of lines (never on the sweep's tile shape): 256 contiguous chunks,
+// each summed in line order, then a fixed pairwise tree.  Called by every
+// thread of a block of at least 256 threads; the sum is returned to all.
+template <bool F32>
+__device__ __forceinline__ double line_sum(const double* __restrict__ part, long long n, double* s) {
+  const int t = threadIdx.x;
+  if (t < 256) {
+    const long long C = (n + 255) / 256, a = (long long)t * C, b = a + C < n ? a + C : n;
+    double acc = 0.0;
+    float accf = 0.f;
+    for (long long q = a; q < b; ++q) {
+      const double v = ((volatile const double*)part)[q];
+      if (F32) accf = __fadd_rn(accf, (float)v); else acc = __dadd_rn(acc, v);
+    }
+    s[t] = F32 ? (double)accf : acc;
+  }
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if (t < h) s[t] = F32 ? (double)__fadd_rn((float)s[t], (float)s[t + h]) : __dadd_rn(s[t], s[t + h]);
+    __syncthreads();
+  }
+  const double r = s[0];
+  __syncthreads();
+  return r;
+}
 
 // Scalars of one PCG solve, resident on the device.
 struct PcgScalars {

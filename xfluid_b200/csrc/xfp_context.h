@@ -4,6 +4,7 @@
 #pragma once
 
 #include <algorithm>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -67,6 +68,7 @@ struct xfp_ctx {
   // sizes of the current layout
   int ni = 0, nj = 0, nk = 0, NJt = 0, NKt = 0, nw = 8;
   long long M = 0, rows = 0, nlines_act = 0, ntiles = 0;
+  long long nlines_all = 0;       // lines of the layout (nj*nk, or the whole batch's)
   xfp::PcgScalars host_sc{};
   // stats
   double ms_setup = 0, ms_factor = 0, ms_solve = 0, ms_apply = 0;
@@ -79,6 +81,8 @@ struct xfp_ctx {
   long long launches = 0;
   // batched scenes (xfp_project_batch_*): buffers, tables and tuning cache
   xfp_host::BatchState* batch = nullptr;
+  // single scenes with options.tile_k == 0: tile height picked per grid shape
+  std::map<std::string, int> tuned_nw;
 };
 
 namespace xfp_host {

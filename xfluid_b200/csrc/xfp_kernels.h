@@ -51,7 +51,7 @@ struct SweepData {
   CT* flz = nullptr;
   IT* oinv = nullptr;
   CT omega = CT(0.97), ratio = CT(0.25);
-  double* partials = nullptr;   // backward: one dot partial per tile
+  double* partials = nullptr;   // backward: one z.r partial per x-line (line table order)
   // Tile-boundary values published for neighbouring tiles: per cell up to 4
   // 64-bit words (32-bit payload chunk | launch generation << 32).
   unsigned long long* sy = nullptr;  // to the j-neighbour tile
@@ -142,12 +142,11 @@ cudaError_t batch_absmax_init(const BatchSeg* segs, int nseg, int blocks, const 
 cudaError_t batch_residual64(const BatchSeg* segs, int nseg, int blocks, const double* diag, const double* ax,
                              const double* ay, const double* az, const double* b, const double* x, double* r,
                              PcgScalars* sc, cudaStream_t st);
-// Per-scene z.r from the backward sweep's per-tile partials, summed in each
-// scene's own tile order; mode 0: rho, mode 1: beta and rho (the single-scene
-// backward epilogue).  scene_tiles lists tile positions scene by scene.
+// Per-scene z.r from the backward sweep's per-line partials (line_sum, the
+// single-scene order); mode 0: rho, mode 1: beta and rho.
 template <typename DT>
-cudaError_t batch_bwd_reduce(int nseg, const int* scene_tile_start, const int* scene_tiles,
-                             const double* tpartials, PcgScalars* sc, int mode, cudaStream_t st);
+cudaError_t batch_bwd_reduce(const BatchSeg* segs, int nseg, const double* line_partials, PcgScalars* sc, int mode,
+                             cudaStream_t st);
 // ---- semi-Lagrangian MAC self-advection and its adjoint (xfp_advect.cu) ----
 template <typename T>
 cudaError_t advect(const T* u, const T* v, const T* w, T* ou, T* ov, T* ow, int ni, int nj, int nk, T c,

@@ -949,22 +949,19 @@ template cudaError_t batch_absmax_init<double>(const BatchSeg*, int, int, const 
 template cudaError_t batch_absmax_init<float>(const BatchSeg*, int, int, const float*, PcgScalars*, double, int,
                                               const double*, const int*, cudaStream_t);
 
-// One thread per scene: the same sequential sum over the scene's tiles, in
-// its own tile order, that the single-scene backward sweep's last CTA does.
+// One block per scene: z.r from the scene's per-line partials with line_sum,
+// the same order the single-scene backward sweep's last CTA uses.
 template <typename DT>
-__global__ void batch_bwd_reduce_kernel(int nseg, const int* __restrict__ start, const int* __restrict__ tiles,
-                                        const double* __restrict__ tpartials, PcgScalars* sc, int mode) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nseg) return;
+__global__ void __launch_bounds__(256) batch_bwd_reduce_kernel(const BatchSeg* __restrict__ segs,
+                                                               const double* __restrict__ lpart, PcgScalars* sc,
+                                                               int mode) {
+  __shared__ double s[256];
+  const int q = blockIdx.x;
   PcgScalars* S = sc + q;
-  if (S->done) return;
-  double acc = 0.0;
-  float accf = 0.f;
-  for (int t = start[q]; t < start[q + 1]; ++t) {
-    const double pv = tpartials[tiles[t]];
-    if (std::is_same<DT, float>::value) accf = __fadd_rn(accf, (float)pv); else acc = __dadd_rn(acc, pv);
-  }
-  const double rho_new = std::is_same<DT, float>::value ? (double)accf : acc;
+  if (*(volatile int*)&S->done) return;
+  const BatchSeg& G = segs[q];
+  const double rho_new = line_sum<std::is_same<DT, float>::value>(lpart + G.line_base, (long long)G.nj * G.nk, s);
+  if (threadIdx.x != 0) return;
   if (mode == 0) {
     S->rho = rho_new;
     if (rho_new == 0.0 || rho_new != rho_new) { S->status = -5; S->done = 1; }
@@ -975,17 +972,14 @@ __global__ void batch_bwd_reduce_kernel(int nseg, const int* __restrict__ start,
   }
 }
 template <typename DT>
-cudaError_t batch_bwd_reduce(int nseg, const int* scene_tile_start, const int* scene_tiles,
-                             const double* tpartials, PcgScalars* sc, int mode, cudaStream_t st) {
+cudaError_t batch_bwd_reduce(const BatchSeg* segs, int nseg, const double* line_partials, PcgScalars* sc, int mode,
+                             cudaStream_t st) {
   ++g_kernel_launches;
-  batch_bwd_reduce_kernel<DT><<<(nseg + 63) / 64, 64, 0, st>>>(nseg, scene_tile_start, scene_tiles, tpartials, sc,
-                                                               mode);
+  batch_bwd_reduce_kernel<DT><<<nseg, 256, 0, st>>>(segs, line_partials, sc, mode);
   return cudaGetLastError();
 }
-template cudaError_t batch_bwd_reduce<double>(int, const int*, const int*, const double*, PcgScalars*, int,
-                                              cudaStream_t);
-template cudaError_t batch_bwd_reduce<float>(int, const int*, const int*, const double*, PcgScalars*, int,
-                                             cudaStream_t);
+template cudaError_t batch_bwd_reduce<double>(const BatchSeg*, int, const double*, PcgScalars*, int, cudaStream_t);
+template cudaError_t batch_bwd_reduce<float>(const BatchSeg*, int, const double*, PcgScalars*, int, cudaStream_t);
 
 __global__ void offset_lines_kernel(Line* __restrict__ lines, long long nlines, long long base) {
   for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nlines;

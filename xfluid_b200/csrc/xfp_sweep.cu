@@ -202,6 +202,7 @@ struct OpTraits {
   static constexpr int LB = 8 / P;      // loader batch (steps polled together)
   static constexpr int PF = 4;  // cell prefetch depth (steps)
   static_assert(RING > QPUB, "ring must be deeper than the progress interval");
+  static_assert(RING * P * 32 * 8 >= 256, "rings must hold the 256-slot line reduction");
   static_assert(LRING >= LB + QPUB - 1, "loader ring too shallow");
 };
 
@@ -253,6 +254,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
     // the tile's grid: the launch's one scene, or its scene of the batch
     int nj = g.nj, nk = g.nk, maxT = g.maxT;
     const Line* lines = g.lines;
+    long long line_base = 0;
     if (g.tile_scene != nullptr) {
       const int sid = g.tile_scene[tpos];
       const BatchSeg& S = g.segs[sid];
@@ -263,6 +265,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
       nk = S.nk;
       maxT = S.ni + S.nj + S.nk;
       lines = S.lines;
+      line_base = S.line_base;
     }
     const int packed = g.tiles[tpos];
     const int J = packed & 0xffff, K = packed >> 16;
@@ -785,31 +788,12 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
     }
 
     // ---------------- tile epilogue: dot partial (backward) ----------------
-    if (OP == SWEEP_BWD) {
-      double v;
-      if (DOT32) {
-        float f = dot_acc_f;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) f = __fadd_rn(f, __shfl_xor_sync(XFP_FULL, f, o));
-        v = f;
-      } else {
-        v = dot_acc;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_xor_sync(XFP_FULL, v, o));
-      }
-      if (lane == 0) s_red[warp] = (warp < NW) ? v : 0.0;
-    }
-    __syncthreads();
-    if (OP == SWEEP_BWD && threadIdx.x == 0) {
-      if (DOT32) {
-        float t = 0.f;
-        for (int w = 0; w < NW; ++w) t = __fadd_rn(t, (float)s_red[w]);
-        d.partials[tpos] = t;
-      } else {
-        double t = 0.0;
-        for (int w = 0; w < NW; ++w) t = __dadd_rn(t, s_red[w]);
-        d.partials[tpos] = t;
-      }
+    // One z.r partial per x-line (each lane sums its own line in cell order),
+    // so the reduction below is the same for every tile height.
+    if (OP == SWEEP_BWD && warp < NW) {
+      const int jl = j0 + lane, kl = k0 + warp;
+      if (jl < nj && kl < nk)
+        d.partials[line_base + (size_t)kl * nj + jl] = DOT32 ? (double)dot_acc_f : dot_acc;
     }
     __syncthreads();
   }
@@ -823,17 +807,12 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
     s_last = (t == gridDim.x - 1);
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
+  if (OP == SWEEP_BWD && g.scal != nullptr && s_last) {
+    // rho_new = z.r over every line, in line order (line_sum)
     __threadfence();
-    if (OP == SWEEP_BWD && g.scal != nullptr) {
-      // deterministic reduction of the per-tile partials: rho_new = z.r
-      double acc = 0.0;
-      float accf = 0.f;
-      for (int t = 0; t < g.ntiles; ++t) {
-        const double pv = ((volatile double*)d.partials)[t];
-        if (DOT32) accf = __fadd_rn(accf, (float)pv); else acc = __dadd_rn(acc, pv);
-      }
-      const double rho_new = DOT32 ? (double)accf : acc;
+    // the rings are idle now (every tile of this CTA is done): 256 doubles of scratch
+    const double rho_new = line_sum<DOT32>(d.partials, (long long)g.nj * g.nk, reinterpret_cast<double*>(ring));
+    if (threadIdx.x == 0) {
       PcgScalars* sc = g.scal;
       if (g.bwd_mode == 0) {
         sc->rho = rho_new;
@@ -843,6 +822,9 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
         sc->rho = rho_new;
       }
     }
+  }
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
     g.ctl->finished = 0;
     __threadfence();
     atomicExch(&g.ctl->gen, gen + 1);
@@ -896,6 +878,7 @@ static cudaError_t launch_op(const SweepGrid& g, const SweepData<VT, IT, CT>& d,
   switch (nw) {
     case 8: return launch_nw<OP, VT, IT, CT, 8>(g, d, grid, st);
     case 16: return launch_nw<OP, VT, IT, CT, 16>(g, d, grid, st);
+    case 15: return launch_nw<OP, VT, IT, CT, 15>(g, d, grid, st);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -906,6 +889,7 @@ static int max_grid_op(int nw) {
   switch (nw) {
     case 8: prepare<OP, VT, IT, CT, 8>(&maxg); break;
     case 16: prepare<OP, VT, IT, CT, 16>(&maxg); break;
+    case 15: prepare<OP, VT, IT, CT, 15>(&maxg); break;
     default: break;
   }
   return maxg;

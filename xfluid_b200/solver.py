@@ -62,7 +62,7 @@ class VariationalPressureSolver:
 
     def __init__(self, precision: str = "f64", device: int = 0, tol: float = 1e-5, max_iter: int = 100,
                  omega: float = 0.97, min_diag_ratio: float = 0.25, check_every: int = 8,
-                 timeout_ms: float = 2000.0, tile_k: int = 8):
+                 timeout_ms: float = 2000.0, tile_k: int = 0):
         o = _lib.default_options()
         o.tol, o.max_iter, o.omega, o.min_diag_ratio = tol, max_iter, omega, min_diag_ratio
         o.precision = _lib.PREC[precision]
