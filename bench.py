@@ -379,7 +379,8 @@ def ours(args, rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "mixed f32/f64",
             "data": "synthetic (seeded blob scene)",
             "config": dict(workload_config(args.n, rows, iters),
-                           parallelism="replicas" if world > 1 else "single GPU"),
+                           parallelism="replicas" if world > 1 else "single GPU",
+                           tile_k=int(last.get("tile_k", 0))),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk.summary(), "accuracy": accs, "forms": forms, "batch": batch}
     if rank == 0:
@@ -465,16 +466,45 @@ def batch_leg(args, rank, world, stream, barrier, max_over_ranks):
             "sharding": f"LPT over {world} rank(s)"}
 
 
+def profile_case(n):
+    """Two mixed-precision projections of the n^3 blob scene, inputs on the device."""
+    import ctypes as C
+    import torch
+    from xfluid_b200 import _lib, scenes
+    sc = scenes.blob_scene(n, seed=SEED, dtype=np.float32)
+    o = _lib.default_options()
+    o.precision, o.tol, o.max_iter, o.device_pointers, o.tile_k = _lib.PREC["mixed"], TOL, MAXIT, 1, 8
+    ctx = _lib.Context(o)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    P = lambda x: C.c_void_p(x.data_ptr())
+    mat, wts = T(sc.mat), [T(a) for a in (sc.wu, sc.wv, sc.ww)]
+    for _ in range(2):
+        vel = [T(a) for a in (sc.u, sc.v, sc.w)]
+        st = _lib.XfpStats()
+        ctx.check(ctx.lib.xfp_project_f32(ctx.ptr, sc.ni, sc.nj, sc.nk, P(mat), *map(P, vel), *map(P, wts), None,
+                                          C.byref(st)))
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": n, "rows": st.rows, "iterations": st.iterations,
+                      "sweep_ms": st.ms_sweeps / max(1, st.sweeps)}))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=25)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes leg")
+    ap.add_argument("--profile-case", type=int, default=0, metavar="N",
+                    help="only project the N^3 blob scene twice (mixed, device-resident) and exit: "
+                         "the small case the ncu captures of the sweep kernels use")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
