@@ -113,6 +113,11 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
   if (base[n] >= (1LL << 31)) return fail(ctx, XFP_ERR_ARGS, "batch too large: more than 2^31 stored cells");
   for (int s = 0; s < n; ++s)
     XFP_CUDA(ctx, offset_lines(lines + B->line_base[s], B->line_base[s + 1] - B->line_base[s], base[s], st));
+  // cell -> line index (line numbers local to each scene's table; cells global)
+  XFP_CUDA(ctx, ctx->cell_line.ensure((std::max<long long>(base[n], 4) + 8) * sizeof(int)));
+  for (int s = 0; s < n; ++s)
+    XFP_CUDA(ctx, build_cell_line(lines + B->line_base[s], B->line_base[s + 1] - B->line_base[s],
+                                  ctx->cell_line.as<int>(), st));
   // merge the scenes' tile lists by wavefront level (each list is already in
   // its own topological order, which the merge keeps)
   std::vector<int> all_tiles(ntile_slots > 0 ? ntile_slots : 1);
@@ -260,7 +265,9 @@ int batch_pcg(xfp_ctx* ctx, BatchState* B, const VT* const A[4], const VT* b, VT
   XFP_CUDA(ctx, copy_vec<VT>(z, s, (long long)M, st));
   auto iteration = [&]() -> cudaError_t {
     cudaError_t e;
-    if ((e = batch_spmv_dot<VT, VT, DT>(segs, n, B->blocks_lines, A[0], A[1], A[2], A[3], s, z, dsc, 0, st))) return e;
+    if ((e = batch_spmv_dot<VT, VT, DT>(segs, n, B->blocks_cells, A[0], A[1], A[2], A[3], s, z,
+                                        ctx->cell_line.as<int>(), dsc, 0, st)))
+      return e;
     if ((e = batch_update_xr<VT>(segs, n, B->blocks_cells, x, r, s, z, dsc, st))) return e;
     if ((e = batch_sweep<VT, IT, DT>(ctx, B, SWEEP_FWD, g, d))) return e;
     if ((e = batch_sweep<VT, IT, DT>(ctx, B, SWEEP_BWD, g, d))) return e;

@@ -66,6 +66,8 @@ int build_layout(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk) {
   ctx->NJt = NJt; ctx->NKt = NKt;
   ctx->M = cnt[0]; ctx->rows = cnt[1]; ctx->nlines_act = cnt[2]; ctx->ntiles = cnt[3];
   ctx->nlines_all = nlines;
+  XFP_CUDA(ctx, ctx->cell_line.ensure((std::max<long long>(ctx->M, 4) + 8) * sizeof(int)));
+  XFP_CUDA(ctx, build_cell_line(ctx->lines.as<Line>(), nlines, ctx->cell_line.as<int>(), ctx->stream));
   return XFP_OK;
 }
 
@@ -249,8 +251,9 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   DT* part = reinterpret_cast<DT*>(ctx->partials.p);
   for (int done_iters = 0;;) {
     for (int q = 0; q < K; ++q) {
-      XFP_CUDA(ctx, (spmv_dot<VT, VT, DT>(A[0], A[1], A[2], A[3], s, z, ctx->lines.as<Line>(), ctx->ni,
-                                          ctx->nj, ctx->nk, M, dsc, part, NBLK_MAX, 0, st)));
+      XFP_CUDA(ctx, (spmv_dot<VT, VT, DT>(A[0], A[1], A[2], A[3], s, z, ctx->lines.as<Line>(),
+                                          ctx->cell_line.as<int>(), ctx->nj, ctx->nk, M, dsc, part, NBLK_MAX, 0,
+                                          st)));
       XFP_CUDA(ctx, (update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), NBLK_MAX, st)));
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g1, d)) != XFP_OK) return rc;
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_BWD, g1, d)) != XFP_OK) return rc;
@@ -777,8 +780,9 @@ int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* c
     XFP_CUDA(ctx, cudaStreamSynchronize(st));
     if ((rc = dump_dense<VT>(ctx, z, out[9]))) return rc;
     if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_BWD, g, d))) return rc;
-    XFP_CUDA(ctx, (spmv_dot<VT, VT, VT>(Av[0], Av[1], Av[2], Av[3], r, qv, ctx->lines.as<Line>(), ctx->ni, ctx->nj,
-                                        ctx->nk, M, nullptr, (VT*)nullptr, NBLK_MAX, 1, st)));
+    XFP_CUDA(ctx, (spmv_dot<VT, VT, VT>(Av[0], Av[1], Av[2], Av[3], r, qv, ctx->lines.as<Line>(),
+                                        ctx->cell_line.as<int>(), ctx->nj, ctx->nk, M, nullptr, (VT*)nullptr,
+                                        NBLK_MAX, 1, st)));
   }
   XFP_CUDA(ctx, cudaStreamSynchronize(st));
   if ((rc = check_sweep_error(ctx))) return rc;
@@ -883,7 +887,7 @@ int xfp_destroy(xfp_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   DevBuf* all[] = {&ctx->io_mat, &ctx->io_u, &ctx->io_v, &ctx->io_w, &ctx->io_wu, &ctx->io_wv, &ctx->io_ww,
                    &ctx->io_p, &ctx->io_gu, &ctx->io_gv, &ctx->io_gw, &ctx->lines, &ctx->lens,
-                   &ctx->tile_active, &ctx->tiles, &ctx->counters, &ctx->inv64, &ctx->inv32, &ctx->x64,
+                   &ctx->tile_active, &ctx->tiles, &ctx->counters, &ctx->cell_line, &ctx->inv64, &ctx->inv32, &ctx->x64,
                    &ctx->r64, &ctx->x32, &ctx->r32, &ctx->s32, &ctx->z32, &ctx->s64, &ctx->z64, &ctx->dense,
                    &ctx->sy, &ctx->sz, &ctx->ctl, &ctx->scal, &ctx->scal2, &ctx->partials, &ctx->tpartials};
   for (DevBuf* b : all) b->release();

@@ -55,7 +55,7 @@ struct xfp_ctx {
   // I/O staging (host-pointer mode)
   DevBuf io_mat, io_u, io_v, io_w, io_wu, io_wv, io_ww, io_p, io_gu, io_gv, io_gw;
   // layout
-  DevBuf lines, lens, tile_active, tiles, counters;
+  DevBuf lines, lens, tile_active, tiles, counters, cell_line;
   // compact arrays
   DevBuf A64[5];                  // diag, ax, ay, az, b (FP64)
   DevBuf A32[5];                  // same in FP32

@@ -103,10 +103,14 @@ cudaError_t rhs_T(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww, 
                   const FT* gw, FT* du, FT* dv, FT* dw, cudaStream_t st);
 
 // PCG vector kernels over the compact arrays (length M).
+// z = A s with the fused dot s.z; one thread per stored cell (cell_line maps a
+// cell to its line).
 template <typename VT, typename AT, typename DT>
-cudaError_t spmv_dot(const AT* diag, const AT* ax, const AT* ay, const AT* az, const VT* s,
-                     VT* z, const Line* lines, int ni, int nj, int nk, long long M,
-                     PcgScalars* sc, DT* partials, int nblk_max, int mode, cudaStream_t st);
+cudaError_t spmv_dot(const AT* diag, const AT* ax, const AT* ay, const AT* az, const VT* s, VT* z,
+                     const Line* lines, const int* cell_line, int nj, int nk, long long M, PcgScalars* sc,
+                     DT* partials, int nblk_max, int mode, cudaStream_t st);
+// cell_line[c] = index of the line storing cell c (for every cell of every line).
+cudaError_t build_cell_line(const Line* lines, long long nlines, int* cell_line, cudaStream_t st);
 template <typename VT, typename DT>
 cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgScalars* sc,
                       double* partials, int nblk_max, cudaStream_t st);
@@ -127,8 +131,8 @@ cudaError_t copy_vec(const T* in, T* out, long long n, cudaStream_t st);
 // nseg scenes, per-scene scalars sc[nseg]); grid = the table's total blocks ----
 template <typename VT, typename AT, typename DT>
 cudaError_t batch_spmv_dot(const BatchSeg* segs, int nseg, int blocks, const AT* diag, const AT* ax,
-                           const AT* ay, const AT* az, const VT* s, VT* z, PcgScalars* sc, int mode,
-                           cudaStream_t st);
+                           const AT* ay, const AT* az, const VT* s, VT* z, const int* cell_line, PcgScalars* sc,
+                           int mode, cudaStream_t st);
 template <typename VT>
 cudaError_t batch_update_xr(const BatchSeg* segs, int nseg, int blocks, VT* x, VT* r, const VT* s,
                             const VT* z, PcgScalars* sc, cudaStream_t st);

@@ -517,56 +517,59 @@ __device__ __forceinline__ int batch_scene_of(const BatchSeg* __restrict__ segs,
 // z = A s (7-point, row order of sparse_matrix.h:264-276: columns c-nn, c-ni,
 // c-1, c, c+1, c+ni, c+nn; absent entries skipped) fused with the partial dot
 // s.z.  mode 0: alpha = rho / (s.z) (pcg_solver.h:269); mode 1: no dot.
-// One warp per x-line; the warp's lanes walk the line span.
+// One thread per stored cell (cell_line gives its line); block partials of the
+// dot are summed in block order by the last block.
 // ---------------------------------------------------------------------------
 template <typename VT, typename AT, typename DT>
 __device__ __forceinline__ void spmv_dot_body(
     unsigned bid, unsigned nblk, const AT* __restrict__ diag, const AT* __restrict__ ax,
     const AT* __restrict__ ay, const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
-    const Line* __restrict__ lines, int ni, int nj, int nk, PcgScalars* sc,
-    DT* __restrict__ partials, int mode) {
+    const Line* __restrict__ lines, const int* __restrict__ cell_line, int nj, int nk, long long base, long long M,
+    PcgScalars* sc, DT* __restrict__ partials, int mode) {
   __shared__ DT sh[32];
   if (sc && *(volatile int*)&sc->done) return;
-  const int lane = threadIdx.x & 31;
-  const long long nlines = (long long)nj * nk;
   DT acc = DT(0);
-  for (long long line = (long long)bid * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
-       line += (long long)nblk * (blockDim.x >> 5)) {
+  for (long long q = (long long)bid * blockDim.x + threadIdx.x; q < M; q += (long long)nblk * blockDim.x) {
+    const size_t c = (size_t)(base + q);
+    const int line = cell_line[c];
     const Line L = lines[line];
-    if (L.len == 0) continue;
-    const int j = (int)(line % nj), k = (int)(line / nj);
-    Line Lym = {0, 0, 0, 0}, Lyp = {0, 0, 0, 0}, Lzm = {0, 0, 0, 0}, Lzp = {0, 0, 0, 0};
-    if (j > 0) Lym = lines[line - 1];
-    if (j + 1 < nj) Lyp = lines[line + 1];
-    if (k > 0) Lzm = lines[line - nj];
-    if (k + 1 < nk) Lzp = lines[line + nj];
-    for (int q = lane; q < L.len; q += 32) {
-      const int i = L.lo + q;
-      const size_t c = (size_t)L.off + q;
-      VT acc_z = VT(0);
-      const VT dz = (VT)az[c], dy = (VT)ay[c], dx = (VT)ax[c], dd = (VT)diag[c];
-      if (dz != VT(0)) acc_z = add_rn(acc_z, mul_rn(dz, s[(size_t)Lzm.off + (i - Lzm.lo)]));
-      if (dy != VT(0)) acc_z = add_rn(acc_z, mul_rn(dy, s[(size_t)Lym.off + (i - Lym.lo)]));
-      if (dx != VT(0)) acc_z = add_rn(acc_z, mul_rn(dx, s[c - 1]));
-      const VT sc_ = s[c];
-      if (dd != VT(0)) acc_z = add_rn(acc_z, mul_rn(dd, sc_));
-      if (q + 1 < L.len) {
-        const VT cx = (VT)ax[c + 1];
-        if (cx != VT(0)) acc_z = add_rn(acc_z, mul_rn(cx, s[c + 1]));
-      }
+    const int i = L.lo + (int)((long long)c - L.off);
+    const int j = line % nj, k = line / nj;
+    VT acc_z = VT(0);
+    const VT dz = (VT)az[c], dy = (VT)ay[c], dx = (VT)ax[c], dd = (VT)diag[c];
+    if (dz != VT(0)) {
+      const Line Lzm = lines[line - nj];
+      acc_z = add_rn(acc_z, mul_rn(dz, s[(size_t)Lzm.off + (i - Lzm.lo)]));
+    }
+    if (dy != VT(0)) {
+      const Line Lym = lines[line - 1];
+      acc_z = add_rn(acc_z, mul_rn(dy, s[(size_t)Lym.off + (i - Lym.lo)]));
+    }
+    if (dx != VT(0)) acc_z = add_rn(acc_z, mul_rn(dx, s[c - 1]));
+    const VT sc_ = s[c];
+    if (dd != VT(0)) acc_z = add_rn(acc_z, mul_rn(dd, sc_));
+    if ((long long)c + 1 < (long long)L.off + L.len) {
+      const VT cx = (VT)ax[c + 1];
+      if (cx != VT(0)) acc_z = add_rn(acc_z, mul_rn(cx, s[c + 1]));
+    }
+    if (j + 1 < nj) {
+      const Line Lyp = lines[line + 1];
       if ((unsigned)(i - Lyp.lo) < (unsigned)Lyp.len) {
         const size_t n = (size_t)Lyp.off + (i - Lyp.lo);
         const VT cy = (VT)ay[n];
         if (cy != VT(0)) acc_z = add_rn(acc_z, mul_rn(cy, s[n]));
       }
+    }
+    if (k + 1 < nk) {
+      const Line Lzp = lines[line + nj];
       if ((unsigned)(i - Lzp.lo) < (unsigned)Lzp.len) {
         const size_t n = (size_t)Lzp.off + (i - Lzp.lo);
         const VT cz = (VT)az[n];
         if (cz != VT(0)) acc_z = add_rn(acc_z, mul_rn(cz, s[n]));
       }
-      z[c] = acc_z;
-      if (mode == 0) acc = add_rn(acc, mul_rn((DT)sc_, (DT)acc_z));
     }
+    z[c] = acc_z;
+    if (mode == 0) acc = add_rn(acc, mul_rn((DT)sc_, (DT)acc_z));
   }
   if (mode != 0) return;
   DT t = block_sum(acc, sh);
@@ -585,44 +588,42 @@ template <typename VT, typename AT, typename DT>
 __global__ void __launch_bounds__(256) spmv_dot_kernel(
     const AT* __restrict__ diag, const AT* __restrict__ ax, const AT* __restrict__ ay,
     const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
-    const Line* __restrict__ lines, int ni, int nj, int nk, PcgScalars* sc,
+    const Line* __restrict__ lines, const int* __restrict__ cell_line, int nj, int nk, long long M, PcgScalars* sc,
     DT* __restrict__ partials, int mode) {
-  spmv_dot_body<VT, AT, DT>(blockIdx.x, gridDim.x, diag, ax, ay, az, s, z, lines, ni, nj, nk, sc, partials, mode);
+  spmv_dot_body<VT, AT, DT>(blockIdx.x, gridDim.x, diag, ax, ay, az, s, z, lines, cell_line, nj, nk, 0, M, sc,
+                            partials, mode);
 }
 template <typename VT, typename AT, typename DT>
 __global__ void __launch_bounds__(256) batch_spmv_dot_kernel(
     const BatchSeg* __restrict__ segs, int nseg, const AT* __restrict__ diag, const AT* __restrict__ ax,
     const AT* __restrict__ ay, const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
-    PcgScalars* sc, int mode) {
-  const int q = batch_scene_of(segs, nseg, true);
+    const int* __restrict__ cell_line, PcgScalars* sc, int mode) {
+  const int q = batch_scene_of(segs, nseg, false);
   const BatchSeg& S = segs[q];
-  spmv_dot_body<VT, AT, DT>(blockIdx.x - S.blk_lines_start, S.blk_lines, diag, ax, ay, az, s, z, S.lines, S.ni,
-                            S.nj, S.nk, sc + q, reinterpret_cast<DT*>(S.partials), mode);
+  spmv_dot_body<VT, AT, DT>(blockIdx.x - S.blk_cells_start, S.blk_cells, diag, ax, ay, az, s, z, S.lines,
+                            cell_line, S.nj, S.nk, S.base, S.M, sc + q, reinterpret_cast<DT*>(S.partials), mode);
 }
 template <typename VT, typename AT, typename DT>
 cudaError_t spmv_dot(const AT* diag, const AT* ax, const AT* ay, const AT* az, const VT* s, VT* z,
-                     const Line* lines, int ni, int nj, int nk, long long M, PcgScalars* sc,
+                     const Line* lines, const int* cell_line, int nj, int nk, long long M, PcgScalars* sc,
                      DT* partials, int nblk_max, int mode, cudaStream_t st) {
-  (void)M;
-  const long long nlines = (long long)nj * nk;
-  int blocks = (int)std::min<long long>((nlines + 7) / 8, (long long)nblk_max);
+  int blocks = (int)std::min<long long>((M + 255) / 256, (long long)nblk_max);
+  if (blocks < 1) blocks = 1;
   ++g_kernel_launches;
-  spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(diag, ax, ay, az, s, z, lines, ni, nj, nk, sc,
+  spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(diag, ax, ay, az, s, z, lines, cell_line, nj, nk, M, sc,
                                                      partials, mode);
   return cudaGetLastError();
 }
 template cudaError_t spmv_dot<double, double, double>(const double*, const double*, const double*,
-                                                      const double*, const double*, double*,
-                                                      const Line*, int, int, int, long long,
-                                                      PcgScalars*, double*, int, int, cudaStream_t);
-template cudaError_t spmv_dot<float, float, float>(const float*, const float*, const float*,
-                                                   const float*, const float*, float*, const Line*,
-                                                   int, int, int, long long, PcgScalars*, float*,
-                                                   int, int, cudaStream_t);
-template cudaError_t spmv_dot<float, float, double>(const float*, const float*, const float*,
-                                                    const float*, const float*, float*, const Line*,
-                                                    int, int, int, long long, PcgScalars*, double*,
-                                                    int, int, cudaStream_t);
+                                                      const double*, const double*, double*, const Line*,
+                                                      const int*, int, int, long long, PcgScalars*, double*, int,
+                                                      int, cudaStream_t);
+template cudaError_t spmv_dot<float, float, float>(const float*, const float*, const float*, const float*,
+                                                   const float*, float*, const Line*, const int*, int, int,
+                                                   long long, PcgScalars*, float*, int, int, cudaStream_t);
+template cudaError_t spmv_dot<float, float, double>(const float*, const float*, const float*, const float*,
+                                                    const float*, float*, const Line*, const int*, int, int,
+                                                    long long, PcgScalars*, double*, int, int, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // x += alpha s ; r += (-alpha) z ; |r|_inf  (pcg_solver.h:270-276).  The last
@@ -896,22 +897,40 @@ cudaError_t residual64(const double* diag, const double* ax, const double* ay, c
 // ---------------------------------------------------------------------------
 template <typename VT, typename AT, typename DT>
 cudaError_t batch_spmv_dot(const BatchSeg* segs, int nseg, int blocks, const AT* diag, const AT* ax,
-                           const AT* ay, const AT* az, const VT* s, VT* z, PcgScalars* sc, int mode,
-                           cudaStream_t st) {
+                           const AT* ay, const AT* az, const VT* s, VT* z, const int* cell_line, PcgScalars* sc,
+                           int mode, cudaStream_t st) {
   ++g_kernel_launches;
-  batch_spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(segs, nseg, diag, ax, ay, az, s, z, sc, mode);
+  batch_spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(segs, nseg, diag, ax, ay, az, s, z, cell_line, sc,
+                                                           mode);
   return cudaGetLastError();
 }
 template cudaError_t batch_spmv_dot<double, double, double>(const BatchSeg*, int, int, const double*,
                                                             const double*, const double*, const double*,
-                                                            const double*, double*, PcgScalars*, int,
+                                                            const double*, double*, const int*, PcgScalars*, int,
                                                             cudaStream_t);
 template cudaError_t batch_spmv_dot<float, float, float>(const BatchSeg*, int, int, const float*, const float*,
                                                          const float*, const float*, const float*, float*,
-                                                         PcgScalars*, int, cudaStream_t);
+                                                         const int*, PcgScalars*, int, cudaStream_t);
 template cudaError_t batch_spmv_dot<float, float, double>(const BatchSeg*, int, int, const float*, const float*,
                                                           const float*, const float*, const float*, float*,
-                                                          PcgScalars*, int, cudaStream_t);
+                                                          const int*, PcgScalars*, int, cudaStream_t);
+
+// cell_line[c] = the line (index in its scene's table) that stores cell c.
+__global__ void cell_line_kernel(const Line* __restrict__ lines, long long nlines, int* __restrict__ cell_line) {
+  const int lane = threadIdx.x & 31;
+  for (long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
+       line += (long long)gridDim.x * (blockDim.x >> 5)) {
+    const Line L = lines[line];
+    for (int q = lane; q < L.len; q += 32) cell_line[(size_t)L.off + q] = (int)line;
+  }
+}
+cudaError_t build_cell_line(const Line* lines, long long nlines, int* cell_line, cudaStream_t st) {
+  if (nlines <= 0) return cudaSuccess;
+  ++g_kernel_launches;
+  cell_line_kernel<<<(unsigned)std::min<long long>((nlines + 7) / 8, 65535LL * 8), 256, 0, st>>>(lines, nlines,
+                                                                                              cell_line);
+  return cudaGetLastError();
+}
 
 template <typename VT>
 cudaError_t batch_update_xr(const BatchSeg* segs, int nseg, int blocks, VT* x, VT* r, const VT* s,
