@@ -208,6 +208,16 @@ int xfp_box_loss_f64(xfp_ctx* ctx, int ni, int nj, int nk, const double* u, cons
 int xfp_box_loss_f32(xfp_ctx* ctx, int ni, int nj, int nk, const float* u, const float* v,
                      const float* w, const double* box, double* loss, float* gu, float* gv, float* gw);
 
+/* Failure-path diagnostic (no reference counterpart): the next MIC(0) sweep
+ * launched on this context waits, at every tile hand-off, for a boundary word
+ * that no producer writes.  Every such wait is bounded (options.timeout_ms):
+ * the first to run out records where it gave up and raises the context's
+ * error flag, every other wait then returns within a few hundred polls, and
+ * the call returns XFP_ERR_TIMEOUT with the site in xfp_last_error().  The
+ * context stays usable; nothing faults.  Needs a grid with more than one
+ * sweep tile.  Used by the tests of the timeout path. */
+int xfp_debug_expire_next_sweep(xfp_ctx* ctx);
+
 /* Diagnostics: runs the internal stages on one scene and returns them on the
  * dense grid (ni*nj*nk doubles each; any output may be NULL), in the
  * context's precision.  Exposes, for verification against the reference:

@@ -277,3 +277,29 @@ def test_results_do_not_depend_on_tile_height(prec, dtype):
     for tk in (15, 16, 0):
         assert out[tk][2] == out[8][2], tk
         assert np.array_equal(out[tk][0], out[8][0]) and np.array_equal(out[tk][1], out[8][1]), tk
+
+
+@pytest.mark.gpu
+def test_expired_wait_is_reported_and_context_recovers():
+    """A sweep whose tile hand-off waits can never be satisfied
+    (xfp_debug_expire_next_sweep) ends with XFP_ERR_TIMEOUT after the bounded
+    wait (20 ms here) instead of hanging; the same context then projects
+    normally, bit-identical to a fresh context."""
+    from xfluid_b200._lib import XFP_ERR_TIMEOUT, XfpError
+    sc = scenes.blob_scene(48, seed=4, dtype=np.float64)
+    ctx = make_ctx("f64", tile_k=8, timeout_ms=20.0, tol=1e-8, max_iter=500)
+    try:
+        assert ctx.lib.xfp_debug_expire_next_sweep(ctx.ptr) == 0
+        with pytest.raises(XfpError) as err:
+            project(ctx, sc)
+        assert err.value.code == XFP_ERR_TIMEOUT and "timed out" in str(err.value)
+        rc, p, u, v, w, st = project(ctx, sc)
+        assert rc == 0
+    finally:
+        ctx.close()
+    fresh = make_ctx("f64", tile_k=8, tol=1e-8, max_iter=500)
+    try:
+        rc2, p2, u2, v2, w2, st2 = project(fresh, sc)
+    finally:
+        fresh.close()
+    assert np.array_equal(p, p2) and np.array_equal(u, u2) and st["iterations"] == st2["iterations"]

@@ -88,6 +88,7 @@ EXPORTS = [
     "xfp_project_backward_f32", "xfp_debug_stages", "xfp_rhs_inf_noalloc_f64",
     "xfp_project_batch_f32", "xfp_project_batch_f64", "xfp_advect_f64", "xfp_advect_f32",
     "xfp_advect_backward_f64", "xfp_advect_backward_f32", "xfp_box_loss_f64", "xfp_box_loss_f32",
+    "xfp_debug_expire_next_sweep",
 ]
 
 
@@ -126,6 +127,7 @@ def load() -> C.CDLL:
         getattr(L, "xfp_advect_backward_" + sfx).argtypes = [vp, C.c_int, C.c_int, C.c_int] + [vp] * 9 + [C.c_double]
         getattr(L, "xfp_box_loss_" + sfx).argtypes = [vp, C.c_int, C.c_int, C.c_int] + [vp] * 3 + [
             C.POINTER(C.c_double), C.POINTER(C.c_double)] + [vp] * 3
+    L.xfp_debug_expire_next_sweep.argtypes = [vp]
     L.xfp_rhs_inf_noalloc_f64.argtypes = [C.c_int] * 3 + [vp] * 9 + [C.c_char_p, C.c_size_t]
     for name in EXPORTS:
         f = getattr(L, name)

@@ -143,7 +143,12 @@ int run_sweep(xfp_ctx* ctx, int op, const SweepGrid& g, const SweepData<VT, IT, 
   int grid = std::min(maxg, g.ntiles);
   const bool timed = op != SWEEP_FACTOR && ctx->sweep_ev_used + 2 <= (int)ctx->sweep_ev.size();
   if (timed) cudaEventRecord(ctx->sweep_ev[ctx->sweep_ev_used], ctx->stream);
-  XFP_CUDA(ctx, sweep_launch(op, g, d, ctx->nw, grid, ctx->stream));
+  SweepGrid gl = g;
+  if (ctx->expire_next_sweep) {
+    gl.expect_bias = 1;
+    ctx->expire_next_sweep = false;
+  }
+  XFP_CUDA(ctx, sweep_launch(op, gl, d, ctx->nw, grid, ctx->stream));
   if (timed) {
     cudaEventRecord(ctx->sweep_ev[ctx->sweep_ev_used + 1], ctx->stream);
     ctx->sweep_ev_used += 2;
@@ -383,6 +388,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     for (int q = 0; q < 6; ++q) F[q] = ctx->F64[q].as<double>();
     const double* Ac[4] = {A[0], A[1], A[2], A[3]};
     if ((rc = factor<double, double, double>(ctx, Ac, F, ctx->inv64.as<double>(), omega, ratio)) != XFP_OK) return rc;
+    if ((rc = check_sweep_error(ctx)) != XFP_OK) return rc;
     ev_record(ctx, 2);
     const double* Lc[3] = {F[0], F[1], F[2]};
     rc = pcg<double, double, double>(ctx, Ac, A[4], ctx->x64.as<double>(), ctx->r64.as<double>(),
@@ -403,6 +409,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     const float* Ac[4] = {A[0], A[1], A[2], A[3]};
     if ((rc = factor<float, float, float>(ctx, Ac, F, ctx->inv32.as<float>(), (float)omega, (float)ratio)) != XFP_OK)
       return rc;
+    if ((rc = check_sweep_error(ctx)) != XFP_OK) return rc;
     ev_record(ctx, 2);
     const float* Lc[3] = {F[0], F[1], F[2]};
     rc = pcg<float, float, float>(ctx, Ac, A[4], ctx->x32.as<float>(), ctx->r32.as<float>(), ctx->s32.as<float>(),
@@ -427,6 +434,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     for (int q = 0; q < 6; ++q) F[q] = ctx->F64[q].as<double>();
     const double* Ac[4] = {A[0], A[1], A[2], A[3]};
     if ((rc = factor<float, double, double>(ctx, Ac, F, ctx->inv64.as<double>(), omega, ratio)) != XFP_OK) return rc;
+    if ((rc = check_sweep_error(ctx)) != XFP_OK) return rc;
     for (int q = 0; q < 3; ++q) XFP_CUDA(ctx, (convert<double, float>(F[q], ctx->L32[q].as<float>(), M, st)));
     ev_record(ctx, 2);
     const float* Lc[3] = {ctx->L32[0].as<float>(), ctx->L32[1].as<float>(), ctx->L32[2].as<float>()};
@@ -1035,3 +1043,9 @@ int xfp_project_backward_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t
 }
 
 }  // extern "C"
+
+extern "C" int xfp_debug_expire_next_sweep(xfp_ctx* ctx) {
+  if (!ctx) return XFP_ERR_ARGS;
+  ctx->expire_next_sweep = true;
+  return XFP_OK;
+}

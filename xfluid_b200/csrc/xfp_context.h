@@ -83,6 +83,8 @@ struct xfp_ctx {
   xfp_host::BatchState* batch = nullptr;
   // single scenes with options.tile_k == 0: tile height picked per grid shape
   std::map<std::string, int> tuned_nw;
+  // xfp_debug_expire_next_sweep: the next sweep launch's boundary waits run out
+  bool expire_next_sweep = false;
 };
 
 namespace xfp_host {

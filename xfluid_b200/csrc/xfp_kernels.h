@@ -30,6 +30,10 @@ struct SweepGrid {
   const int* tile_scene = nullptr;
   const BatchSeg* segs = nullptr;
   PcgScalars* scal_batch = nullptr;
+  // Diagnostic (xfp_debug_expire_next_sweep): the loaders expect boundary
+  // words stamped with generation + expect_bias, which no producer writes, so
+  // their bounded waits run out.  0 in normal operation.
+  unsigned expect_bias = 0;
 };
 
 // Arrays of one sweep.  VT: vector/L type of the solves, IT: invdiag type,

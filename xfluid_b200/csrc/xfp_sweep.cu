@@ -739,6 +739,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
           }
         }
         const int nsteps = min(LB, tileHi - base + 1);
+        const unsigned want = gen + g.expect_bias;   // bias != 0 only in the expired-wait diagnostic
         int fwd = 0;   // steps of this batch already forwarded (a prefix)
         Spin s2;
         for (;;) {
@@ -748,8 +749,8 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
               bool rdy = true;
 #pragma unroll
               for (int p = 0; p < P; ++p) {
-                rdy &= !needj(q) || (uint32_t)(vj[q][p] >> 32) == gen;
-                rdy &= !needk(q) || (uint32_t)(vk[q][p] >> 32) == gen;
+                rdy &= !needj(q) || (uint32_t)(vj[q][p] >> 32) == want;
+                rdy &= !needk(q) || (uint32_t)(vk[q][p] >> 32) == want;
               }
               if (rdy) {
                 const uint32_t st = tstamp | (base + q);
@@ -768,7 +769,7 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
           }
           if (fwd >= nsteps) break;
           if (!s2.step(g.ctl, g.spin_limit)) {
-            raise_timeout(g.ctl, 6, tpos, base + fwd, OP, 0ull, gen);
+            raise_timeout(g.ctl, 6, tpos, base + fwd, OP, 0ull, want);
             break;
           }
           trace_wait(g, 6, base + fwd);
@@ -777,8 +778,8 @@ __global__ void __launch_bounds__((NW + 1) * 32, 1)
             if (q >= fwd) {
 #pragma unroll
               for (int p = 0; p < P; ++p) {
-                if (needj(q) && (uint32_t)(vj[q][p] >> 32) != gen) vj[q][p] = ld_gpu64(&d.sy[oj(q) + p]);
-                if (needk(q) && (uint32_t)(vk[q][p] >> 32) != gen) vk[q][p] = ld_gpu64(&d.sz[ok_(q) + p]);
+                if (needj(q) && (uint32_t)(vj[q][p] >> 32) != want) vj[q][p] = ld_gpu64(&d.sy[oj(q) + p]);
+                if (needk(q) && (uint32_t)(vk[q][p] >> 32) != want) vk[q][p] = ld_gpu64(&d.sz[ok_(q) + p]);
               }
             }
           }
