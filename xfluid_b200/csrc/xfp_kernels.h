@@ -62,6 +62,13 @@ struct SweepData {
   unsigned long long* sz = nullptr;  // to the k-neighbour tile
 };
 
+// Forward/backward solves (xfp_solve.cu); sweep_launch routes them there.
+template <typename VT, typename IT, typename CT>
+cudaError_t solve_launch(int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d, int nw, int grid,
+                         cudaStream_t st);
+template <typename VT, typename IT, typename CT>
+int solve_max_grid(int op, int nw);
+
 #define XFP_SWEEP_DECL(VT, IT, CT)                                                             \
   cudaError_t sweep_launch(int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d, int nw, \
                            int grid, cudaStream_t st);                                         \

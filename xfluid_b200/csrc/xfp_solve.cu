@@ -1,0 +1,581 @@
+// xfp_solve.cu -- forward and backward triangular solves of the MIC(0)
+// preconditioner in xFluid's natural (lexicographic) order, as wavefronts that
+// advance in lockstep: one CTA barrier per wavefront step.
+//
+// Reference semantics (xFluid/xFluid/variationalpressure/pcg_solver.h):
+//   forward  solve_lower (column-scatter L y = r)  :192-204
+//   backward solve_lower_transpose_in_place        :207-220
+// Every update is applied in the reference's column order with separately
+// rounded multiplies and subtractions, so the FP64 path is bit-identical to
+// the reference (the factorisation is in xfp_sweep.cu).
+//
+// Work decomposition (the same tiles as the factorisation).  A thread owns
+// one x-line (j,k) and walks it in i; a warp holds 32 consecutive j at one k;
+// a CTA holds a tile of 32 x NW lines.  Cell (i,j,k) is processed at
+// wavefront step tau = i+j+k (mirrored for the backward solve), so at step
+// tau a thread needs
+//   x-neighbour  its own result of step tau-1          (register)
+//   y-neighbour  the neighbouring lane's, step tau-1    (warp shuffle)
+//   z-neighbour  the neighbouring warp's, step tau-1    (shared memory)
+// and values from the neighbouring tiles, brought in by a loader warp.
+//
+// Lockstep.  Every compute warp runs every step of the tile's step range
+// (cells outside a lane's line are masked to zero) and the step ends at a
+// named barrier shared by the compute warps and a gate warp.  After barrier
+// tau every z-value of step tau-1 is in shared memory, so the ring between
+// warps is a plain double buffer: no stamps, no polling, no back-pressure on
+// the per-step path.  A warp-to-warp hand-off costs one barrier, against a
+// poll/vote round trip per step for a dataflow pipeline.
+//
+// Tile boundaries.  Producers publish boundary values in global memory as
+// 64-bit words stamped with the launch generation (single-copy atomic, so no
+// fence is needed).  The loader warp polls them ahead of the compute warps,
+// batch by batch, and forwards every step as soon as its stamps are current
+// into a shared ring of plain values; it then raises its progress word.  The
+// gate warp lets barrier tau complete only once the loader has forwarded
+// step tau, and reports the steps the compute warps have finished, which the
+// loader needs before reusing a ring slot.
+//
+// Tiles are visited in topological order (J+K ascending) and assigned
+// round-robin to a fully co-resident grid (cooperative launch), so a CTA only
+// waits on tiles that earlier CTAs hold.  The loader's and the gate's waits
+// are bounded (spin_limit polls); on expiry the kernel records SweepCtl::err,
+// every other wait gives up quickly, all warps still reach the same barriers
+// and the host reports XFP_ERR_TIMEOUT.
+#include "xfp_sweep_util.cuh"
+
+namespace xfp {
+namespace {
+
+constexpr int SRING = 32;   // loader ring depth (steps)
+constexpr int SLB = 8;      // loader batch: steps polled together
+static_assert(SRING >= SLB + 1, "the loader could wait for a slot the gate cannot free");
+
+__device__ __forceinline__ void step_barrier(int nthreads) {
+  asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+template <typename VT, int NW>
+struct SolveShared {
+  VT zr[2][NW][32];   // z hand-off between warps, by step parity
+  VT kr[SRING][32];   // k-boundary values from the loader, by step
+  VT jr[SRING][NW];   // j-boundary values from the loader, by step
+  int tlo[NW], thi[NW];
+  int lo, hi, last;
+  volatile int lprog;   // last step the loader has forwarded
+  volatile int gate;    // last step every compute warp has finished
+};
+
+template <int OP, typename VT, typename IT, typename CT, int NW>
+__global__ void __launch_bounds__((NW + 2) * 32, 1)
+    solve_kernel(SweepGrid g, SweepData<VT, IT, CT> d) {
+  constexpr bool REV = (OP == SWEEP_BWD);
+  constexpr int P = Words<VT>::P;
+  constexpr bool DOT32 = std::is_same<VT, float>::value && !std::is_same<IT, double>::value;
+  constexpr int GATE = NW, LOADER = NW + 1;
+  constexpr int NT = (NW + 1) * 32;   // threads at the per-step barrier: compute warps + gate
+  constexpr int GS = XFP_ALIGN;
+  static_assert(GS == 4, "group load/store helpers cover 4-cell groups");
+  static_assert(sizeof(VT) * SRING * 32 >= 256 * sizeof(double), "kr doubles as line_sum scratch");
+  __shared__ __align__(16) SolveShared<VT, NW> sh;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned gen = ld_volatile_u32(&g.ctl->gen);
+
+  if (g.scal != nullptr && *(volatile int*)&g.scal->done != 0) return;
+
+  for (int pos = blockIdx.x, seq = 0; pos < g.ntiles; pos += gridDim.x, ++seq) {
+    const int tpos = REV ? g.ntiles - 1 - pos : pos;
+    // the tile's grid: the launch's one scene, or its scene of the batch
+    int nj = g.nj, nk = g.nk, maxT = g.maxT;
+    const Line* lines = g.lines;
+    long long line_base = 0;
+    if (g.tile_scene != nullptr) {
+      const int sid = g.tile_scene[tpos];
+      const BatchSeg& S = g.segs[sid];
+      // a converged scene's tiles are skipped (its scalars only change between
+      // launches, so every CTA of this launch decides the same way)
+      if (g.scal_batch != nullptr && *(volatile int*)&g.scal_batch[sid].done != 0) continue;
+      nj = S.nj;
+      nk = S.nk;
+      maxT = S.ni + S.nj + S.nk;
+      lines = S.lines;
+      line_base = S.line_base;
+    }
+    const int packed = g.tiles[tpos];
+    const int J = packed & 0xffff, K = packed >> 16;
+    const int j0 = J * 32, k0 = K * NW;
+
+    // ---------------- setup: wavefront ranges, cleared hand-off ring ----------------
+    Line L = {0, 0, 0, 0};
+    int s = 0;
+    if (warp < NW) {
+      const int j = j0 + lane, k = k0 + warp;
+      if (j < nj && k < nk) L = lines[(size_t)k * nj + j];
+      s = j + k;
+      int tl = INF_T, th = INT_MIN;
+      if (L.len > 0) {
+        const int a = L.lo + s, b = L.lo + L.len - 1 + s;
+        if (!REV) { tl = a; th = b; } else { tl = maxT - b; th = maxT - a; }
+      }
+      const int Tlo = __reduce_min_sync(XFP_FULL, tl);
+      const int Thi = __reduce_max_sync(XFP_FULL, th);
+      if (lane == 0) {
+        sh.tlo[warp] = Tlo;
+        sh.thi[warp] = Thi;
+      }
+    }
+    for (int q = threadIdx.x; q < 2 * NW * 32; q += blockDim.x) (&sh.zr[0][0][0])[q] = VT(0);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int lo = INF_T, hi = INT_MIN;
+      for (int w = 0; w < NW; ++w) {
+        lo = min(lo, sh.tlo[w]);
+        hi = max(hi, sh.thi[w]);
+      }
+      sh.lo = lo;
+      sh.hi = hi;
+      sh.lprog = lo - 1;
+      sh.gate = lo - 1;
+    }
+    __syncthreads();
+    const int tileLo = sh.lo, tileHi = sh.hi;
+
+    double dot_acc = 0.0;
+    float dot_acc_f = 0.0f;
+
+    if (tileLo != INF_T && warp < NW && sh.tlo[warp] == INF_T) {
+      // a warp without cells in this tile only keeps the barrier count (its
+      // ring slots stay zero)
+      for (int tau = tileLo; tau <= tileHi; ++tau) step_barrier(NT);
+    } else if (tileLo != INF_T && warp < NW) {
+      // ======================= compute warp =======================
+      const int zsrc = REV ? warp + 1 : warp - 1;   // producer warp in this tile (or the loader)
+      const int zdst = REV ? warp - 1 : warp + 1;   // consumer warp in this tile
+      const bool kb = zsrc < 0 || zsrc >= NW;        // fed by the loader (k boundary)
+      const bool zdst_in = zdst >= 0 && zdst < NW;
+      const bool jb = REV ? (lane == 31) : (lane == 0);    // fed by the loader (j boundary)
+      const bool jpub = REV ? (lane == 0) : (lane == 31);  // publish for the j-neighbour tile
+      const bool kpub = REV ? (warp == 0) : (warp == NW - 1);
+
+      VT out_x = VT(0), out_y = VT(0);
+
+      // Grouped access.  A line is stored so that cell (i,j,k) sits at an
+      // address = i+j+k (mod GS): at every wavefront step all lanes are at the
+      // same position within an aligned group of GS cells, so each lane loads
+      // the next GS cells of each array with vector accesses and stores GS
+      // results at once.  The group of steps t0..t0+GS-1 is loaded one group
+      // ahead into the buffer the previous group has just released.  A group
+      // lies entirely inside or outside a line.
+      struct Grp {
+        VT r[GS], lx[GS], ly[GS], lz[GS], rr[GS];
+        IT inv[GS];
+      };
+      // forward: address phase of step t is t mod GS (increasing cells);
+      // backward: (maxT - t) mod GS, cells decreasing
+      const int a = REV ? ((maxT + 1) & (GS - 1)) : 0;
+      const int base0 = tileLo - ((tileLo - a) & (GS - 1));
+      auto group_c4 = [&](int t0) -> int {
+        const int ilow = REV ? (maxT - (t0 + GS - 1)) - s : t0 - s;
+        const int rel = ilow - L.lo;
+        return (unsigned)rel < (unsigned)L.len ? L.off + rel : -1;
+      };
+      auto load_grp = [&](Grp& G, int c4) {
+        const int cc = c4 >= 0 ? c4 : 0;
+        if constexpr (OP == SWEEP_FWD) {
+          ldg(G.r, d.r + cc);
+        } else {
+          ldg(G.r, d.y + cc);
+          ldg(G.rr, d.r + cc);
+        }
+        ldg(G.lx, d.lx + cc);
+        ldg(G.ly, d.ly + cc);
+        ldg(G.lz, d.lz + cc);
+        ldg(G.inv, d.inv + cc);
+      };
+
+      // One wavefront step: everything that needs only this warp's previous
+      // step is done before the barrier; after it, the z and boundary inputs
+      // of step tau-1 are in shared memory.
+      auto step = [&](const int tau, const Grp& G, const int e, const bool in, const int c) -> VT {
+        const VT vy_sh = REV ? shfl_down_any(out_y) : shfl_up_any(out_y);
+        const int slot = tau & (SRING - 1);
+        VT res;
+        if constexpr (OP == SWEEP_FWD) {
+          // solve_lower: columns c-nn, c-ni, c-1 scatter into row c in that
+          // order, then result[c] *= invdiag[c]  (pcg_solver.h:198-203)
+          const VT px = mul_rn(G.lx[e], out_x);
+          const VT py_sh = mul_rn(G.ly[e], vy_sh);
+          step_barrier(NT);
+          const VT vz = kb ? sh.kr[slot][lane] : sh.zr[(tau - 1) & 1][zsrc][lane];
+          const VT vj = sh.jr[slot][warp];
+          const VT py = jb ? mul_rn(G.ly[e], vj) : py_sh;
+          VT t = sub_rn(G.r[e], mul_rn(G.lz[e], vz));
+          t = sub_rn(t, py);
+          t = sub_rn(t, px);
+          const VT y = in ? VT(mul_rn((IT)t, G.inv[e])) : VT(0);
+          if (zdst_in) sh.zr[tau & 1][warp][lane] = y;
+          out_x = y;
+          out_y = y;
+          res = y;
+          if (in && jpub) {
+            uint32_t w[P];
+            to_words(y, w);
+#pragma unroll
+            for (int p = 0; p < P; ++p) st_gpu64(&d.sy[(size_t)c * P + p], stamped(gen, w[p]));
+          }
+          if (in && kpub) {
+            uint32_t w[P];
+            to_words(y, w);
+#pragma unroll
+            for (int p = 0; p < P; ++p) st_gpu64(&d.sz[(size_t)c * P + p], stamped(gen, w[p]));
+          }
+        } else {
+          // solve_lower_transpose_in_place: x[c] -= L(m,c) x[m] for m = c+1,
+          // c+ni, c+nn in that order, then x[c] *= invdiag[c]  (:215-218).
+          // The products L(m,c) x[m] arrive ready-made from the producers.
+          const VT t1 = sub_rn(G.r[e], out_x);
+          const VT t2_sh = sub_rn(t1, vy_sh);
+          step_barrier(NT);
+          const VT vz = kb ? sh.kr[slot][lane] : sh.zr[(tau - 1) & 1][zsrc][lane];
+          const VT vj = sh.jr[slot][warp];
+          const VT t2 = jb ? sub_rn(t1, vj) : t2_sh;
+          const VT t = sub_rn(t2, vz);
+          const VT z = in ? VT(mul_rn((IT)t, G.inv[e])) : VT(0);
+          const VT oz = mul_rn(in ? G.lz[e] : VT(0), z);
+          if (zdst_in) sh.zr[tau & 1][warp][lane] = oz;
+          const VT rr = in ? G.rr[e] : VT(0);
+          if (DOT32) dot_acc_f = in ? __fadd_rn(dot_acc_f, __fmul_rn((float)z, (float)rr)) : dot_acc_f;
+          else dot_acc = in ? __dadd_rn(dot_acc, __dmul_rn((double)z, (double)rr)) : dot_acc;
+          const VT ox = mul_rn(in ? G.lx[e] : VT(0), z);
+          const VT oy = mul_rn(in ? G.ly[e] : VT(0), z);
+          out_x = ox;
+          out_y = oy;
+          res = z;
+          if (in && jpub) {
+            uint32_t w[P];
+            to_words(oy, w);
+#pragma unroll
+            for (int p = 0; p < P; ++p) st_gpu64(&d.sy[(size_t)c * P + p], stamped(gen, w[p]));
+          }
+          if (in && kpub) {
+            uint32_t w[P];
+            to_words(oz, w);
+#pragma unroll
+            for (int p = 0; p < P; ++p) st_gpu64(&d.sz[(size_t)c * P + p], stamped(gen, w[p]));
+          }
+        }
+        return res;
+      };
+      auto run_group = [&](int t0, const Grp& G, int c4) {
+        VT yb[GS];
+        const bool in = c4 >= 0;
+        const int cc = in ? c4 : 0;
+#pragma unroll
+        for (int q = 0; q < GS; ++q) {
+          const int tau = t0 + q;
+          const int e = REV ? GS - 1 - q : q;
+          yb[e] = VT(0);
+          if (tau >= tileLo && tau <= tileHi) yb[e] = step(tau, G, e, in, cc + e);
+        }
+        if (in) stg(d.y + c4, yb);
+      };
+      Grp GA, GB;
+      int cA = group_c4(base0);
+      load_grp(GA, cA);
+      for (int gb = base0; gb <= tileHi; gb += 2 * GS) {
+        const int cB = group_c4(gb + GS);
+        load_grp(GB, cB);
+        run_group(gb, GA, cA);
+        if (gb + GS > tileHi) break;
+        const int cA2 = group_c4(gb + 2 * GS);
+        load_grp(GA, cA2);
+        run_group(gb + GS, GB, cB);
+        cA = cA2;
+      }
+    } else if (tileLo != INF_T && warp == GATE) {
+      // ======================= gate warp =======================
+      // Barrier tau completes only once the loader has forwarded step tau;
+      // after it, every compute warp has finished step tau-1.
+      int seen = tileLo - 1;
+      for (int tau = tileLo; tau <= tileHi; ++tau) {
+        if (seen < tau) {
+          if (lane == 0) {
+            seen = sh.lprog;
+            if (seen < tau) {
+              trace_wait(g, 7, tau);
+              Spin sp;
+              while ((seen = sh.lprog) < tau) {
+                if (!sp.step(g.ctl, g.spin_limit)) {
+                  raise_timeout(g.ctl, 7, tpos, tau, OP, (unsigned long long)(unsigned)seen, (unsigned)tau);
+                  seen = tileHi;   // proceed: results are void, the host reports the timeout
+                  break;
+                }
+              }
+              trace_wait(g, 0, tau);
+            }
+          }
+          seen = __shfl_sync(XFP_FULL, seen, 0);
+        }
+        step_barrier(NT);
+        if (lane == 0) sh.gate = tau - 1;
+      }
+    } else if (tileLo != INF_T && warp == LOADER) {
+      // ======================= loader warp =======================
+      // lane r < NW feeds jr column r (line k0+r); every lane l feeds kr
+      // column l (line j0+l).  Sources are the neighbouring tiles' stamped
+      // boundary values (global), or zero where the source cell has no row.
+      const int jc = REV ? j0 + 31 : j0, js = REV ? j0 + 32 : j0 - 1;
+      const int kc = REV ? k0 + NW - 1 : k0, ks = REV ? k0 + NW : k0 - 1;
+      Line Ljs = {0, 0, 0, 0};
+      int sj_c = 0, Sj_lo = INF_T, Sj_hi = INT_MIN;
+      {
+        const int kr_ = k0 + lane;
+        if (lane < NW && kr_ < nk && js >= 0 && js < nj) Ljs = lines[(size_t)kr_ * nj + js];
+        sj_c = jc + kr_;
+        if (Ljs.len > 0) {
+          const int a = Ljs.lo + sj_c, b = Ljs.lo + Ljs.len - 1 + sj_c;
+          if (!REV) { Sj_lo = a; Sj_hi = b; } else { Sj_lo = maxT - b; Sj_hi = maxT - a; }
+        }
+      }
+      Line Lks = {0, 0, 0, 0};
+      int sk_c = 0, Sk_lo = INF_T, Sk_hi = INT_MIN;
+      {
+        const int jl = j0 + lane;
+        if (jl < nj && ks >= 0 && ks < nk) Lks = lines[(size_t)ks * nj + jl];
+        sk_c = jl + kc;
+        if (Lks.len > 0) {
+          const int a = Lks.lo + sk_c, b = Lks.lo + Lks.len - 1 + sk_c;
+          if (!REV) { Sk_lo = a; Sk_hi = b; } else { Sk_lo = maxT - b; Sk_hi = maxT - a; }
+        }
+      }
+      const unsigned want = gen + g.expect_bias;   // bias != 0 only in the expired-wait diagnostic
+      int gate_seen = tileLo - 1;
+      bool failed = false;
+      for (int base = tileLo; base <= tileHi; base += SLB) {
+        // ring space: the slot of step t last held step t-SRING, which the
+        // compute warps have used once the gate reports it finished
+        const int need = base + SLB - 1 - SRING;
+        if (need > gate_seen && !failed) {
+          gate_seen = sh.gate;
+          if (need > gate_seen) {
+            trace_wait(g, 5, base);
+            Spin sp;
+            while ((gate_seen = sh.gate) < need) {
+              if (!sp.step(g.ctl, g.spin_limit)) {
+                raise_timeout(g.ctl, 5, tpos, base, OP, (unsigned long long)(unsigned)gate_seen, (unsigned)need);
+                failed = true;
+                break;
+              }
+            }
+            trace_wait(g, 0, base);
+          }
+        }
+        // Issue the whole batch's loads, then forward every step as soon as
+        // its stamps are current: each poll round re-issues the loads of all
+        // steps still missing (all in flight together) and forwards the ready
+        // prefix.  The source cell of step base+q lies q cells further along
+        // the source line (backward: q cells back).
+        const int ij0 = REV ? (maxT - base) - sj_c : base - sj_c;
+        const int ik0 = REV ? (maxT - base) - sk_c : base - sk_c;
+        const int cj0 = Ljs.off + (ij0 - Ljs.lo), ck0 = Lks.off + (ik0 - Lks.lo);
+        auto needj = [&](int q) {
+          const int tau = base + q;
+          return lane < NW && tau <= tileHi && tau >= Sj_lo && tau <= Sj_hi;
+        };
+        auto needk = [&](int q) {
+          const int tau = base + q;
+          return tau <= tileHi && tau >= Sk_lo && tau <= Sk_hi;
+        };
+        auto oj = [&](int q) { return (size_t)(REV ? cj0 - q : cj0 + q) * P; };
+        auto ok_ = [&](int q) { return (size_t)(REV ? ck0 - q : ck0 + q) * P; };
+        unsigned long long vj[SLB][P], vk[SLB][P];
+#pragma unroll
+        for (int q = 0; q < SLB; ++q) {
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            vj[q][p] = needj(q) ? ld_gpu64(&d.sy[oj(q) + p]) : 0ull;
+            vk[q][p] = needk(q) ? ld_gpu64(&d.sz[ok_(q) + p]) : 0ull;
+          }
+        }
+        const int nsteps = min(SLB, tileHi - base + 1);
+        int fwd = 0;         // steps of this batch this lane has forwarded (a prefix)
+        int published = 0;   // steps of this batch the progress word covers
+        Spin s2;
+        for (;;) {
+#pragma unroll
+          for (int q = 0; q < SLB; ++q) {
+            if (q == fwd && q < nsteps) {
+              bool rdy = true;
+#pragma unroll
+              for (int p = 0; p < P; ++p) {
+                rdy &= !needj(q) || (uint32_t)(vj[q][p] >> 32) == want;
+                rdy &= !needk(q) || (uint32_t)(vk[q][p] >> 32) == want;
+              }
+              if (rdy || failed) {
+                uint32_t wj[P], wk[P];
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                  wj[p] = (uint32_t)vj[q][p];
+                  wk[p] = (uint32_t)vk[q][p];
+                }
+                const int slot = (base + q) & (SRING - 1);
+                if (lane < NW) sh.jr[slot][lane] = needj(q) ? from_words<VT>(wj) : VT(0);
+                sh.kr[slot][lane] = needk(q) ? from_words<VT>(wk) : VT(0);
+                fwd = q + 1;
+              }
+            }
+          }
+          const int all = __reduce_min_sync(XFP_FULL, fwd);
+          if (all > published) {
+            __threadfence_block();
+            __syncwarp();
+            if (lane == 0) sh.lprog = base + all - 1;
+            published = all;
+          }
+          if (all >= nsteps) break;
+          if (!failed && !s2.step(g.ctl, g.spin_limit)) {
+            raise_timeout(g.ctl, 6, tpos, base + all, OP, 0ull, want);
+            failed = true;
+          }
+          failed = __any_sync(XFP_FULL, failed);
+          trace_wait(g, 6, base + all);
+#pragma unroll
+          for (int q = 0; q < SLB; ++q) {
+            if (q >= fwd && !failed) {
+#pragma unroll
+              for (int p = 0; p < P; ++p) {
+                if (needj(q) && (uint32_t)(vj[q][p] >> 32) != want) vj[q][p] = ld_gpu64(&d.sy[oj(q) + p]);
+                if (needk(q) && (uint32_t)(vk[q][p] >> 32) != want) vk[q][p] = ld_gpu64(&d.sz[ok_(q) + p]);
+              }
+            }
+          }
+        }
+        trace_wait(g, 0, base + fwd);
+      }
+    }
+
+    // ---------------- tile epilogue: dot partial (backward) ----------------
+    // One z.r partial per x-line (each lane sums its own line in cell order),
+    // so the reduction below is the same for every tile height.
+    if (OP == SWEEP_BWD && warp < NW) {
+      const int jl = j0 + lane, kl = k0 + warp;
+      if (jl < nj && kl < nk)
+        d.partials[line_base + (size_t)kl * nj + jl] = DOT32 ? (double)dot_acc_f : dot_acc;
+    }
+    __syncthreads();
+  }
+
+  // ---------------- launch epilogue: last CTA closes the generation ----------------
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned t = atomicAdd(&g.ctl->finished, 1u);
+    sh.last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (OP == SWEEP_BWD && g.scal != nullptr && sh.last) {
+    // rho_new = z.r over every line, in line order (line_sum); the loader
+    // ring is idle now and serves as its 256-double scratch
+    __threadfence();
+    const double rho_new = line_sum<DOT32>(d.partials, (long long)g.nj * g.nk, reinterpret_cast<double*>(&sh.kr[0][0]));
+    if (threadIdx.x == 0) {
+      PcgScalars* sc = g.scal;
+      if (g.bwd_mode == 0) {
+        sc->rho = rho_new;
+        if (rho_new == 0.0 || rho_new != rho_new) { sc->status = -5; sc->done = 1; }
+      } else {
+        sc->beta = DOT32 ? (double)__fdiv_rn((float)rho_new, (float)sc->rho) : __ddiv_rn(rho_new, sc->rho);
+        sc->rho = rho_new;
+      }
+    }
+  }
+  if (sh.last && threadIdx.x == 0) {
+    __threadfence();
+    g.ctl->finished = 0;
+    __threadfence();
+    atomicExch(&g.ctl->gen, gen + 1);
+  }
+}
+
+template <int OP, typename VT, typename IT, typename CT, int NW>
+cudaError_t prepare(int* max_grid) {
+  static int cached = -1;
+  static cudaError_t cached_err = cudaSuccess;
+  if (cached < 0) {
+    int dev = 0, nsm = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cached_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, solve_kernel<OP, VT, IT, CT, NW>,
+                                                               (NW + 2) * 32, 0);
+    cached = per * nsm;
+  }
+  *max_grid = cached;
+  return cached_err;
+}
+
+template <int OP, typename VT, typename IT, typename CT, int NW>
+cudaError_t launch_nw(const SweepGrid& g, const SweepData<VT, IT, CT>& d, int grid, cudaStream_t st) {
+  int maxg = 0;
+  cudaError_t e = prepare<OP, VT, IT, CT, NW>(&maxg);
+  if (e != cudaSuccess) return e;
+  if (grid > maxg) grid = maxg;
+  if (grid <= 0) return cudaErrorInvalidConfiguration;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3((NW + 2) * 32);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  ++g_kernel_launches;
+  return cudaLaunchKernelEx(&cfg, solve_kernel<OP, VT, IT, CT, NW>, g, d);
+}
+
+template <int OP, typename VT, typename IT, typename CT>
+cudaError_t launch_op(const SweepGrid& g, const SweepData<VT, IT, CT>& d, int nw, int grid, cudaStream_t st) {
+  switch (nw) {
+    case 8: return launch_nw<OP, VT, IT, CT, 8>(g, d, grid, st);
+    case 15: return launch_nw<OP, VT, IT, CT, 15>(g, d, grid, st);
+    case 16: return launch_nw<OP, VT, IT, CT, 16>(g, d, grid, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int OP, typename VT, typename IT, typename CT>
+int max_grid_op(int nw) {
+  int maxg = 0;
+  switch (nw) {
+    case 8: prepare<OP, VT, IT, CT, 8>(&maxg); break;
+    case 15: prepare<OP, VT, IT, CT, 15>(&maxg); break;
+    case 16: prepare<OP, VT, IT, CT, 16>(&maxg); break;
+    default: break;
+  }
+  return maxg;
+}
+
+}  // namespace
+
+template <typename VT, typename IT, typename CT>
+cudaError_t solve_launch(int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d, int nw, int grid,
+                         cudaStream_t st) {
+  return op == SWEEP_FWD ? launch_op<SWEEP_FWD, VT, IT, CT>(g, d, nw, grid, st)
+                         : launch_op<SWEEP_BWD, VT, IT, CT>(g, d, nw, grid, st);
+}
+template <typename VT, typename IT, typename CT>
+int solve_max_grid(int op, int nw) {
+  return op == SWEEP_FWD ? max_grid_op<SWEEP_FWD, VT, IT, CT>(nw) : max_grid_op<SWEEP_BWD, VT, IT, CT>(nw);
+}
+
+#define XFP_SOLVE_INST(VT, IT, CT)                                                                   \
+  template cudaError_t solve_launch<VT, IT, CT>(int, const SweepGrid&, const SweepData<VT, IT, CT>&, \
+                                                int, int, cudaStream_t);                             \
+  template int solve_max_grid<VT, IT, CT>(int, int);
+XFP_SOLVE_INST(double, double, double)
+XFP_SOLVE_INST(float, float, float)
+XFP_SOLVE_INST(float, double, double)
+
+}  // namespace xfp
