@@ -47,6 +47,8 @@ int check_dims(xfp_ctx* ctx, int ni, int nj, int nk, const void* mat) {
 }
 
 // ---------------------------------------------------------------- layout
+int build_sweep_layout(xfp_ctx* ctx);
+
 int build_layout(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk) {
   const int nw = ctx->nw;
   const long long nlines = (long long)nj * nk;
@@ -68,6 +70,59 @@ int build_layout(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk) {
   ctx->nlines_all = nlines;
   XFP_CUDA(ctx, ctx->cell_line.ensure((std::max<long long>(ctx->M, 4) + 8) * sizeof(int)));
   XFP_CUDA(ctx, build_cell_line(ctx->lines.as<Line>(), nlines, ctx->cell_line.as<int>(), ctx->stream));
+  return build_sweep_layout(ctx);
+}
+
+// Tile table of the sweep layout: per-tile spans on the device, block offsets
+// scanned here (tile order), table uploaded again.
+int build_sweep_layout(xfp_ctx* ctx) {
+  const int nt = (int)ctx->ntiles;
+  XFP_CUDA(ctx, ctx->swt.ensure(std::max(nt, 1) * sizeof(SwTile)));
+  XFP_CUDA(ctx, ctx->tile_pos.ensure((size_t)std::max(ctx->NJt * ctx->NKt, 1) * sizeof(int)));
+  ctx->Msw = 0;
+  if (nt == 0) return XFP_OK;
+  XFP_CUDA(ctx, sw_tiles_build(ctx->lines.as<Line>(), ctx->tiles.as<int>(), nt, ctx->nj, ctx->nk, ctx->nw, ctx->NJt,
+                               ctx->swt.as<SwTile>(), ctx->tile_pos.as<int>(), ctx->stream));
+  std::vector<SwTile> t(nt);
+  XFP_CUDA(ctx, cudaMemcpyAsync(t.data(), ctx->swt.p, nt * sizeof(SwTile), cudaMemcpyDeviceToHost, ctx->stream));
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  long long off = 0;
+  for (auto& e : t) {
+    e.off = off;
+    off += (long long)ctx->nw * e.ng * 128;
+  }
+  ctx->Msw = off;
+  XFP_CUDA(ctx, cudaMemcpyAsync(ctx->swt.p, t.data(), nt * sizeof(SwTile), cudaMemcpyHostToDevice, ctx->stream));
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XFP_OK;
+}
+
+// Sweep-layout copies of the factor (after it is final in the solve type).
+template <typename VT, typename IT, typename CT>
+int sweep_copies(xfp_ctx* ctx, const VT* const L[3], const IT* inv, SweepGrid* gs, int ng,
+                 SweepData<VT, IT, CT>* d) {
+  if (ctx->ntiles == 0) return XFP_OK;
+  const size_t bytes = (size_t)(ctx->Msw + 8) * 8;
+  for (auto& b : ctx->sw_l) XFP_CUDA(ctx, b.ensure(bytes));
+  XFP_CUDA(ctx, ctx->sw_inv.ensure(bytes));
+  XFP_CUDA(ctx, ctx->sw_y.ensure(bytes));
+  cudaStream_t st = ctx->stream;
+  for (int q = 0; q < 3; ++q) {
+    XFP_CUDA(ctx, cudaMemsetAsync(ctx->sw_l[q].p, 0, (size_t)ctx->Msw * sizeof(VT), st));
+    XFP_CUDA(ctx, sw_permute<VT>(const_cast<VT*>(L[q]), ctx->sw_l[q].as<VT>(), ctx->cell_line.as<int>(),
+                                 ctx->lines.as<Line>(), ctx->nj, ctx->nw, ctx->NJt, ctx->tile_pos.as<int>(),
+                                 ctx->swt.as<SwTile>(), ctx->M, 0, st));
+  }
+  XFP_CUDA(ctx, cudaMemsetAsync(ctx->sw_inv.p, 0, (size_t)ctx->Msw * sizeof(IT), st));
+  XFP_CUDA(ctx, sw_permute<IT>(const_cast<IT*>(inv), ctx->sw_inv.as<IT>(), ctx->cell_line.as<int>(),
+                               ctx->lines.as<Line>(), ctx->nj, ctx->nw, ctx->NJt, ctx->tile_pos.as<int>(),
+                               ctx->swt.as<SwTile>(), ctx->M, 0, st));
+  d->lxs = ctx->sw_l[0].as<VT>();
+  d->lys = ctx->sw_l[1].as<VT>();
+  d->lzs = ctx->sw_l[2].as<VT>();
+  d->invs = ctx->sw_inv.as<IT>();
+  d->ys = ctx->sw_y.as<VT>();
+  for (int q = 0; q < ng; ++q) gs[q].swt = ctx->swt.as<SwTile>();
   return XFP_OK;
 }
 
@@ -247,8 +302,11 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   d.partials = ctx->tpartials.as<double>();
   d.sy = ctx->sy.as<unsigned long long>();
   d.sz = ctx->sz.as<unsigned long long>();
-  SweepGrid g0 = make_grid(ctx, dsc, 0), g1 = make_grid(ctx, dsc, 1);
+  SweepGrid gs[2] = {make_grid(ctx, dsc, 0), make_grid(ctx, dsc, 1)};
   int rc;
+  if ((rc = sweep_copies<VT, IT, DT>(ctx, L, inv, gs, 2, &d)) != XFP_OK) return rc;
+  const SweepGrid& g0 = gs[0];
+  const SweepGrid& g1 = gs[1];
   if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g0, d)) != XFP_OK) return rc;
   if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_BWD, g0, d)) != XFP_OK) return rc;
   XFP_CUDA(ctx, copy_vec<VT>(z, s, M, st));
@@ -330,7 +388,9 @@ int tune_tile_height(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, 
     d.partials = ctx->tpartials.as<double>();
     d.sy = ctx->sy.as<unsigned long long>();
     d.sz = ctx->sz.as<unsigned long long>();
-    const SweepGrid g = make_grid(ctx, nullptr, 0);
+    SweepGrid g = make_grid(ctx, nullptr, 0);
+    const float* Lc[3] = {F[0], F[1], F[2]};
+    if ((rc = sweep_copies<float, float, float>(ctx, Lc, ctx->inv32.as<float>(), &g, 1, &d)) != XFP_OK) break;
     const int maxg = sweep_max_grid(SWEEP_FWD, d, cand);
     if (maxg <= 0) continue;
     const int grid = std::min(maxg, (int)ctx->ntiles);
@@ -784,7 +844,12 @@ int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* c
     d.sy = ctx->sy.as<unsigned long long>();
     d.sz = ctx->sz.as<unsigned long long>();
     SweepGrid g = make_grid(ctx, nullptr, 0);
+    if ((rc = sweep_copies<VT, IT, CT>(ctx, L, inv, &g, 1, &d))) return rc;
     if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_FWD, g, d))) return rc;
+    // the forward result is in the sweep layout: back to the line layout
+    if (ctx->ntiles > 0)
+      XFP_CUDA(ctx, sw_permute<VT>(z, ctx->sw_y.as<VT>(), ctx->cell_line.as<int>(), ctx->lines.as<Line>(), ctx->nj,
+                                   ctx->nw, ctx->NJt, ctx->tile_pos.as<int>(), ctx->swt.as<SwTile>(), ctx->M, 1, st));
     XFP_CUDA(ctx, cudaStreamSynchronize(st));
     if ((rc = dump_dense<VT>(ctx, z, out[9]))) return rc;
     if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_BWD, g, d))) return rc;

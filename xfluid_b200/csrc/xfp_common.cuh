@@ -30,6 +30,19 @@ struct __align__(16) Line {
   int off, lo, len, nrows;
 };
 
+// Sweep-ordered copy ("sweep layout") of the arrays the triangular solves
+// stream.  For every active tile, compute warp (k) and group g of 4 forward
+// wavefront steps (steps 4g..4g+3) it holds a block of 32 lanes x 4 cells:
+// element [off + (w*ng + g - g0)*128 + lane*4 + e] is the cell of line
+// (j0+lane, k0+w) at forward step 4g+e, or zero where that line has no cell.
+// A warp's group access is then 512 contiguous bytes (4-byte values) instead
+// of 32 scattered 16-byte pieces.  g0/ng: the tile's first group and group
+// count (its step span, both sweep directions); off: its first element.
+struct __align__(16) SwTile {
+  long long off;
+  int g0, ng;
+};
+
 // Control block of the persistent sweep kernels (one per context).
 struct SweepCtl {
   unsigned int gen;        // launch generation; stamped words carry it in their high half

@@ -34,6 +34,9 @@ struct SweepGrid {
   // words stamped with generation + expect_bias, which no producer writes, so
   // their bounded waits run out.  0 in normal operation.
   unsigned expect_bias = 0;
+  // Sweep layout of the solve arrays (one entry per tile of `tiles`), or null:
+  // the solves then read the factor and write y in the line layout.
+  const SwTile* swt = nullptr;
 };
 
 // Arrays of one sweep.  VT: vector/L type of the solves, IT: invdiag type,
@@ -60,6 +63,14 @@ struct SweepData {
   // 64-bit words (32-bit payload chunk | launch generation << 32).
   unsigned long long* sy = nullptr;  // to the j-neighbour tile
   unsigned long long* sz = nullptr;  // to the k-neighbour tile
+  // Sweep-layout copies (used when SweepGrid::swt is set): the factor, and
+  // y, which the forward solve writes and the backward solve reads (z is
+  // still written to y's line-layout array).
+  const VT* lxs = nullptr;
+  const VT* lys = nullptr;
+  const VT* lzs = nullptr;
+  const IT* invs = nullptr;
+  VT* ys = nullptr;
 };
 
 // Forward/backward solves (xfp_solve.cu); sweep_launch routes them there.
@@ -77,6 +88,16 @@ XFP_SWEEP_DECL(double, double, double)
 XFP_SWEEP_DECL(float, float, float)
 XFP_SWEEP_DECL(float, double, double)
 #undef XFP_SWEEP_DECL
+
+// ---- sweep layout (xfp_swlayout.cu) ----
+// Per-tile step spans of the active tiles (off left 0; the host scans them),
+// and the (K*NJt + J) -> tile position map.
+cudaError_t sw_tiles_build(const Line* lines, const int* tiles, int ntiles, int nj, int nk, int nw, int NJt,
+                           SwTile* swt, int* tile_pos, cudaStream_t st);
+// dir 0: sw[p(c)] = line[c]; dir 1: line[c] = sw[p(c)] for the M stored cells.
+template <typename T>
+cudaError_t sw_permute(T* line, T* sw, const int* cell_line, const Line* lines, int nj, int nw, int NJt,
+                       const int* tile_pos, const SwTile* swt, long long M, int dir, cudaStream_t st);
 
 // ---- layout (xfp_layout.cu) ----
 // Builds the line table and the active-tile list for a material grid.

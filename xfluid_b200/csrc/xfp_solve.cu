@@ -160,6 +160,13 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
 
       VT out_x = VT(0), out_y = VT(0);
 
+      // Sweep layout (when the launch has one): this warp's stream of
+      // 32-lane blocks, one per group of 4 forward steps.
+      const bool swl = g.swt != nullptr;
+      SwTile T = {0, 0, 0};
+      if (swl) T = g.swt[tpos];
+      const long long wbase = T.off + (long long)warp * T.ng * 128 + lane * 4;
+
       // Grouped access.  A line is stored so that cell (i,j,k) sits at an
       // address = i+j+k (mod GS): at every wavefront step all lanes are at the
       // same position within an aligned group of GS cells, so each lane loads
@@ -180,18 +187,33 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
         const int rel = ilow - L.lo;
         return (unsigned)rel < (unsigned)L.len ? L.off + rel : -1;
       };
-      auto load_grp = [&](Grp& G, int c4) {
+      // sweep-layout element of the group of steps t0..t0+GS-1 (clamped into
+      // the tile's blocks for the look-ahead past its last group)
+      auto sw_at = [&](int t0) -> long long {
+        int gi = (REV ? (maxT - t0 - (GS - 1)) : t0) >> 2;
+        gi = min(max(gi, T.g0), T.g0 + T.ng - 1);
+        return wbase + (long long)(gi - T.g0) * 128;
+      };
+      auto load_grp = [&](Grp& G, int c4, long long si) {
         const int cc = c4 >= 0 ? c4 : 0;
         if constexpr (OP == SWEEP_FWD) {
           ldg(G.r, d.r + cc);
         } else {
-          ldg(G.r, d.y + cc);
+          if (swl) ldg(G.r, d.ys + si);
+          else ldg(G.r, d.y + cc);
           ldg(G.rr, d.r + cc);
         }
-        ldg(G.lx, d.lx + cc);
-        ldg(G.ly, d.ly + cc);
-        ldg(G.lz, d.lz + cc);
-        ldg(G.inv, d.inv + cc);
+        if (swl) {
+          ldg(G.lx, d.lxs + si);
+          ldg(G.ly, d.lys + si);
+          ldg(G.lz, d.lzs + si);
+          ldg(G.inv, d.invs + si);
+        } else {
+          ldg(G.lx, d.lx + cc);
+          ldg(G.ly, d.ly + cc);
+          ldg(G.lz, d.lz + cc);
+          ldg(G.inv, d.inv + cc);
+        }
       };
 
       // One wavefront step: everything that needs only this warp's previous
@@ -267,7 +289,7 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
         }
         return res;
       };
-      auto run_group = [&](int t0, const Grp& G, int c4) {
+      auto run_group = [&](int t0, const Grp& G, int c4, long long si) {
         VT yb[GS];
         const bool in = c4 >= 0;
         const int cc = in ? c4 : 0;
@@ -278,20 +300,28 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           yb[e] = VT(0);
           if (tau >= tileLo && tau <= tileHi) yb[e] = step(tau, G, e, in, cc + e);
         }
-        if (in) stg(d.y + c4, yb);
+        // forward with a sweep layout: y goes to its sweep-ordered copy (the
+        // whole block, zeros where a lane has no cell); otherwise, and for
+        // the backward result z, to the line layout
+        if (OP == SWEEP_FWD && swl) stg(d.ys + si, yb);
+        else if (in) stg(d.y + c4, yb);
       };
       Grp GA, GB;
       int cA = group_c4(base0);
-      load_grp(GA, cA);
+      long long sA = sw_at(base0);
+      load_grp(GA, cA, sA);
       for (int gb = base0; gb <= tileHi; gb += 2 * GS) {
         const int cB = group_c4(gb + GS);
-        load_grp(GB, cB);
-        run_group(gb, GA, cA);
+        const long long sB = sw_at(gb + GS);
+        load_grp(GB, cB, sB);
+        run_group(gb, GA, cA, sA);
         if (gb + GS > tileHi) break;
         const int cA2 = group_c4(gb + 2 * GS);
-        load_grp(GA, cA2);
-        run_group(gb + GS, GB, cB);
+        const long long sA2 = sw_at(gb + 2 * GS);
+        load_grp(GA, cA2, sA2);
+        run_group(gb + GS, GB, cB, sB);
         cA = cA2;
+        sA = sA2;
       }
     } else if (tileLo != INF_T && warp == GATE) {
       // ======================= gate warp =======================
