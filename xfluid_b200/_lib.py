@@ -137,6 +137,21 @@ def load() -> C.CDLL:
     return L
 
 
+def torch_stream(device: int) -> C.c_void_p:
+    """Handle of torch's current CUDA stream on `device`.  A context that is
+    given CUDA tensors runs on it, so the library reads them only after the
+    torch work that produced them and torch sees the results in order."""
+    import torch
+    return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def sync_torch(device: int) -> None:
+    """Wait for torch's current stream on `device` (CUDA tensors about to be
+    read on a context stream that is not ordered after it)."""
+    import torch
+    torch.cuda.current_stream(device).synchronize()
+
+
 def default_options() -> XfpOptions:
     o = XfpOptions()
     load().xfp_default_options(C.byref(o))

@@ -54,6 +54,7 @@ class BatchProjector:
         o = _lib.default_options()
         o.precision = _lib.PREC[precision]
         o.tol, o.max_iter, o.tile_k, o.device, o.check_every = tol, max_iter, tile_k, device, check_every
+        self._stream_given = stream is not None
         if stream is not None:
             o.stream = C.c_void_p(stream)
         self._ctx = Context(o)
@@ -86,6 +87,10 @@ class BatchProjector:
         if o.device_pointers != dev:
             o.device_pointers = dev
             self._ctx.set_options(o)
+        if dev and not self._stream_given:
+            # the context's own stream is not ordered after torch's: finish
+            # the torch work that produced the tensors first
+            _lib.sync_torch(o.device)
         st = (XfpStats * n)()
         fn = self._ctx.lib.xfp_project_batch_f64 if dtypes.pop() == "float64" else self._ctx.lib.xfp_project_batch_f32
         rc = self._ctx.check(fn(self._ctx.ptr, n, arr, st))

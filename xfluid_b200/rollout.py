@@ -32,6 +32,9 @@ class Rollout:
         o = _lib.default_options()
         o.precision = _lib.PREC[precision]
         o.tol, o.max_iter, o.device, o.device_pointers = tol, max_iter, device, 1
+        # torch produces and consumes every tensor this class passes: order the
+        # library's kernels on torch's stream
+        o.stream = _lib.torch_stream(device)
         self._ctx = Context(o)
         self.mat = mat
         self.nk, self.nj, self.ni = mat.shape

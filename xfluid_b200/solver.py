@@ -125,6 +125,11 @@ class VariationalPressureSolver:
         if o.device_pointers != want:
             o.device_pointers = want
             self._ctx.set_options(o)
+        if want:
+            # the context's stream is not ordered after torch's: finish the
+            # torch work that produced the tensors (each call returns only
+            # after its own stream is done)
+            _lib.sync_torch(o.device)
 
     def solve(self, pressure) -> bool:
         """Fills pressure (nk,nj,ni) for every cell; True when converged."""
