@@ -92,37 +92,53 @@ int build_sweep_layout(xfp_ctx* ctx) {
     off += (long long)ctx->nw * e.ng * 128;
   }
   ctx->Msw = off;
+  if (off >= (1LL << 31)) return fail(ctx, XFP_ERR_ARGS, "grid too large for the sweep layout");
   XFP_CUDA(ctx, cudaMemcpyAsync(ctx->swt.p, t.data(), nt * sizeof(SwTile), cudaMemcpyHostToDevice, ctx->stream));
+  XFP_CUDA(ctx, ctx->sw_perm.ensure((size_t)(std::max<long long>(ctx->M, 4) + 8) * sizeof(int)));
+  XFP_CUDA(ctx, sw_perm_build(ctx->cell_line.as<int>(), ctx->lines.as<Line>(), ctx->nj, ctx->nw, ctx->NJt,
+                              ctx->tile_pos.as<int>(), ctx->swt.as<SwTile>(), ctx->M, ctx->sw_perm.as<int>(),
+                              ctx->stream));
   XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return XFP_OK;
 }
 
-// Sweep-layout copies of the factor (after it is final in the solve type).
+// Sweep-layout copies of the factor (after it is final in the solve type)
+// and of r; element slots of lanes without a cell stay zero.
 template <typename VT, typename IT, typename CT>
-int sweep_copies(xfp_ctx* ctx, const VT* const L[3], const IT* inv, SweepGrid* gs, int ng,
+int sweep_copies(xfp_ctx* ctx, const VT* const L[3], const IT* inv, const VT* r, SweepGrid* gs, int ng,
                  SweepData<VT, IT, CT>* d) {
   if (ctx->ntiles == 0) return XFP_OK;
   const size_t bytes = (size_t)(ctx->Msw + 8) * 8;
   for (auto& b : ctx->sw_l) XFP_CUDA(ctx, b.ensure(bytes));
   XFP_CUDA(ctx, ctx->sw_inv.ensure(bytes));
+  XFP_CUDA(ctx, ctx->sw_r.ensure(bytes));
   XFP_CUDA(ctx, ctx->sw_y.ensure(bytes));
   cudaStream_t st = ctx->stream;
+  const int* perm = ctx->sw_perm.as<int>();
   for (int q = 0; q < 3; ++q) {
     XFP_CUDA(ctx, cudaMemsetAsync(ctx->sw_l[q].p, 0, (size_t)ctx->Msw * sizeof(VT), st));
-    XFP_CUDA(ctx, sw_permute<VT>(const_cast<VT*>(L[q]), ctx->sw_l[q].as<VT>(), ctx->cell_line.as<int>(),
-                                 ctx->lines.as<Line>(), ctx->nj, ctx->nw, ctx->NJt, ctx->tile_pos.as<int>(),
-                                 ctx->swt.as<SwTile>(), ctx->M, 0, st));
+    XFP_CUDA(ctx, sw_permute<VT>(const_cast<VT*>(L[q]), ctx->sw_l[q].as<VT>(), perm, ctx->M, 0, st));
   }
   XFP_CUDA(ctx, cudaMemsetAsync(ctx->sw_inv.p, 0, (size_t)ctx->Msw * sizeof(IT), st));
-  XFP_CUDA(ctx, sw_permute<IT>(const_cast<IT*>(inv), ctx->sw_inv.as<IT>(), ctx->cell_line.as<int>(),
-                               ctx->lines.as<Line>(), ctx->nj, ctx->nw, ctx->NJt, ctx->tile_pos.as<int>(),
-                               ctx->swt.as<SwTile>(), ctx->M, 0, st));
+  XFP_CUDA(ctx, sw_permute<IT>(const_cast<IT*>(inv), ctx->sw_inv.as<IT>(), perm, ctx->M, 0, st));
+  XFP_CUDA(ctx, cudaMemsetAsync(ctx->sw_r.p, 0, (size_t)ctx->Msw * sizeof(VT), st));
+  XFP_CUDA(ctx, sw_permute<VT>(const_cast<VT*>(r), ctx->sw_r.as<VT>(), perm, ctx->M, 0, st));
   d->lxs = ctx->sw_l[0].as<VT>();
   d->lys = ctx->sw_l[1].as<VT>();
   d->lzs = ctx->sw_l[2].as<VT>();
   d->invs = ctx->sw_inv.as<IT>();
+  d->rs = ctx->sw_r.as<VT>();
   d->ys = ctx->sw_y.as<VT>();
   for (int q = 0; q < ng; ++q) gs[q].swt = ctx->swt.as<SwTile>();
+  return XFP_OK;
+}
+
+// Line-layout copy of the sweep-ordered solve result (z, or y after a
+// forward solve alone).
+template <typename VT>
+int sweep_result(xfp_ctx* ctx, VT* out) {
+  if (ctx->ntiles == 0) return XFP_OK;
+  XFP_CUDA(ctx, sw_permute<VT>(out, ctx->sw_y.as<VT>(), ctx->sw_perm.as<int>(), ctx->M, 1, ctx->stream));
   return XFP_OK;
 }
 
@@ -304,12 +320,22 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   d.sz = ctx->sz.as<unsigned long long>();
   SweepGrid gs[2] = {make_grid(ctx, dsc, 0), make_grid(ctx, dsc, 1)};
   int rc;
-  if ((rc = sweep_copies<VT, IT, DT>(ctx, L, inv, gs, 2, &d)) != XFP_OK) return rc;
+  if ((rc = sweep_copies<VT, IT, DT>(ctx, L, inv, r, gs, 2, &d)) != XFP_OK) return rc;
   const SweepGrid& g0 = gs[0];
   const SweepGrid& g1 = gs[1];
+  // with a sweep layout, r is kept in both layouts (update_xr writes both)
+  // and z lives in the sweep layout only (update_s reads it through perm)
+  const bool swl = ctx->ntiles > 0;
+  VT* rsw = swl ? ctx->sw_r.as<VT>() : nullptr;
+  const VT* zsw = swl ? ctx->sw_y.as<VT>() : nullptr;
+  const int* perm = swl ? ctx->sw_perm.as<int>() : nullptr;
   if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g0, d)) != XFP_OK) return rc;
   if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_BWD, g0, d)) != XFP_OK) return rc;
-  XFP_CUDA(ctx, copy_vec<VT>(z, s, M, st));
+  if (swl) {
+    if ((rc = sweep_result<VT>(ctx, s)) != XFP_OK) return rc;
+  } else {
+    XFP_CUDA(ctx, copy_vec<VT>(z, s, M, st));
+  }
   const int K = ctx->opt.check_every > 0 ? ctx->opt.check_every : 8;
   DT* part = reinterpret_cast<DT*>(ctx->partials.p);
   for (int done_iters = 0;;) {
@@ -317,10 +343,10 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
       XFP_CUDA(ctx, (spmv_dot<VT, VT, DT>(A[0], A[1], A[2], A[3], s, z, ctx->lines.as<Line>(),
                                           ctx->cell_line.as<int>(), ctx->nj, ctx->nk, M, dsc, part, NBLK_MAX, 0,
                                           st)));
-      XFP_CUDA(ctx, (update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), NBLK_MAX, st)));
+      XFP_CUDA(ctx, (update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), NBLK_MAX, st, rsw, perm)));
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g1, d)) != XFP_OK) return rc;
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_BWD, g1, d)) != XFP_OK) return rc;
-      XFP_CUDA(ctx, update_s<VT>(s, z, M, dsc, st));
+      XFP_CUDA(ctx, update_s<VT>(s, z, M, dsc, st, zsw, perm));
     }
     done_iters += K;
     XFP_CUDA(ctx, cudaMemcpyAsync(hsc, dsc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
@@ -390,7 +416,7 @@ int tune_tile_height(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, 
     d.sz = ctx->sz.as<unsigned long long>();
     SweepGrid g = make_grid(ctx, nullptr, 0);
     const float* Lc[3] = {F[0], F[1], F[2]};
-    if ((rc = sweep_copies<float, float, float>(ctx, Lc, ctx->inv32.as<float>(), &g, 1, &d)) != XFP_OK) break;
+    if ((rc = sweep_copies<float, float, float>(ctx, Lc, ctx->inv32.as<float>(), A[4], &g, 1, &d)) != XFP_OK) break;
     const int maxg = sweep_max_grid(SWEEP_FWD, d, cand);
     if (maxg <= 0) continue;
     const int grid = std::min(maxg, (int)ctx->ntiles);
@@ -844,15 +870,14 @@ int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* c
     d.sy = ctx->sy.as<unsigned long long>();
     d.sz = ctx->sz.as<unsigned long long>();
     SweepGrid g = make_grid(ctx, nullptr, 0);
-    if ((rc = sweep_copies<VT, IT, CT>(ctx, L, inv, &g, 1, &d))) return rc;
+    if ((rc = sweep_copies<VT, IT, CT>(ctx, L, inv, r, &g, 1, &d))) return rc;
     if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_FWD, g, d))) return rc;
-    // the forward result is in the sweep layout: back to the line layout
-    if (ctx->ntiles > 0)
-      XFP_CUDA(ctx, sw_permute<VT>(z, ctx->sw_y.as<VT>(), ctx->cell_line.as<int>(), ctx->lines.as<Line>(), ctx->nj,
-                                   ctx->nw, ctx->NJt, ctx->tile_pos.as<int>(), ctx->swt.as<SwTile>(), ctx->M, 1, st));
+    // the solve results are in the sweep layout: back to the line layout
+    if ((rc = sweep_result<VT>(ctx, z))) return rc;
     XFP_CUDA(ctx, cudaStreamSynchronize(st));
     if ((rc = dump_dense<VT>(ctx, z, out[9]))) return rc;
     if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_BWD, g, d))) return rc;
+    if ((rc = sweep_result<VT>(ctx, z))) return rc;
     XFP_CUDA(ctx, (spmv_dot<VT, VT, VT>(Av[0], Av[1], Av[2], Av[3], r, qv, ctx->lines.as<Line>(),
                                         ctx->cell_line.as<int>(), ctx->nj, ctx->nk, M, nullptr, (VT*)nullptr,
                                         NBLK_MAX, 1, st)));

@@ -64,9 +64,10 @@ struct xfp_ctx {
   DevBuf x64, r64, x32, r32, s32, z32, s64, z64, dense;
   // control
   DevBuf ctl, scal, scal2, partials, tpartials, sy, sz, trace;
-  // sweep layout (SwTile): tile table, (K,J) -> tile map and the copies the
-  // solves stream (lx, ly, lz, inv, y; 8 bytes per element covers every precision)
-  DevBuf swt, tile_pos, sw_l[3], sw_inv, sw_y;
+  // sweep layout (SwTile): tile table, (K,J) -> tile map, cell -> element map
+  // and the copies the solves stream (lx, ly, lz, inv, r, y; 8 bytes per
+  // element covers every precision)
+  DevBuf swt, tile_pos, sw_perm, sw_l[3], sw_inv, sw_r, sw_y;
   long long Msw = 0;
   bool tracing = false;
   // sizes of the current layout

@@ -63,13 +63,14 @@ struct SweepData {
   // 64-bit words (32-bit payload chunk | launch generation << 32).
   unsigned long long* sy = nullptr;  // to the j-neighbour tile
   unsigned long long* sz = nullptr;  // to the k-neighbour tile
-  // Sweep-layout copies (used when SweepGrid::swt is set): the factor, and
-  // y, which the forward solve writes and the backward solve reads (z is
-  // still written to y's line-layout array).
+  // Sweep-layout copies (used when SweepGrid::swt is set): the factor, r,
+  // and y, which the forward solve writes and the backward solve overwrites
+  // with z (the line-layout r and y are then not touched).
   const VT* lxs = nullptr;
   const VT* lys = nullptr;
   const VT* lzs = nullptr;
   const IT* invs = nullptr;
+  const VT* rs = nullptr;
   VT* ys = nullptr;
 };
 
@@ -94,10 +95,12 @@ XFP_SWEEP_DECL(float, double, double)
 // and the (K*NJt + J) -> tile position map.
 cudaError_t sw_tiles_build(const Line* lines, const int* tiles, int ntiles, int nj, int nk, int nw, int NJt,
                            SwTile* swt, int* tile_pos, cudaStream_t st);
-// dir 0: sw[p(c)] = line[c]; dir 1: line[c] = sw[p(c)] for the M stored cells.
+// perm[c] = sweep-layout element of stored cell c (c < M).
+cudaError_t sw_perm_build(const int* cell_line, const Line* lines, int nj, int nw, int NJt, const int* tile_pos,
+                          const SwTile* swt, long long M, int* perm, cudaStream_t st);
+// dir 0: sw[perm[c]] = line[c]; dir 1: line[c] = sw[perm[c]] for the M stored cells.
 template <typename T>
-cudaError_t sw_permute(T* line, T* sw, const int* cell_line, const Line* lines, int nj, int nw, int NJt,
-                       const int* tile_pos, const SwTile* swt, long long M, int dir, cudaStream_t st);
+cudaError_t sw_permute(T* line, T* sw, const int* perm, long long M, int dir, cudaStream_t st);
 
 // ---- layout (xfp_layout.cu) ----
 // Builds the line table and the active-tile list for a material grid.
@@ -143,11 +146,15 @@ cudaError_t spmv_dot(const AT* diag, const AT* ax, const AT* ay, const AT* az, c
                      DT* partials, int nblk_max, int mode, cudaStream_t st);
 // cell_line[c] = index of the line storing cell c (for every cell of every line).
 cudaError_t build_cell_line(const Line* lines, long long nlines, int* cell_line, cudaStream_t st);
+// rsw/perm (optional): the updated r is also stored at rsw[perm[c]].
 template <typename VT, typename DT>
 cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgScalars* sc,
-                      double* partials, int nblk_max, cudaStream_t st);
+                      double* partials, int nblk_max, cudaStream_t st, VT* rsw = nullptr,
+                      const int* perm = nullptr);
+// zsw/perm (optional): z is read from zsw[perm[c]] instead of z[c].
 template <typename VT>
-cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st);
+cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st, const VT* zsw = nullptr,
+                     const int* perm = nullptr);
 template <typename VT>
 cudaError_t absmax_init(const VT* b, long long M, PcgScalars* sc, double* partials, int nblk_max,
                         double tol, int maxit, cudaStream_t st);

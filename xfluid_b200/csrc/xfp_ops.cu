@@ -633,7 +633,8 @@ template <typename VT>
 __device__ __forceinline__ void update_xr_body(unsigned bid, unsigned nblk, VT* __restrict__ x,
                                                VT* __restrict__ r, const VT* __restrict__ s,
                                                const VT* __restrict__ z, long long M, PcgScalars* sc,
-                                               double* __restrict__ partials) {
+                                               double* __restrict__ partials, VT* __restrict__ rsw = nullptr,
+                                               const int* __restrict__ perm = nullptr) {
   __shared__ double sh[32];
   if (*(volatile int*)&sc->done) return;
   const VT alpha = (VT)sc->alpha;
@@ -643,6 +644,7 @@ __device__ __forceinline__ void update_xr_body(unsigned bid, unsigned nblk, VT* 
     x[c] = add_rn(x[c], mul_rn(alpha, s[c]));
     const VT rv = add_rn(r[c], mul_rn(nalpha, z[c]));
     r[c] = rv;
+    if (rsw != nullptr) rsw[perm[c]] = rv;
     m = fmax(m, (double)fabs(rv));
   }
   double t = block_max(m, sh);
@@ -666,8 +668,9 @@ template <typename VT>
 __global__ void __launch_bounds__(256) update_xr_kernel(VT* __restrict__ x, VT* __restrict__ r,
                                                         const VT* __restrict__ s,
                                                         const VT* __restrict__ z, long long M,
-                                                        PcgScalars* sc, double* __restrict__ partials) {
-  update_xr_body<VT>(blockIdx.x, gridDim.x, x, r, s, z, M, sc, partials);
+                                                        PcgScalars* sc, double* __restrict__ partials,
+                                                        VT* __restrict__ rsw, const int* __restrict__ perm) {
+  update_xr_body<VT>(blockIdx.x, gridDim.x, x, r, s, z, M, sc, partials, rsw, perm);
 }
 template <typename VT>
 __global__ void __launch_bounds__(256) batch_update_xr_kernel(const BatchSeg* __restrict__ segs, int nseg,
@@ -681,33 +684,35 @@ __global__ void __launch_bounds__(256) batch_update_xr_kernel(const BatchSeg* __
 }
 template <typename VT, typename DT>
 cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgScalars* sc,
-                      double* partials, int nblk_max, cudaStream_t st) {
+                      double* partials, int nblk_max, cudaStream_t st, VT* rsw, const int* perm) {
   int blocks = (int)std::min<long long>((M + 255) / 256, (long long)nblk_max);
   if (blocks < 1) blocks = 1;
   ++g_kernel_launches;
-  update_xr_kernel<VT><<<blocks, 256, 0, st>>>(x, r, s, z, M, sc, partials);
+  update_xr_kernel<VT><<<blocks, 256, 0, st>>>(x, r, s, z, M, sc, partials, rsw, perm);
   return cudaGetLastError();
 }
 template cudaError_t update_xr<double, double>(double*, double*, const double*, const double*, long long,
-                                               PcgScalars*, double*, int, cudaStream_t);
+                                               PcgScalars*, double*, int, cudaStream_t, double*, const int*);
 template cudaError_t update_xr<float, float>(float*, float*, const float*, const float*, long long,
-                                             PcgScalars*, double*, int, cudaStream_t);
+                                             PcgScalars*, double*, int, cudaStream_t, float*, const int*);
 template cudaError_t update_xr<float, double>(float*, float*, const float*, const float*, long long,
-                                              PcgScalars*, double*, int, cudaStream_t);
+                                              PcgScalars*, double*, int, cudaStream_t, float*, const int*);
 
 // s = z + beta s  (add_scaled(beta, s, z) then swap, pcg_solver.h:280)
 template <typename VT>
 __device__ __forceinline__ void update_s_body(unsigned bid, unsigned nblk, VT* __restrict__ s,
-                                              const VT* __restrict__ z, long long M, PcgScalars* sc) {
+                                              const VT* __restrict__ z, long long M, PcgScalars* sc,
+                                              const VT* __restrict__ zsw = nullptr,
+                                              const int* __restrict__ perm = nullptr) {
   if (*(volatile int*)&sc->done) return;
   const VT beta = (VT)sc->beta;
   for (long long c = (long long)bid * blockDim.x + threadIdx.x; c < M; c += (long long)nblk * blockDim.x)
-    s[c] = add_rn(z[c], mul_rn(beta, s[c]));
+    s[c] = add_rn(zsw != nullptr ? zsw[perm[c]] : z[c], mul_rn(beta, s[c]));
 }
 template <typename VT>
 __global__ void update_s_kernel(VT* __restrict__ s, const VT* __restrict__ z, long long M,
-                                PcgScalars* sc) {
-  update_s_body<VT>(blockIdx.x, gridDim.x, s, z, M, sc);
+                                PcgScalars* sc, const VT* __restrict__ zsw, const int* __restrict__ perm) {
+  update_s_body<VT>(blockIdx.x, gridDim.x, s, z, M, sc, zsw, perm);
 }
 template <typename VT>
 __global__ void batch_update_s_kernel(const BatchSeg* __restrict__ segs, int nseg, VT* __restrict__ s,
@@ -717,15 +722,18 @@ __global__ void batch_update_s_kernel(const BatchSeg* __restrict__ segs, int nse
   update_s_body<VT>(blockIdx.x - S.blk_cells_start, S.blk_cells, s + S.base, z + S.base, S.M, sc + q);
 }
 template <typename VT>
-cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st) {
+cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st, const VT* zsw,
+                     const int* perm) {
   int blocks = (int)std::min<long long>((M + 255) / 256, 148LL * 16);
   if (blocks < 1) blocks = 1;
   ++g_kernel_launches;
-  update_s_kernel<VT><<<blocks, 256, 0, st>>>(s, z, M, sc);
+  update_s_kernel<VT><<<blocks, 256, 0, st>>>(s, z, M, sc, zsw, perm);
   return cudaGetLastError();
 }
-template cudaError_t update_s<double>(double*, const double*, long long, PcgScalars*, cudaStream_t);
-template cudaError_t update_s<float>(float*, const float*, long long, PcgScalars*, cudaStream_t);
+template cudaError_t update_s<double>(double*, const double*, long long, PcgScalars*, cudaStream_t, const double*,
+                                      const int*);
+template cudaError_t update_s<float>(float*, const float*, long long, PcgScalars*, cudaStream_t, const float*,
+                                     const int*);
 
 // |b|_inf, tolerance and loop state at the start of a solve (pcg_solver.h:247-254).
 template <typename VT>

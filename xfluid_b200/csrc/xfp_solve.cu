@@ -51,6 +51,28 @@ constexpr int SRING = 32;   // loader ring depth (steps)
 constexpr int SLB = 8;      // loader batch: steps polled together
 static_assert(SRING >= SLB + 1, "the loader could wait for a slot the gate cannot free");
 
+// y = t * inv rounded to the solve type.  FP64 and FP32 solves multiply in
+// their own type.  The mixed solve (FP32 values, FP64 inverse pivot) splits the
+// pivot into FP32 parts hi + lo (exact to about 48 bits, split before the
+// step's barrier, off the dependency chain) and forms fma(t, hi, t*lo): within
+// about half an FP32 ulp of the FP64 product, at a fraction of the latency of
+// converting t to FP64, multiplying and converting back.
+template <typename VT, typename IT>
+struct Pivot {
+  IT v;
+  __device__ __forceinline__ explicit Pivot(IT inv) : v(inv) {}
+  __device__ __forceinline__ VT mul(VT t) const { return VT(mul_rn((IT)t, v)); }
+};
+template <>
+struct Pivot<float, double> {
+  float hi, lo;
+  __device__ __forceinline__ explicit Pivot(double inv) {
+    hi = __double2float_rn(inv);
+    lo = __double2float_rn(__dsub_rn(inv, (double)hi));
+  }
+  __device__ __forceinline__ float mul(float t) const { return __fmaf_rn(t, hi, __fmul_rn(t, lo)); }
+};
+
 __device__ __forceinline__ void step_barrier(int nthreads) {
   asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
@@ -197,10 +219,13 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
       auto load_grp = [&](Grp& G, int c4, long long si) {
         const int cc = c4 >= 0 ? c4 : 0;
         if constexpr (OP == SWEEP_FWD) {
-          ldg(G.r, d.r + cc);
+          if (swl) ldg(G.r, d.rs + si);
+          else ldg(G.r, d.r + cc);
+        } else if (swl) {
+          ldg(G.r, d.ys + si);
+          ldg(G.rr, d.rs + si);
         } else {
-          if (swl) ldg(G.r, d.ys + si);
-          else ldg(G.r, d.y + cc);
+          ldg(G.r, d.y + cc);
           ldg(G.rr, d.r + cc);
         }
         if (swl) {
@@ -228,6 +253,7 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           // order, then result[c] *= invdiag[c]  (pcg_solver.h:198-203)
           const VT px = mul_rn(G.lx[e], out_x);
           const VT py_sh = mul_rn(G.ly[e], vy_sh);
+          const Pivot<VT, IT> piv(G.inv[e]);
           step_barrier(NT);
           const VT vz = kb ? sh.kr[slot][lane] : sh.zr[(tau - 1) & 1][zsrc][lane];
           const VT vj = sh.jr[slot][warp];
@@ -235,7 +261,7 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           VT t = sub_rn(G.r[e], mul_rn(G.lz[e], vz));
           t = sub_rn(t, py);
           t = sub_rn(t, px);
-          const VT y = in ? VT(mul_rn((IT)t, G.inv[e])) : VT(0);
+          const VT y = in ? piv.mul(t) : VT(0);
           if (zdst_in) sh.zr[tau & 1][warp][lane] = y;
           out_x = y;
           out_y = y;
@@ -258,12 +284,13 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           // The products L(m,c) x[m] arrive ready-made from the producers.
           const VT t1 = sub_rn(G.r[e], out_x);
           const VT t2_sh = sub_rn(t1, vy_sh);
+          const Pivot<VT, IT> piv(G.inv[e]);
           step_barrier(NT);
           const VT vz = kb ? sh.kr[slot][lane] : sh.zr[(tau - 1) & 1][zsrc][lane];
           const VT vj = sh.jr[slot][warp];
           const VT t2 = jb ? sub_rn(t1, vj) : t2_sh;
           const VT t = sub_rn(t2, vz);
-          const VT z = in ? VT(mul_rn((IT)t, G.inv[e])) : VT(0);
+          const VT z = in ? piv.mul(t) : VT(0);
           const VT oz = mul_rn(in ? G.lz[e] : VT(0), z);
           if (zdst_in) sh.zr[tau & 1][warp][lane] = oz;
           const VT rr = in ? G.rr[e] : VT(0);
@@ -300,12 +327,39 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           yb[e] = VT(0);
           if (tau >= tileLo && tau <= tileHi) yb[e] = step(tau, G, e, in, cc + e);
         }
-        // forward with a sweep layout: y goes to its sweep-ordered copy (the
-        // whole block, zeros where a lane has no cell); otherwise, and for
-        // the backward result z, to the line layout
-        if (OP == SWEEP_FWD && swl) stg(d.ys + si, yb);
+        // with a sweep layout y (forward) and z (backward, in place) go to
+        // the sweep-ordered copy, the whole block (zeros where a lane has no
+        // cell); otherwise to the line layout
+        if (swl) stg(d.ys + si, yb);
         else if (in) stg(d.y + c4, yb);
       };
+      // Groups are loaded into registers one group ahead (two buffers), or two
+      // groups ahead (three buffers) where the register budget allows: the
+      // height-8 tile has 10 warps, i.e. about 170 registers per thread (FP32
+      // values; FP64 groups are twice the size and stay double-buffered).
+      if constexpr (NW <= 8 && sizeof(VT) == 4) {
+        Grp GA, GB, GC;
+        int cA = group_c4(base0), cB = group_c4(base0 + GS);
+        long long sA = sw_at(base0), sB = sw_at(base0 + GS);
+        load_grp(GA, cA, sA);
+        load_grp(GB, cB, sB);
+        for (int gb = base0; gb <= tileHi; gb += 3 * GS) {
+          const int cC = group_c4(gb + 2 * GS);
+          const long long sC = sw_at(gb + 2 * GS);
+          load_grp(GC, cC, sC);
+          run_group(gb, GA, cA, sA);
+          if (gb + GS > tileHi) break;
+          cA = group_c4(gb + 3 * GS);
+          sA = sw_at(gb + 3 * GS);
+          load_grp(GA, cA, sA);
+          run_group(gb + GS, GB, cB, sB);
+          if (gb + 2 * GS > tileHi) break;
+          cB = group_c4(gb + 4 * GS);
+          sB = sw_at(gb + 4 * GS);
+          load_grp(GB, cB, sB);
+          run_group(gb + 2 * GS, GC, cC, sC);
+        }
+      } else {
       Grp GA, GB;
       int cA = group_c4(base0);
       long long sA = sw_at(base0);
@@ -322,6 +376,7 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
         run_group(gb + GS, GB, cB, sB);
         cA = cA2;
         sA = sA2;
+      }
       }
     } else if (tileLo != INF_T && warp == GATE) {
       // ======================= gate warp =======================

@@ -43,21 +43,26 @@ __global__ void sw_tiles_kernel(const Line* __restrict__ lines, const int* __res
   }
 }
 
-template <typename T>
-__global__ void sw_permute_kernel(T* __restrict__ line, T* __restrict__ sw, const int* __restrict__ cell_line,
-                                  const Line* __restrict__ lines, int nj, int nw, int NJt,
-                                  const int* __restrict__ tile_pos, const SwTile* __restrict__ swt, long long M,
-                                  int dir) {
+// perm[c] = sweep-layout element of stored cell c
+__global__ void sw_perm_kernel(const int* __restrict__ cell_line, const Line* __restrict__ lines, int nj, int nw,
+                               int NJt, const int* __restrict__ tile_pos, const SwTile* __restrict__ swt, long long M,
+                               int* __restrict__ perm) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x) {
     const int l = cell_line[c];
     const int j = l % nj, k = l / nj;
     const Line L = lines[l];
     const int tau = L.lo + (int)(c - L.off) + j + k;
-    const int tp = tile_pos[(k / nw) * NJt + (j >> 5)];
-    const SwTile S = swt[tp];
-    const long long p = S.off + ((long long)(k % nw) * S.ng + ((tau >> 2) - S.g0)) * 128 + (j & 31) * 4 + (tau & 3);
-    if (dir == 0) sw[p] = line[c];
-    else line[c] = sw[p];
+    const SwTile S = swt[tile_pos[(k / nw) * NJt + (j >> 5)]];
+    perm[c] = (int)(S.off + ((long long)(k % nw) * S.ng + ((tau >> 2) - S.g0)) * 128 + (j & 31) * 4 + (tau & 3));
+  }
+}
+
+template <typename T>
+__global__ void sw_permute_kernel(T* __restrict__ line, T* __restrict__ sw, const int* __restrict__ perm, long long M,
+                                  int dir) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x) {
+    if (dir == 0) sw[perm[c]] = line[c];
+    else line[c] = sw[perm[c]];
   }
 }
 
@@ -71,19 +76,24 @@ cudaError_t sw_tiles_build(const Line* lines, const int* tiles, int ntiles, int 
   return cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t sw_permute(T* line, T* sw, const int* cell_line, const Line* lines, int nj, int nw, int NJt,
-                       const int* tile_pos, const SwTile* swt, long long M, int dir, cudaStream_t st) {
+cudaError_t sw_perm_build(const int* cell_line, const Line* lines, int nj, int nw, int NJt, const int* tile_pos,
+                          const SwTile* swt, long long M, int* perm, cudaStream_t st) {
   if (M <= 0) return cudaSuccess;
   ++g_kernel_launches;
   const long long blocks = std::min<long long>((M + 255) / 256, 148LL * 16);
-  sw_permute_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(line, sw, cell_line, lines, nj, nw, NJt, tile_pos, swt, M,
-                                                          dir);
+  sw_perm_kernel<<<(unsigned)blocks, 256, 0, st>>>(cell_line, lines, nj, nw, NJt, tile_pos, swt, M, perm);
   return cudaGetLastError();
 }
-template cudaError_t sw_permute<float>(float*, float*, const int*, const Line*, int, int, int, const int*,
-                                       const SwTile*, long long, int, cudaStream_t);
-template cudaError_t sw_permute<double>(double*, double*, const int*, const Line*, int, int, int, const int*,
-                                        const SwTile*, long long, int, cudaStream_t);
+
+template <typename T>
+cudaError_t sw_permute(T* line, T* sw, const int* perm, long long M, int dir, cudaStream_t st) {
+  if (M <= 0) return cudaSuccess;
+  ++g_kernel_launches;
+  const long long blocks = std::min<long long>((M + 255) / 256, 148LL * 16);
+  sw_permute_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(line, sw, perm, M, dir);
+  return cudaGetLastError();
+}
+template cudaError_t sw_permute<float>(float*, float*, const int*, long long, int, cudaStream_t);
+template cudaError_t sw_permute<double>(double*, double*, const int*, long long, int, cudaStream_t);
 
 }  // namespace xfp
