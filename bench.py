@@ -287,7 +287,7 @@ def ours(args, rank, world):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = bytes_per_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else None
     tr = sweep_traffic_per_row()
-    roofline = {"bound": "hbm", "kernel": "MIC(0) triangular-solve sweeps (sweep_kernel fwd/bwd)",
+    roofline = {"bound": "hbm", "kernel": "MIC(0) triangular solves (solve_kernel fwd/bwd, lockstep wavefronts)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
                 "frac": (achieved / peak) if achieved else None,
