@@ -217,9 +217,10 @@ def ours(args, rank, world):
     sc = scenes.blob_scene(args.n, seed=SEED, dtype=np.float32)
     ni, nj, nk = sc.ni, sc.nj, sc.nk
 
-    def ctx_for(prec, device_pointers):
+    def ctx_for(prec, device_pointers, matrix="variational"):
         o = _lib.default_options()
         o.precision = _lib.PREC[prec]
+        o.matrix = _lib.MATRIX[matrix]
         o.tol, o.max_iter = TOL, MAXIT
         o.device = dev
         o.device_pointers = device_pointers
@@ -235,10 +236,10 @@ def ours(args, rank, world):
     pres = torch.zeros((nk, nj, ni), dtype=torch.float32, device="cuda")
     P = lambda x: C.c_void_p(x.data_ptr())
 
-    def project_dev(ctx, vel, p):
+    def project_dev(ctx, vel, p, weights=True):
         st = _lib.XfpStats()
         rc = ctx.lib.xfp_project_f32(ctx.ptr, ni, nj, nk, P(mat), P(vel[0]), P(vel[1]), P(vel[2]),
-                                     *map(P, wts), P(p), C.byref(st))
+                                     *(map(P, wts) if weights else (None, None, None)), P(p), C.byref(st))
         ctx.check(rc)
         return rc, st.as_dict()
 
@@ -358,6 +359,24 @@ def ours(args, rank, world):
                                   "iterations": int(st2["iterations"]), "rel_residual": st2["rel_residual"],
                                   "pressure_rel_l2_vs_fp64": rel(p2), "status": rc2}
         c2.close()
+    # xFluid's NormalPressureSolver matrix (classic Poisson, no face weights)
+    # on the same scene and tolerance, mixed precision
+    cn = ctx_for("mixed", 1, "normal")
+    pn = torch.zeros_like(pres)
+    project_dev(cn, [a.clone() for a in vel0], pn, weights=False)
+    torch.cuda.synchronize()
+    reps = 2
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    vs = [[a.clone() for a in vel0] for _ in range(reps)]
+    e0.record(stream)
+    for r_ in range(reps):
+        rcn, stn = project_dev(cn, vs[r_], pn, weights=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    forms["normal_matrix_mixed"] = {"value": reps / (e0.elapsed_time(e1) / 1000.0), "unit": UNIT,
+                                    "iterations": int(stn["iterations"]), "rel_residual": stn["rel_residual"],
+                                    "status": rcn, "matrix": "NormalPressureSolver (pressuresolver.cpp)"}
+    cn.close()
     forms["mixed_over_plain_f32"] = value / world / forms["plain_f32"]["value"]
     forms["mixed_over_plain_f64"] = value / world / forms["plain_f64"]["value"]
 

@@ -51,6 +51,14 @@ extern "C" {
 #define XFP_PREC_MIXED 2 /* FP32 stencil/vectors; FP64 dots, MIC(0) pivots and
                             iterative-refinement residual */
 
+/* Pressure matrix (xfp_options.matrix).
+ * VARIATIONAL: VariationalPressureSolver's (variational_pressuresolver.cpp:231-327), with optional face weights.
+ * NORMAL: NormalPressureSolver's classic Poisson matrix (pressuresolver.cpp:220-347) -- diagonal = in-range
+ *   non-solid neighbours, -1 to fluid neighbours, fluid rows only -- and its applyPressure (:109-212).  Face
+ *   weights must be NULL; the batch and backward entry points return XFP_ERR_UNSUPPORTED for it. */
+#define XFP_MATRIX_VARIATIONAL 0
+#define XFP_MATRIX_NORMAL 1
+
 typedef struct xfp_ctx xfp_ctx;
 
 typedef struct xfp_options {
@@ -67,6 +75,7 @@ typedef struct xfp_options {
   double inner_tol;      /* mixed: relative residual reduction per cycle (0: 1e-4) */
   int tile_k;            /* sweep tile height in k-lines: 8, 15 or 16; 0: timed on the first call per grid (or batch) shape and cached */
   void* stream;          /* cudaStream_t to run on; NULL: the context's own stream */
+  int matrix;            /* XFP_MATRIX_*: which pressure matrix the solve/project/apply entry points use */
 } xfp_options;
 
 typedef struct xfp_stats {

@@ -42,11 +42,8 @@ namespace xfp {
 class VariationalPressureSolver {
  public:
   // Precision XFP_PREC_F64 reproduces the reference's FP64 operation order.
-  explicit VariationalPressureSolver(int precision = XFP_PREC_F64, int device = 0) {
-    xfp_default_options(&opt_);
-    opt_.precision = precision;
-    opt_.device = device;
-  }
+  explicit VariationalPressureSolver(int precision = XFP_PREC_F64, int device = 0)
+      : VariationalPressureSolver(precision, device, XFP_MATRIX_VARIATIONAL) {}
   ~VariationalPressureSolver() {
     if (ctx_) xfp_destroy(ctx_);
   }
@@ -105,6 +102,14 @@ class VariationalPressureSolver {
   const xfp_stats& stats() const { return stats_; }
   const std::string& last_error() const { return err_; }
 
+ protected:
+  VariationalPressureSolver(int precision, int device, int matrix) {
+    xfp_default_options(&opt_);
+    opt_.precision = precision;
+    opt_.device = device;
+    opt_.matrix = matrix;
+  }
+
  private:
   bool ready() {
     if (!mat_ || !u_ || !v_ || !w_ || ni_ < 1 || nj_ < 1 || nk_ < 1) {
@@ -136,6 +141,16 @@ class VariationalPressureSolver {
   std::function<const uint8_t*()> mat_;
   void* disfield_ = nullptr;
   double density_ = 0.0, dt_ = 0.0, dx_ = 0.0;
+};
+
+// xFluid's NormalPressureSolver (xFluid/xFluid/pressuresolver.h:9-25): the same
+// nine methods over the classic Poisson matrix (pressuresolver.cpp:220-347) and
+// its applyPressure (:109-212), for a simulator built with the member at
+// FluidSimulator.h:216 (NormalPressureSolver _pressureSolver;).
+class NormalPressureSolver : public VariationalPressureSolver {
+ public:
+  explicit NormalPressureSolver(int precision = XFP_PREC_F64, int device = 0)
+      : VariationalPressureSolver(precision, device, XFP_MATRIX_NORMAL) {}
 };
 
 }  // namespace xfp

@@ -100,6 +100,11 @@ class Oracle(_Lib):
         L.xo_project.argtypes = ([C.c_int] * 3 + [_u8] + [_dp] * 6 + [C.c_double, C.c_int, _dp,
                                  C.POINTER(C.c_int), _dp])
         L.xo_project.restype = C.c_int
+        L.xo_assemble_normal.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 8
+        L.xo_apply_normal.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 4
+        L.xo_project_normal.argtypes = ([C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_double, C.c_int, _dp,
+                                        C.POINTER(C.c_int), _dp])
+        L.xo_project_normal.restype = C.c_int
 
     @staticmethod
     def _dims(sc):
@@ -189,6 +194,30 @@ class Oracle(_Lib):
                                  _p(wu), _p(wv), _p(ww), tol, maxit, _p(p), C.byref(it), C.byref(res))
         return dict(ok=bool(ok), p=p, u=u, v=v, w=w, iters=it.value, resid=res.value)
 
+    # ---- NormalPressureSolver (classic Poisson matrix) ----
+    def assemble_normal(self, sc):
+        n = (sc.nk, sc.nj, sc.ni)
+        out = [np.zeros(n) for _ in range(5)]
+        u, v, w = map(_f64, (sc.u, sc.v, sc.w))
+        self.lib.xo_assemble_normal(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w),
+                                    *[_p(a) for a in out])
+        return dict(zip(("diag", "ax", "ay", "az", "b"), out))
+
+    def apply_normal(self, sc, p):
+        u, v, w = (np.array(a, dtype=np.float64) for a in (sc.u, sc.v, sc.w))
+        self.lib.xo_apply_normal(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(_f64(p)), _p(u), _p(v),
+                                 _p(w))
+        return u, v, w
+
+    def project_normal(self, sc, tol=1e-6, maxit=200):
+        u, v, w = (np.array(a, dtype=np.float64) for a in (sc.u, sc.v, sc.w))
+        p = np.zeros((sc.nk, sc.nj, sc.ni))
+        it = C.c_int(0)
+        res = C.c_double(0)
+        ok = self.lib.xo_project_normal(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w),
+                                        tol, maxit, _p(p), C.byref(it), C.byref(res))
+        return dict(ok=bool(ok), p=p, u=u, v=v, w=w, iters=it.value, resid=res.value)
+
     def weighted_divergence(self, sc, u, v, w):
         """Per-cell m-weighted divergence that the projection drives to zero:
         the right-hand side b assembled from the given face velocities."""
@@ -214,6 +243,37 @@ class Reference(_Lib):
         L.xfref_factor.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 7
         L.xfref_precond.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 5
         L.xfref_divergence.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 4
+
+    def _normal_argtypes(self):
+        L = self.lib
+        L.xfref_normal_assemble.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 8
+        L.xfref_normal_assemble.restype = C.c_int
+        L.xfref_normal_solve.argtypes = ([C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_double, C.c_int, _dp,
+                                         C.POINTER(C.c_int), _dp])
+        L.xfref_normal_solve.restype = C.c_int
+        L.xfref_normal_apply.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 4
+
+    def normal_assemble(self, sc):
+        self._normal_argtypes()
+        n = (sc.nk, sc.nj, sc.ni)
+        out = [np.zeros(n) for _ in range(5)]
+        self.lib.xfref_normal_assemble(*self._in(sc), *[_p(a) for a in out])
+        return dict(zip(("diag", "ax", "ay", "az", "b"), out))
+
+    def normal_solve(self, sc, tol=1e-6, maxit=200):
+        self._normal_argtypes()
+        p = np.zeros((sc.nk, sc.nj, sc.ni))
+        it = C.c_int(0)
+        res = C.c_double(0)
+        ok = self.lib.xfref_normal_solve(*self._in(sc), tol, maxit, _p(p), C.byref(it), C.byref(res))
+        return dict(ok=bool(ok), p=p, iters=it.value, resid=res.value)
+
+    def normal_apply(self, sc, p):
+        self._normal_argtypes()
+        u, v, w = (np.array(a, dtype=np.float64) for a in (sc.u, sc.v, sc.w))
+        self.lib.xfref_normal_apply(sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(_f64(p)),
+                                    _p(u), _p(v), _p(w))
+        return u, v, w
 
     def _in(self, sc):
         return (sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(_f64(sc.u)),

@@ -1,5 +1,6 @@
 #!/usr/bin/env bash
-# Builds the reference xFluid pressure solver, unmodified, from its own sources
+# Builds the reference xFluid pressure solvers (variational and normal),
+# unmodified, from their own sources
 # into oracle/_ref/libxfref.so, together with oracle/ref_harness.cpp (the test
 # harness that binds it).  TEST INFRASTRUCTURE ONLY.
 #
@@ -25,6 +26,7 @@ CXX="${XFREF_CXX:-/usr/bin/g++}"
   -include climits -include cmath \
   -I"$SRC" -I"$SRC/variationalpressure" \
   "$SRC/variationalpressure/variational_pressuresolver.cpp" \
+  "$SRC/pressuresolver.cpp" \
   "$SRC/xfluidutil.cpp" \
   "$HERE/ref_harness.cpp" \
   -o "$OUT/libxfref.so.tmp"

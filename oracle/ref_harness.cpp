@@ -13,6 +13,8 @@
 //   xfref_factor     factor_modified_incomplete_cholesky0    variationalpressure/pcg_solver.h:85-186
 //   xfref_precond    solve_lower + solve_lower_transpose_in_place  pcg_solver.h:192-220
 //   xfref_divergence VariationalPressureSolver::_calculate_divergience :526-597
+//   xfref_normal_*   NormalPressureSolver (pressuresolver.cpp): solve :50-106,
+//                    applyPressure :109-212, _calculate_coefficient :220-347
 //
 // The solver's members are private; standard headers are included first and the
 // reference header is then included with private/protected mapped to public so
@@ -33,6 +35,7 @@
 #define private public
 #define protected public
 #include "variationalpressure/variational_pressuresolver.h"
+#include "pressuresolver.h"
 #undef private
 #undef protected
 
@@ -74,7 +77,8 @@ struct Scene {
         for (int i = 0; i < a.sizei(); ++i)
           dst[(size_t)k * a.sizei() * a.sizej() + (size_t)j * a.sizei() + i] = a(i, j, k);
   }
-  void wire(VariationalPressureSolver& s) {
+  template <typename Solver>
+  void wire(Solver& s) {
     s.setSize(ni, nj, nk);
     s.setMaterial(&mat);
     s.setVelocityField(&u, &v, &w);
@@ -246,6 +250,74 @@ void xfref_divergence(int ni, int nj, int nk, const uint8_t* mat, const double* 
   std::vector<double> d;
   s._calculate_divergience(d);
   std::memcpy(div, d.data(), d.size() * sizeof(double));
+}
+
+// ---- NormalPressureSolver (pressuresolver.cpp), the classic Poisson matrix ----
+
+// Its assembly, as dense per-cell arrays (the layout of xfref_assemble).
+int xfref_normal_assemble(int ni, int nj, int nk, const uint8_t* mat, const double* u,
+                          const double* v, const double* w, double* diag, double* ax,
+                          double* ay, double* az, double* b_out) {
+  MuteCout mute;
+  Scene sc(ni, nj, nk, mat, u, v, w);
+  NormalPressureSolver s;
+  sc.wire(s);
+  SparseMatrix<double> A;
+  std::vector<double> b;
+  s._calculate_coefficient(A, b);
+  const long n = (long)ni * nj * nk, nn = (long)ni * nj;
+  int maxrow = 0;
+  for (long c = 0; c < n; ++c) {
+    if ((int)A.index[c].size() > maxrow) maxrow = (int)A.index[c].size();
+    diag[c] = A(c, c);
+    ax[c] = entry(A, c, c - 1);
+    ay[c] = entry(A, c, c - ni);
+    az[c] = entry(A, c, c - nn);
+    b_out[c] = b[c];
+  }
+  return maxrow;
+}
+
+// Its solve at (tol, maxit); pressure written when it reports success.
+// Iterations and residual from the same PCG rerun on the same system.
+int xfref_normal_solve(int ni, int nj, int nk, const uint8_t* mat, const double* u,
+                       const double* v, const double* w, double tol, int maxit,
+                       double* p_out, int* iters_out, double* resid_out) {
+  MuteCout mute;
+  Scene sc(ni, nj, nk, mat, u, v, w);
+  NormalPressureSolver s;
+  sc.wire(s);
+  s.solver.set_solver_parameters(tol, maxit);
+  Array3d<double> p;
+  bool ok = s.solve(p);
+  SparseMatrix<double> A;
+  std::vector<double> b;
+  s._calculate_coefficient(A, b);
+  std::vector<double> x(b.size(), 0.0);
+  double res = 0.0;
+  int it = 0;
+  PCGSolver<double> pcg;
+  pcg.set_solver_parameters(tol, maxit);
+  pcg.solve(A, b, x, res, it);
+  if (iters_out) *iters_out = it;
+  if (resid_out) *resid_out = res;
+  if (ok && p_out) Scene::dump(p, p_out);
+  return ok ? 1 : 0;
+}
+
+// Its applyPressure on (u,v,w) in place, given a pressure grid.
+void xfref_normal_apply(int ni, int nj, int nk, const uint8_t* mat, const double* p,
+                        double* u, double* v, double* w) {
+  MuteCout mute;
+  Scene sc(ni, nj, nk, mat, u, v, w);
+  NormalPressureSolver s;
+  sc.wire(s);
+  Array3d<double> pg(ni, nj, nk);
+  Scene::fill(pg, p);
+  s.applyPressure(pg);
+  Scene::dump(sc.u, u);
+  Scene::dump(sc.v, v);
+  Scene::dump(sc.w, w);
 }
 
 }  // extern "C"

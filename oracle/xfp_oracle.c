@@ -19,6 +19,9 @@
  * Faces: u (ni+1,nj,nk), v (ni,nj+1,nk), w (ni,nj,nk+1) (FluidSimulator.h:177-181).
  * Material: 0 air, 1 fluid, 2 solid (material.h:4-8).
  *
+ * The normal solver (pressuresolver.cpp, the classic Poisson matrix and its
+ * applyPressure) is restated at the end of the file, pinned the same way.
+ *
  * Generalisation beyond the reference (fractional mode): optional per-face
  * open fractions wu/wv/ww in [0,1] multiply every face's contribution.  NULL
  * weights give exactly the reference's matrix.  A neighbour outside the grid is
@@ -520,6 +523,110 @@ int xo_project(int ni, int nj, int nk, const uint8_t* mat, double* u, double* v,
   xo_assemble(ni, nj, nk, mat, u, v, w, wu, wv, ww, d, ax, ay, az, b);
   int ok = xo_pcg(ni, nj, nk, d, ax, ay, az, b, tol, maxit, 0.97, 0.25, p, iters, resid);
   xo_apply(ni, nj, nk, mat, wu, wv, ww, p, u, v, w);
+  free(d); free(ax); free(ay); free(az); free(b);
+  return ok;
+}
+
+/* ---- NormalPressureSolver (pressuresolver.cpp): the classic Poisson matrix ----
+ * Assembly, _calculate_coefficient (:220-347).  Fluid rows only: A(c,c) is the
+ * number of in-range neighbours that are not solid, A(c,n) = -1 for each fluid
+ * neighbour n.  b(c) gathers the faces towards non-solid neighbours (out of
+ * range counts as solid, :288-339) in the order low-x face added, high-x face
+ * subtracted, then y, then z.  Each entry is written once, so the visiting
+ * order of the matrix loop does not matter; b's order does. */
+void xo_assemble_normal(int ni, int nj, int nk, const uint8_t* mat, const double* u,
+                        const double* v, const double* w, double* diag, double* ax,
+                        double* ay, double* az, double* b) {
+  grid_t g = mkgrid(ni, nj, nk);
+  static const int B_ORDER[6] = {1, 0, 3, 2, 5, 4}; /* -x,+x,-y,+y,-z,+z */
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i) {
+        size_t c = cidx(&g, i, j, k);
+        double bb = 0.0, ox = 0.0, oy = 0.0, oz = 0.0;
+        int count = 0;
+        if (mat[c] == FLUID) {
+          for (int t = 0; t < 6; ++t) {
+            int nb = B_ORDER[t];
+            int a = i + NEI[nb].di, bj = j + NEI[nb].dj, ck = k + NEI[nb].dk;
+            if (!inrange(&g, a, bj, ck)) continue;
+            uint8_t mn = mat[cidx(&g, a, bj, ck)];
+            if (mn == SOLID) continue;
+            double uf, mf, vs;
+            face_of(&g, i, j, k, nb, u, v, w, NULL, NULL, NULL, &uf, &mf, &vs);
+            ++count;
+            bb += vs * uf; /* +u on the low face, -u on the high face */
+            double off = mn == FLUID ? -1.0 : 0.0;
+            if (nb == 1) ox = off;
+            else if (nb == 3) oy = off;
+            else if (nb == 5) oz = off;
+          }
+        }
+        diag[c] = (double)count; ax[c] = ox; ay[c] = oy; az[c] = oz; b[c] = bb;
+      }
+}
+
+/* applyPressure (:109-212), factor 1.0, for the face between cells l and r
+ * (out of range counts as solid, :141-142): both fluid p2-p1; fluid|solid
+ * takes p2 = p1 + u, solid|fluid p1 = p2 - u; an air side is 0. */
+static int face_dp_normal(const grid_t* g, const uint8_t* mat, const double* p, int il, int jl,
+                          int kl, int ir, int jr, int kr, double uf, double* dp) {
+  int inl = inrange(g, il, jl, kl), inr = inrange(g, ir, jr, kr);
+  uint8_t ml = inl ? mat[cidx(g, il, jl, kl)] : SOLID;
+  uint8_t mr = inr ? mat[cidx(g, ir, jr, kr)] : SOLID;
+  const double factor = 1.0;
+  double p1, p2;
+  if (ml != FLUID && mr != FLUID) return 0;
+  if (ml == FLUID && mr == FLUID) {
+    p2 = p[cidx(g, ir, jr, kr)];
+    p1 = p[cidx(g, il, jl, kl)];
+  } else if (ml == FLUID) {
+    p1 = p[cidx(g, il, jl, kl)];
+    p2 = mr == SOLID ? p1 + uf / factor : 0.0;
+  } else {
+    p2 = p[cidx(g, ir, jr, kr)];
+    p1 = ml == SOLID ? p2 - uf / factor : 0.0;
+  }
+  *dp = p2 - p1;
+  return 1;
+}
+
+void xo_apply_normal(int ni, int nj, int nk, const uint8_t* mat, const double* p, double* u,
+                     double* v, double* w) {
+  grid_t g = mkgrid(ni, nj, nk);
+  const double factor = 1.0;
+  double dp;
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i <= ni; ++i) {
+        size_t f = uidx(&g, i, j, k);
+        if (face_dp_normal(&g, mat, p, i - 1, j, k, i, j, k, u[f], &dp)) u[f] = u[f] - factor * dp;
+      }
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j <= nj; ++j)
+      for (int i = 0; i < ni; ++i) {
+        size_t f = vidx(&g, i, j, k);
+        if (face_dp_normal(&g, mat, p, i, j - 1, k, i, j, k, v[f], &dp)) v[f] = v[f] - factor * dp;
+      }
+  for (int k = 0; k <= nk; ++k)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i) {
+        size_t f = widx(&g, i, j, k);
+        if (face_dp_normal(&g, mat, p, i, j, k - 1, i, j, k, w[f], &dp)) w[f] = w[f] - factor * dp;
+      }
+}
+
+/* NormalPressureSolver::solve (:50-106) + applyPressure on the same grids. */
+int xo_project_normal(int ni, int nj, int nk, const uint8_t* mat, double* u, double* v, double* w,
+                      double tol, int maxit, double* p, int* iters, double* resid) {
+  grid_t g = mkgrid(ni, nj, nk);
+  size_t n = g.n;
+  double *d = malloc(n * sizeof(double)), *ax = malloc(n * sizeof(double)),
+         *ay = malloc(n * sizeof(double)), *az = malloc(n * sizeof(double)),
+         *b = malloc(n * sizeof(double));
+  xo_assemble_normal(ni, nj, nk, mat, u, v, w, d, ax, ay, az, b);
+  int ok = xo_pcg(ni, nj, nk, d, ax, ay, az, b, tol, maxit, 0.97, 0.25, p, iters, resid);
+  xo_apply_normal(ni, nj, nk, mat, p, u, v, w);
   free(d); free(ax); free(ay); free(az); free(b);
   return ok;
 }

@@ -13,6 +13,12 @@ assembly (diag, ax, ay, az, b), MIC(0) factor (inv, lx, ly, lz), the
 preconditioner applied to a seeded residual (r -> z), the PCG pressure at
 tol 1e-6 (iterations, residual), the velocities after applyPressure, and the
 reference's divergence diagnostic after the projection.
+
+``normal_<case>.npz`` holds the same scene inputs run through xFluid's
+NormalPressureSolver (pressuresolver.cpp, the classic Poisson matrix): its
+assembly (diag, ax, ay, az, b), its PCG pressure at tol 1e-6 (iterations,
+residual) and the velocities after its applyPressure.  ``--normal-only``
+writes just those.
 """
 from __future__ import annotations
 
@@ -40,10 +46,33 @@ def cases():
     }
 
 
+NORMAL_CASES = ("dam16", "blob24x20x22")
+
+
+def normal_fixtures(R):
+    for name, sc in cases().items():
+        if name not in NORMAL_CASES:
+            continue
+        A = R.normal_assemble(sc)
+        sol = R.normal_solve(sc, TOL, MAXIT)
+        assert sol["ok"], name
+        u2, v2, w2 = R.normal_apply(sc, sol["p"])
+        np.savez_compressed(
+            OUT / f"normal_{name}.npz",
+            dims=np.array([sc.ni, sc.nj, sc.nk]), mat=sc.mat, u=sc.u, v=sc.v, w=sc.w,
+            diag=A["diag"], ax=A["ax"], ay=A["ay"], az=A["az"], b=A["b"],
+            p=sol["p"], iters=sol["iters"], resid=sol["resid"], tol=TOL, maxit=MAXIT,
+            u_out=u2, v_out=v2, w_out=w2)
+        print(f"normal_{name}: {int((A['diag'] != 0).sum())} rows, {sol['iters']} iterations")
+
+
 def main():
     if build_reference() is None:
         raise SystemExit("reference sources not found; cannot regenerate golden vectors")
     R = Reference()
+    normal_fixtures(R)
+    if "--normal-only" in sys.argv:
+        return
     for name, sc in cases().items():
         A = R.assemble(sc)
         F = R.factor(sc)

@@ -6,10 +6,10 @@ the Python mirror of VariationalPressureSolver.
 """
 import importlib
 
-__all__ = ["VariationalPressureSolver", "project_scene", "scenes"]
+__all__ = ["VariationalPressureSolver", "NormalPressureSolver", "project_scene", "scenes"]
 
 
 def __getattr__(name):
-    if name in ("VariationalPressureSolver", "project_scene"):
+    if name in ("VariationalPressureSolver", "NormalPressureSolver", "project_scene"):
         return getattr(importlib.import_module(__name__ + ".solver"), name)
     raise AttributeError(name)

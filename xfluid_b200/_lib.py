@@ -20,6 +20,7 @@ XFP_ERR_BREAKDOWN = -5
 XFP_ERR_UNSUPPORTED = -6
 
 PREC = {"f64": 0, "f32": 1, "mixed": 2}
+MATRIX = {"variational": 0, "normal": 1}
 
 
 class XfpOptions(C.Structure):
@@ -37,6 +38,7 @@ class XfpOptions(C.Structure):
         ("inner_tol", C.c_double),
         ("tile_k", C.c_int),
         ("stream", C.c_void_p),
+        ("matrix", C.c_int),
     ]
 
 

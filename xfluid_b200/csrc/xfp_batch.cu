@@ -528,6 +528,8 @@ template <typename IOT>
 int project_batch(xfp_ctx* ctx, int n, const xfp_scene* scenes, xfp_stats* stats) {
   if (!ctx) return XFP_ERR_ARGS;
   if (n < 1 || !scenes) return fail(ctx, XFP_ERR_ARGS, "batch needs n >= 1 scenes");
+  if (ctx->opt.matrix != XFP_MATRIX_VARIATIONAL)
+    return fail(ctx, XFP_ERR_UNSUPPORTED, "batched projection supports the variational matrix only");
   for (int s = 0; s < n; ++s) {
     const xfp_scene& c = scenes[s];
     int rc = check_dims(ctx, c.ni, c.nj, c.nk, c.material);

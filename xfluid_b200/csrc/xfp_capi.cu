@@ -404,7 +404,7 @@ int tune_tile_height(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, 
     float* A[5];
     for (int q = 0; q < 5; ++q) A[q] = ctx->A32[q].as<float>();
     if (assemble<IOT, float>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, ctx->lines.as<Line>(), A[0], A[1], A[2],
-                             A[3], A[4], st) != cudaSuccess) { rc = fail(ctx, XFP_ERR_CUDA, "assembly failed"); break; }
+                             A[3], A[4], st, ctx->opt.matrix) != cudaSuccess) { rc = fail(ctx, XFP_ERR_CUDA, "assembly failed"); break; }
     float* F[6];
     for (int q = 0; q < 6; ++q) F[q] = ctx->F32[q].as<float>();
     const float* Ac[4] = {A[0], A[1], A[2], A[3]};
@@ -466,7 +466,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     double* A[5];
     for (int q = 0; q < 5; ++q) A[q] = ctx->A64[q].as<double>();
     XFP_CUDA(ctx, (assemble<IOT, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
-                                         A[3], A[4], st)));
+                                         A[3], A[4], st, ctx->opt.matrix)));
     if (adj_gu) XFP_CUDA(ctx, (apply_pressure_T<IOT, double>(dmat, dwu, dwv, dww, adj_gu, adj_gv, adj_gw, ni, nj,
                                                              nk, lines, A[4], st)));
     ev_record(ctx, 1);
@@ -486,7 +486,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     float* A[5];
     for (int q = 0; q < 5; ++q) A[q] = ctx->A32[q].as<float>();
     XFP_CUDA(ctx, (assemble<IOT, float>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
-                                        A[3], A[4], st)));
+                                        A[3], A[4], st, ctx->opt.matrix)));
     if (adj_gu) XFP_CUDA(ctx, (apply_pressure_T<IOT, float>(dmat, dwu, dwv, dww, adj_gu, adj_gv, adj_gw, ni, nj,
                                                             nk, lines, A[4], st)));
     ev_record(ctx, 1);
@@ -507,7 +507,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     double* A[5];
     for (int q = 0; q < 5; ++q) A[q] = ctx->A64[q].as<double>();
     XFP_CUDA(ctx, (assemble<IOT, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
-                                         A[3], A[4], st)));
+                                         A[3], A[4], st, ctx->opt.matrix)));
     if (adj_gu) XFP_CUDA(ctx, (apply_pressure_T<IOT, double>(dmat, dwu, dwv, dww, adj_gu, adj_gv, adj_gw, ni, nj,
                                                              nk, lines, A[4], st)));
     float* A32[4];
@@ -646,6 +646,8 @@ int project_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* 
   if (!u || !v || !w) return fail(ctx, XFP_ERR_ARGS, "velocity arrays must not be NULL");
   if ((wu == nullptr) != (wv == nullptr) || (wu == nullptr) != (ww == nullptr))
     return fail(ctx, XFP_ERR_ARGS, "face weights: pass all three or none");
+  if (ctx->opt.matrix == XFP_MATRIX_NORMAL && wu != nullptr)
+    return fail(ctx, XFP_ERR_ARGS, "the normal matrix takes no face weights");
   if (!do_apply && !pressure) return fail(ctx, XFP_ERR_ARGS, "pressure output is NULL");
   XFP_CUDA(ctx, cudaSetDevice(ctx->device));
   ctx->launches = g_kernel_launches;
@@ -680,7 +682,8 @@ int project_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* 
     IOT* mu = const_cast<IOT*>(du_);
     IOT* mv = const_cast<IOT*>(dv);
     IOT* mw = const_cast<IOT*>(dw);
-    XFP_CUDA(ctx, (apply_pressure<IOT, IOT>(dmat, dwu, dwv, dww, dp, ni, nj, nk, mu, mv, mw, ctx->stream)));
+    XFP_CUDA(ctx, (apply_pressure<IOT, IOT>(dmat, dwu, dwv, dww, dp, ni, nj, nk, mu, mv, mw, ctx->stream,
+                                            ctx->opt.matrix)));
   }
   ev_record(ctx, 4);
   if (!ctx->opt.device_pointers) {
@@ -714,6 +717,8 @@ int apply_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, const I
   int rc = check_dims(ctx, ni, nj, nk, mat);
   if (rc) return rc;
   if (!u || !v || !w || !pressure) return fail(ctx, XFP_ERR_ARGS, "NULL array");
+  if (ctx->opt.matrix == XFP_MATRIX_NORMAL && (wu || wv || ww))
+    return fail(ctx, XFP_ERR_ARGS, "the normal matrix takes no face weights");
   XFP_CUDA(ctx, cudaSetDevice(ctx->device));
   const uint8_t* dmat;
   const IOT *du_, *dv, *dw, *dwu, *dwv, *dww, *dp;
@@ -726,7 +731,8 @@ int apply_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, const I
   if ((rc = stage_in<IOT>(ctx, ctx->io_ww, ww, nw_(ni, nj, nk), &dww))) return rc;
   if ((rc = stage_in<IOT>(ctx, ctx->io_p, pressure, ncells(ni, nj, nk), &dp))) return rc;
   XFP_CUDA(ctx, (apply_pressure<IOT, IOT>(dmat, dwu, dwv, dww, dp, ni, nj, nk, const_cast<IOT*>(du_),
-                                          const_cast<IOT*>(dv), const_cast<IOT*>(dw), ctx->stream)));
+                                          const_cast<IOT*>(dv), const_cast<IOT*>(dw), ctx->stream,
+                                          ctx->opt.matrix)));
   if (!ctx->opt.device_pointers) {
     XFP_CUDA(ctx, cudaMemcpyAsync(u, du_, nu(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
     XFP_CUDA(ctx, cudaMemcpyAsync(v, dv, nv(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
@@ -743,6 +749,8 @@ int backward_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, cons
   int rc = check_dims(ctx, ni, nj, nk, mat);
   if (rc) return rc;
   if (!gu || !gv || !gw || !du || !dv || !dw) return fail(ctx, XFP_ERR_ARGS, "NULL gradient array");
+  if (ctx->opt.matrix != XFP_MATRIX_VARIATIONAL)
+    return fail(ctx, XFP_ERR_UNSUPPORTED, "the backward projection supports the variational matrix only");
   if ((wu == nullptr) != (wv == nullptr) || (wu == nullptr) != (ww == nullptr))
     return fail(ctx, XFP_ERR_ARGS, "face weights: pass all three or none");
   XFP_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -920,6 +928,7 @@ void xfp_default_options(xfp_options* o) {
   o->max_refine = 20;
   o->inner_tol = 1e-6;
   o->tile_k = 0;
+  o->matrix = XFP_MATRIX_VARIATIONAL;
   o->stream = nullptr;
 }
 
@@ -929,6 +938,8 @@ static int validate_options(xfp_ctx* ctx, const xfp_options* o) {
   if (!(o->min_diag_ratio >= 0.0)) return fail(ctx, XFP_ERR_ARGS, "min_diag_ratio must be >= 0");
   if (o->tile_k != 0 && o->tile_k != 8 && o->tile_k != 15 && o->tile_k != 16)
     return fail(ctx, XFP_ERR_ARGS, "tile_k must be 0, 8, 15 or 16");
+  if (o->matrix != XFP_MATRIX_VARIATIONAL && o->matrix != XFP_MATRIX_NORMAL)
+    return fail(ctx, XFP_ERR_ARGS, "matrix must be XFP_MATRIX_VARIATIONAL or XFP_MATRIX_NORMAL");
   return XFP_OK;
 }
 
@@ -1089,7 +1100,7 @@ int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* materi
     double* A[5];
     for (int k = 0; k < 5; ++k) A[k] = ctx->A64[k].as<double>();
     XFP_CUDA(ctx, (assemble<double, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
-                                            A[3], A[4], st)));
+                                            A[3], A[4], st, ctx->opt.matrix)));
     double* F[6];
     for (int k = 0; k < 6; ++k) F[k] = ctx->F64[k].as<double>();
     const double* Af[5] = {A[0], A[1], A[2], A[3], A[4]};
@@ -1100,7 +1111,7 @@ int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* materi
     float* A[5];
     for (int k = 0; k < 5; ++k) A[k] = ctx->A32[k].as<float>();
     XFP_CUDA(ctx, (assemble<double, float>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
-                                           A[3], A[4], st)));
+                                           A[3], A[4], st, ctx->opt.matrix)));
     float* F[6];
     for (int k = 0; k < 6; ++k) F[k] = ctx->F32[k].as<float>();
     const float* Af[5] = {A[0], A[1], A[2], A[3], A[4]};
@@ -1111,7 +1122,7 @@ int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* materi
     double* A[5];
     for (int k = 0; k < 5; ++k) A[k] = ctx->A64[k].as<double>();
     XFP_CUDA(ctx, (assemble<double, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
-                                            A[3], A[4], st)));
+                                            A[3], A[4], st, ctx->opt.matrix)));
     float* A32[4];
     for (int k = 0; k < 4; ++k) {
       A32[k] = ctx->A32[k].as<float>();

@@ -19,6 +19,10 @@
 
 #define XFP_ALIGN 4
 #define XFP_FULL 0xffffffffu
+#ifndef XFP_MATRIX_NORMAL   // the same values as include/xfp.h
+#define XFP_MATRIX_VARIATIONAL 0
+#define XFP_MATRIX_NORMAL 1
+#endif
 
 namespace xfp {
 

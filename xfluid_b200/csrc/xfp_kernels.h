@@ -119,7 +119,8 @@ cudaError_t layout_build(const uint8_t* mat, int ni, int nj, int nk, int tile_k,
 template <typename FT, typename AT>
 cudaError_t assemble(const uint8_t* mat, const FT* u, const FT* v, const FT* w, const FT* wu,
                      const FT* wv, const FT* ww, int ni, int nj, int nk, const Line* lines,
-                     AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st);
+                     AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st,
+                     int matrix = XFP_MATRIX_VARIATIONAL);
 
 template <typename T>
 cudaError_t scatter_dense(const T* x, const Line* lines, int ni, int nj, int nk, T* dense,
@@ -127,7 +128,7 @@ cudaError_t scatter_dense(const T* x, const Line* lines, int ni, int nj, int nk,
 template <typename FT, typename PT>
 cudaError_t apply_pressure(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
                            const PT* p, int ni, int nj, int nk, FT* u, FT* v, FT* w,
-                           cudaStream_t st);
+                           cudaStream_t st, int matrix = XFP_MATRIX_VARIATIONAL);
 template <typename FT, typename PT>
 cudaError_t apply_pressure_T(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
                              const FT* gu, const FT* gv, const FT* gw, int ni, int nj, int nk,

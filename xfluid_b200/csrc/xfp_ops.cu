@@ -44,7 +44,7 @@ __global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __res
                                 const FT* __restrict__ ww, int ni, int nj, int nk,
                                 const Line* __restrict__ lines, AT* __restrict__ diag,
                                 AT* __restrict__ ax, AT* __restrict__ ay, AT* __restrict__ az,
-                                AT* __restrict__ b) {
+                                AT* __restrict__ b, int matrix) {
   const int lane = threadIdx.x & 31;
   const long long nlines = (long long)nj * nk;
   const size_t nn = (size_t)ni * nj;
@@ -81,7 +81,34 @@ __global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __res
           }
           return true;
         };
-        if (m == MAT_FLUID) {
+        if (matrix == XFP_MATRIX_NORMAL) {
+          // NormalPressureSolver::_calculate_coefficient (pressuresolver.cpp:220-347):
+          // fluid rows only; diagonal = in-range non-solid neighbours, -1 to
+          // each fluid neighbour; b gathers the faces towards non-solid
+          // neighbours (out of range counts as solid) in the order u low, u
+          // high, v low, v high, w low, w high, the low face added and the
+          // high face subtracted.
+          if (m == MAT_FLUID) {
+            int count = 0;
+            const int order[6] = {1, 0, 3, 2, 5, 4};
+#pragma unroll
+            for (int t = 0; t < 6; ++t) {
+              const int nb = order[t];
+              AT uf, mf, vs;
+              int ii, jj, kk;
+              if (!face(nb, uf, mf, vs, ii, jj, kk)) continue;
+              const uint8_t mn = mat[(size_t)kk * nn + (size_t)jj * ni + ii];
+              if (mn == MAT_SOLID) continue;
+              ++count;
+              bb = add_rn(bb, mul_rn(vs, uf));
+              const AT off = mn == MAT_FLUID ? AT(-1) : AT(0);
+              if (nb == 1) ox = off;
+              if (nb == 3) oy = off;
+              if (nb == 5) oz = off;
+            }
+            d = AT(count);
+          }
+        } else if (m == MAT_FLUID) {
 #pragma unroll
           for (int nb = 0; nb < 6; ++nb) {
             AT uf, mf, vs;
@@ -131,31 +158,31 @@ __global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __res
 template <typename FT, typename AT>
 cudaError_t assemble(const uint8_t* mat, const FT* u, const FT* v, const FT* w, const FT* wu,
                      const FT* wv, const FT* ww, int ni, int nj, int nk, const Line* lines,
-                     AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st) {
+                     AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st, int matrix) {
   const long long nlines = (long long)nj * nk;
   long long blocks = (nlines + 7) / 8;
   if (blocks > 65535 * 8) blocks = 65535 * 8;
   ++g_kernel_launches;
   assemble_kernel<FT, AT><<<(unsigned)blocks, 256, 0, st>>>(mat, u, v, w, wu, wv, ww, ni, nj, nk, lines,
-                                                          diag, ax, ay, az, b);
+                                                          diag, ax, ay, az, b, matrix);
   return cudaGetLastError();
 }
 template cudaError_t assemble<double, double>(const uint8_t*, const double*, const double*,
                                               const double*, const double*, const double*,
                                               const double*, int, int, int, const Line*, double*,
-                                              double*, double*, double*, double*, cudaStream_t);
+                                              double*, double*, double*, double*, cudaStream_t, int);
 template cudaError_t assemble<float, float>(const uint8_t*, const float*, const float*, const float*,
                                             const float*, const float*, const float*, int, int, int,
                                             const Line*, float*, float*, float*, float*, float*,
-                                            cudaStream_t);
+                                            cudaStream_t, int);
 template cudaError_t assemble<float, double>(const uint8_t*, const float*, const float*,
                                              const float*, const float*, const float*, const float*,
                                              int, int, int, const Line*, double*, double*, double*,
-                                             double*, double*, cudaStream_t);
+                                             double*, double*, cudaStream_t, int);
 template cudaError_t assemble<double, float>(const uint8_t*, const double*, const double*,
                                              const double*, const double*, const double*,
                                              const double*, int, int, int, const Line*, float*,
-                                             float*, float*, float*, float*, cudaStream_t);
+                                             float*, float*, float*, float*, cudaStream_t, int);
 
 // ---------------------------------------------------------------------------
 // Compact -> dense pressure grid: every cell written, 0 outside unknowns
@@ -253,16 +280,53 @@ __device__ __forceinline__ bool face_dp(const uint8_t* mat, const PT* p, int ni,
   return true;
 }
 
+// NormalPressureSolver::applyPressure (pressuresolver.cpp:109-212) for one face
+// with left cell l and right cell r (out of range counts as solid), factor 1:
+// fluid|solid takes p2 = p1 + f, solid|fluid p1 = p2 - f, a fluid|air face
+// takes 0 for the air side.  Returns false where no side is fluid.
+template <typename PT>
+__device__ __forceinline__ bool face_dp_normal(const uint8_t* __restrict__ mat, const PT* __restrict__ p, int ni,
+                                               int nj, int nk, int il, int jl, int kl, int ir, int jr, int kr, PT fv,
+                                               PT& dp) {
+  const size_t nn = (size_t)ni * nj;
+  const bool inl = il >= 0 && jl >= 0 && kl >= 0 && il < ni && jl < nj && kl < nk;
+  const bool inr = ir >= 0 && jr >= 0 && kr >= 0 && ir < ni && jr < nj && kr < nk;
+  const size_t cl = inl ? (size_t)kl * nn + (size_t)jl * ni + il : 0;
+  const size_t cr = inr ? (size_t)kr * nn + (size_t)jr * ni + ir : 0;
+  const uint8_t ml = inl ? mat[cl] : MAT_SOLID;
+  const uint8_t mr = inr ? mat[cr] : MAT_SOLID;
+  if (ml != MAT_FLUID && mr != MAT_FLUID) return false;
+  PT p1, p2;
+  if (ml == MAT_FLUID && mr == MAT_FLUID) {
+    p2 = p[cr]; p1 = p[cl];
+  } else if (ml == MAT_FLUID) {
+    p1 = p[cl];
+    p2 = mr == MAT_SOLID ? add_rn(p1, fv) : PT(0);
+  } else {
+    p2 = p[cr];
+    p1 = ml == MAT_SOLID ? sub_rn(p2, fv) : PT(0);
+  }
+  dp = sub_rn(p2, p1);
+  return true;
+}
+
 template <typename FT, typename PT>
 __global__ void apply_kernel(const uint8_t* __restrict__ mat, const FT* __restrict__ wt,
                              const PT* __restrict__ p, int ni, int nj, int nk, int axis,
-                             FT* __restrict__ f) {
+                             FT* __restrict__ f, int matrix) {
   const int si = ni + (axis == 0), sj = nj + (axis == 1), sk = nk + (axis == 2);
   const size_t n = (size_t)si * sj * sk;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(idx % si);
     const int j = (int)((idx / si) % sj);
     const int k = (int)(idx / ((size_t)si * sj));
+    if (matrix == XFP_MATRIX_NORMAL) {
+      PT dp;
+      if (face_dp_normal(mat, p, ni, nj, nk, i - (axis == 0), j - (axis == 1), k - (axis == 2), i, j, k,
+                         (PT)f[idx], dp))
+        f[idx] = sub_rn(f[idx], (FT)mul_rn(PT(1), dp));
+      continue;
+    }
     if (wt && wt[idx] == FT(0)) continue;
     PT dp;
     if (face_dp(mat, p, ni, nj, nk, i - (axis == 0), j - (axis == 1), k - (axis == 2), i, j, k, dp)) {
@@ -273,22 +337,22 @@ __global__ void apply_kernel(const uint8_t* __restrict__ mat, const FT* __restri
 template <typename FT, typename PT>
 cudaError_t apply_pressure(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
                            const PT* p, int ni, int nj, int nk, FT* u, FT* v, FT* w,
-                           cudaStream_t st) {
+                           cudaStream_t st, int matrix) {
   for (int axis = 0; axis < 3; ++axis) {
     size_t n = (size_t)(ni + (axis == 0)) * (nj + (axis == 1)) * (nk + (axis == 2));
     unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32);
     ++g_kernel_launches;
     apply_kernel<FT, PT><<<blocks, 256, 0, st>>>(mat, axis == 0 ? wu : axis == 1 ? wv : ww, p, ni, nj, nk,
-                                                axis, axis == 0 ? u : axis == 1 ? v : w);
+                                                axis, axis == 0 ? u : axis == 1 ? v : w, matrix);
   }
   return cudaGetLastError();
 }
 template cudaError_t apply_pressure<double, double>(const uint8_t*, const double*, const double*,
                                                     const double*, const double*, int, int, int,
-                                                    double*, double*, double*, cudaStream_t);
+                                                    double*, double*, double*, cudaStream_t, int);
 template cudaError_t apply_pressure<float, float>(const uint8_t*, const float*, const float*,
                                                   const float*, const float*, int, int, int, float*,
-                                                  float*, float*, cudaStream_t);
+                                                  float*, float*, cudaStream_t, int);
 
 // ---------------------------------------------------------------------------
 // Adjoint of the pressure update: q = G^T g, where applyPressure computes

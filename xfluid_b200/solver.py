@@ -60,6 +60,8 @@ def _on_device(a) -> bool:
 class VariationalPressureSolver:
     """Drop-in for xFluid's VariationalPressureSolver on a B200."""
 
+    _MATRIX = "variational"
+
     def __init__(self, precision: str = "f64", device: int = 0, tol: float = 1e-5, max_iter: int = 100,
                  omega: float = 0.97, min_diag_ratio: float = 0.25, check_every: int = 8,
                  timeout_ms: float = 2000.0, tile_k: int = 0):
@@ -67,6 +69,7 @@ class VariationalPressureSolver:
         o.tol, o.max_iter, o.omega, o.min_diag_ratio = tol, max_iter, omega, min_diag_ratio
         o.precision = _lib.PREC[precision]
         o.device, o.check_every, o.timeout_ms, o.tile_k = device, check_every, timeout_ms, tile_k
+        o.matrix = _lib.MATRIX[self._MATRIX]
         self._ctx = Context(o)
         self._size = (0, 0, 0)
         self._u = self._v = self._w = None
@@ -204,3 +207,18 @@ def project_scene(sc, precision: str = "f64", tol: float = 1e-6, max_iter: int =
         s.setFaceWeights(None, None, None)
     ok = s.project(p)
     return ok, p, u, v, w, dict(s.stats)
+
+
+class NormalPressureSolver(VariationalPressureSolver):
+    """Drop-in for xFluid's NormalPressureSolver (pressuresolver.h:9-25), the
+    classic Poisson matrix on the same MIC(0)-PCG: for every fluid cell the
+    diagonal is the number of in-range non-solid neighbours and -1 couples it
+    to each fluid neighbour (pressuresolver.cpp:220-347); applyPressure
+    updates faces touching fluid with solid faces reflecting and air faces at
+    zero pressure (:109-212).  The same nine methods with the same meanings;
+    the reference class has no face weights, so setFaceWeights is refused."""
+
+    _MATRIX = "normal"
+
+    def setFaceWeights(self, wu, wv, ww) -> None:
+        raise ValueError("the normal pressure matrix has no face weights")
