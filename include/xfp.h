@@ -227,6 +227,36 @@ int xfp_box_loss_f32(xfp_ctx* ctx, int ni, int nj, int nk, const float* u, const
  * sweep tile.  Used by the tests of the timeout path. */
 int xfp_debug_expire_next_sweep(xfp_ctx* ctx);
 
+/* ---- The simulator steps either side of the projection ----
+ * FluidSimulator::timeStep applies the body forces (FluidSimulator.cpp:310), solves and
+ * applies the pressure (:501-509) and then extrapolates the velocities (:322).
+ *
+ * xfp_apply_forces_*: FluidSimulator::_applyForces (FluidSimulator.cpp:429-499).  force is
+ * the summed constant force (the sum of _forces); every face with a fluid cell on either side
+ * gets force*dt, an axis with |force*dt| <= 1e-10 none.  u,v,w in place.
+ * xfp_extrapolate_*: FluidSimulator::_expolateVelocity(layers, axis) for the three axes
+ * (:521-650): layer by layer outward from the faces of fluid cells, each face of a layer takes
+ * the average of its neighbours in the layer before.  The reference passes
+ * layers = (int)(CFL number + 5) (:513).  0 <= layers <= 30000.  u,v,w in place.
+ * xfp_project_step_*: both around one projection, in the reference's order: the force
+ * enters inside the assembly and apply kernels (no separate pass over the velocities), then
+ * the projection of xfp_project_*, then `layers` extrapolation layers on the projected
+ * velocities (0: none).  Arrays as for xfp_project_*; pressure may be NULL. */
+int xfp_apply_forces_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, double* u, double* v,
+                         double* w, const double force[3], double dt);
+int xfp_apply_forces_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, float* u, float* v,
+                         float* w, const double force[3], double dt);
+int xfp_extrapolate_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, double* u, double* v,
+                        double* w, int layers);
+int xfp_extrapolate_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, float* u, float* v,
+                        float* w, int layers);
+int xfp_project_step_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, double* u, double* v,
+                         double* w, const double* wu, const double* wv, const double* ww, double* pressure,
+                         const double force[3], double dt, int layers, xfp_stats* stats);
+int xfp_project_step_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, float* u, float* v,
+                         float* w, const float* wu, const float* wv, const float* ww, float* pressure,
+                         const double force[3], double dt, int layers, xfp_stats* stats);
+
 /* Diagnostics: runs the internal stages on one scene and returns them on the
  * dense grid (ni*nj*nk doubles each; any output may be NULL), in the
  * context's precision.  Exposes, for verification against the reference:

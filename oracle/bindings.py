@@ -105,6 +105,8 @@ class Oracle(_Lib):
         L.xo_project_normal.argtypes = ([C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_double, C.c_int, _dp,
                                         C.POINTER(C.c_int), _dp])
         L.xo_project_normal.restype = C.c_int
+        L.xo_apply_forces.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_double] * 4
+        L.xo_extrapolate.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_int]
 
     @staticmethod
     def _dims(sc):
@@ -193,6 +195,18 @@ class Oracle(_Lib):
         ok = self.lib.xo_project(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w),
                                  _p(wu), _p(wv), _p(ww), tol, maxit, _p(p), C.byref(it), C.byref(res))
         return dict(ok=bool(ok), p=p, u=u, v=v, w=w, iters=it.value, resid=res.value)
+
+    # ---- the simulator steps either side of the projection ----
+    def apply_forces(self, sc, force, dt, uvw=None):
+        u, v, w = (np.array(a, dtype=np.float64) for a in (uvw or (sc.u, sc.v, sc.w)))
+        self.lib.xo_apply_forces(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w),
+                                 *map(float, force), float(dt))
+        return u, v, w
+
+    def extrapolate(self, sc, layers, uvw=None):
+        u, v, w = (np.array(a, dtype=np.float64) for a in (uvw or (sc.u, sc.v, sc.w)))
+        self.lib.xo_extrapolate(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w), int(layers))
+        return u, v, w
 
     # ---- NormalPressureSolver (classic Poisson matrix) ----
     def assemble_normal(self, sc):
@@ -387,3 +401,26 @@ class RefSim(_Lib):
 
     def fluid_cells(self):
         return self.lib.xfsim_fluid_cells(self.h)
+
+
+class RefSteps(_Lib):
+    """xFluid's own FluidSimulator::_applyForces and _expolateVelocity on given
+    arrays (oracle/sim_harness.cpp, built from the reference sources)."""
+
+    def __init__(self):
+        super().__init__(SIM_LIB)
+        L = self.lib
+        L.xfsim_apply_forces.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_double] * 4
+        L.xfsim_extrapolate.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_int]
+
+    def apply_forces(self, sc, force, dt, uvw=None):
+        u, v, w = (np.array(a, dtype=np.float64) for a in (uvw or (sc.u, sc.v, sc.w)))
+        self.lib.xfsim_apply_forces(sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w),
+                                    *map(float, force), float(dt))
+        return u, v, w
+
+    def extrapolate(self, sc, layers, uvw=None):
+        u, v, w = (np.array(a, dtype=np.float64) for a in (uvw or (sc.u, sc.v, sc.w)))
+        self.lib.xfsim_extrapolate(sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w),
+                                   int(layers))
+        return u, v, w

@@ -165,4 +165,54 @@ void xfsim_end_step(void* h) {
 
 int xfsim_fluid_cells(void* h) { return static_cast<Sim*>(h)->fs._countFluidCell(); }
 
+// The two steps either side of the projection on given arrays, through a
+// simulator of the grid's size (FluidSimulator(ni,nj,nk) only sizes its grids,
+// FluidSimulator.cpp:26-31): material and faces are filled in, the step runs,
+// the faces are read back.
+namespace {
+struct Fields {
+  FluidSimulator fs;
+  Fields(int ni, int nj, int nk, const uint8_t* mat, const double* u, const double* v, const double* w)
+      : fs(ni, nj, nk) {
+    for (int k = 0; k < nk; ++k)
+      for (int j = 0; j < nj; ++j)
+        for (int i = 0; i < ni; ++i)
+          fs._material(i, j, k) = static_cast<Material>(mat[(size_t)k * ni * nj + (size_t)j * ni + i]);
+    fill(fs._u, u);
+    fill(fs._v, v);
+    fill(fs._w, w);
+  }
+  static void fill(Array3d<double>& a, const double* src) {
+    for (int k = 0; k < a.sizek(); ++k)
+      for (int j = 0; j < a.sizej(); ++j)
+        for (int i = 0; i < a.sizei(); ++i)
+          a(i, j, k) = src[(size_t)k * a.sizei() * a.sizej() + (size_t)j * a.sizei() + i];
+  }
+  void out(double* u, double* v, double* w) {
+    dump(fs._u, u);
+    dump(fs._v, v);
+    dump(fs._w, w);
+  }
+};
+}  // namespace
+
+// _applyForces (FluidSimulator.cpp:429-499) with one constant force (fx,fy,fz).
+void xfsim_apply_forces(int ni, int nj, int nk, const uint8_t* mat, double* u, double* v, double* w,
+                        double fx, double fy, double fz, double dt) {
+  MuteCout mute;
+  Fields f(ni, nj, nk, mat, u, v, w);
+  f.fs._forces.clear();
+  f.fs.addConstantForce(Vec3d(fx, fy, fz));
+  f.fs._applyForces(dt);
+  f.out(u, v, w);
+}
+
+// _expolateVelocity(layers, axis) for axes 0, 1, 2 (FluidSimulator.cpp:516-518, 521-650).
+void xfsim_extrapolate(int ni, int nj, int nk, const uint8_t* mat, double* u, double* v, double* w, int layers) {
+  MuteCout mute;
+  Fields f(ni, nj, nk, mat, u, v, w);
+  for (int axis = 0; axis < 3; ++axis) f.fs._expolateVelocity(layers, axis);
+  f.out(u, v, w);
+}
+
 }  // extern "C"

@@ -630,3 +630,108 @@ int xo_project_normal(int ni, int nj, int nk, const uint8_t* mat, double* u, dou
   free(d); free(ax); free(ay); free(az); free(b);
   return ok;
 }
+
+/* ---- The simulator steps either side of the projection (FluidSimulator.cpp) ---- */
+
+/* _applyForces (:429-499): dv = (sum of forces) * dt per axis; every face with
+ * an in-range fluid cell on either side gets +dv; an axis with |dv| <= 1e-10
+ * is skipped. */
+void xo_apply_forces(int ni, int nj, int nk, const uint8_t* mat, double* u, double* v, double* w,
+                     double fx, double fy, double fz, double dt) {
+  grid_t g = mkgrid(ni, nj, nk);
+  double dv[3] = {fx * dt, fy * dt, fz * dt};
+  double* f[3] = {u, v, w};
+  for (int a = 0; a < 3; ++a) {
+    if (!(dv[a] > 1e-10 || dv[a] < -1e-10)) continue;
+    int si = ni + (a == 0), sj = nj + (a == 1), sk = nk + (a == 2);
+    for (int k = 0; k < sk; ++k)
+      for (int j = 0; j < sj; ++j)
+        for (int i = 0; i < si; ++i) {
+          int il = i - (a == 0), jl = j - (a == 1), kl = k - (a == 2);
+          int fr = inrange(&g, i, j, k) && mat[cidx(&g, i, j, k)] == FLUID;
+          int fl = inrange(&g, il, jl, kl) && mat[cidx(&g, il, jl, kl)] == FLUID;
+          if (fr || fl) {
+            size_t q = ((size_t)k * sj + j) * si + i;
+            f[a][q] += dv[a];
+          }
+        }
+  }
+}
+
+/* _expolateVelocity(layers, axis) (:521-650) on one face grid (si,sj,sk):
+ * marker 0 on the faces of fluid cells, -1 elsewhere; layer 1 = unmarked
+ * faces with a layer-0 neighbour; then for each layer in turn every face of it
+ * takes the average of its neighbours in the layer before (neighbour order
+ * +i,-i,+j,-j,+k,-k) and hands its unmarked neighbours to the next layer. */
+static void extrapolate_axis(const grid_t* g, const uint8_t* mat, int a, double* f, int layers) {
+  int si = g->ni + (a == 0), sj = g->nj + (a == 1), sk = g->nk + (a == 2);
+  size_t n = (size_t)si * sj * sk;
+  int* mk = malloc(n * sizeof(int));
+  size_t* cur = malloc(n * sizeof(size_t));
+  size_t* nxt = malloc(n * sizeof(size_t));
+  size_t ncur = 0, nnxt;
+  for (size_t q = 0; q < n; ++q) mk[q] = -1;
+  for (int k = 0; k < g->nk; ++k)
+    for (int j = 0; j < g->nj; ++j)
+      for (int i = 0; i < g->ni; ++i)
+        if (mat[cidx(g, i, j, k)] == FLUID) {
+          mk[((size_t)k * sj + j) * si + i] = 0;
+          mk[((size_t)(k + (a == 2)) * sj + (j + (a == 1))) * si + (i + (a == 0))] = 0;
+        }
+#define NB(i, j, k, nb, ii, jj, kk) \
+  (ii = (i) + NEI[nb].di, jj = (j) + NEI[nb].dj, kk = (k) + NEI[nb].dk, \
+   ii >= 0 && jj >= 0 && kk >= 0 && ii < si && jj < sj && kk < sk)
+  for (int k = 0; k < sk; ++k)
+    for (int j = 0; j < sj; ++j)
+      for (int i = 0; i < si; ++i) {
+        size_t q = ((size_t)k * sj + j) * si + i;
+        if (mk[q] != -1) continue;
+        for (int nb = 0; nb < 6; ++nb) {
+          int ii, jj, kk;
+          if (NB(i, j, k, nb, ii, jj, kk) && mk[((size_t)kk * sj + jj) * si + ii] == 0) {
+            cur[ncur++] = q;
+            mk[q] = 1;
+            break;
+          }
+        }
+      }
+  for (int L = 1; L <= layers; ++L) {
+    nnxt = 0;
+    for (size_t t = 0; t < ncur; ++t) {
+      size_t q = cur[t];
+      int i = (int)(q % si), j = (int)((q / si) % sj), k = (int)(q / ((size_t)si * sj));
+      double sum = 0.0;
+      int count = 0;
+      for (int nb = 0; nb < 6; ++nb) {
+        int ii, jj, kk;
+        if (NB(i, j, k, nb, ii, jj, kk) && mk[((size_t)kk * sj + jj) * si + ii] == L - 1) {
+          sum += f[((size_t)kk * sj + jj) * si + ii];
+          count += 1;
+        }
+      }
+      if (count == 0) continue;
+      f[q] = sum / (double)count;
+      for (int nb = 0; nb < 6; ++nb) {
+        int ii, jj, kk;
+        if (NB(i, j, k, nb, ii, jj, kk)) {
+          size_t p = ((size_t)kk * sj + jj) * si + ii;
+          if (mk[p] == -1) {
+            nxt[nnxt++] = p;
+            mk[p] = L + 1;
+          }
+        }
+      }
+    }
+    size_t* tmp = cur; cur = nxt; nxt = tmp;
+    ncur = nnxt;
+  }
+#undef NB
+  free(mk); free(cur); free(nxt);
+}
+
+void xo_extrapolate(int ni, int nj, int nk, const uint8_t* mat, double* u, double* v, double* w, int layers) {
+  grid_t g = mkgrid(ni, nj, nk);
+  extrapolate_axis(&g, mat, 0, u, layers);
+  extrapolate_axis(&g, mat, 1, v, layers);
+  extrapolate_axis(&g, mat, 2, w, layers);
+}

@@ -18,7 +18,8 @@ reference's divergence diagnostic after the projection.
 NormalPressureSolver (pressuresolver.cpp, the classic Poisson matrix): its
 assembly (diag, ax, ay, az, b), its PCG pressure at tol 1e-6 (iterations,
 residual) and the velocities after its applyPressure.  ``--normal-only``
-writes just those.
+writes just those (and the step fixtures); ``--steps-only`` writes only the
+``steps_<case>.npz`` fixtures (see step_fixtures).
 """
 from __future__ import annotations
 
@@ -47,6 +48,34 @@ def cases():
 
 
 NORMAL_CASES = ("dam16", "blob24x20x22")
+STEP_CASES = ("dam20x14x18",)
+FORCE, DT, LAYERS = (0.3, -9.8, 0.0), 0.01, 6
+
+
+def step_fixtures(R):
+    """``steps_<case>.npz``: FluidSimulator::_applyForces (force FORCE, dt DT)
+    and _expolateVelocity (LAYERS layers) on the scene's faces, and the whole
+    sequence forces -> projection (tol 1e-6) -> extrapolation, all run by the
+    reference's own code (oracle/sim_harness.cpp, oracle/ref_harness.cpp)."""
+    from oracle import RefSteps  # noqa: E402
+    S = RefSteps()
+    for name, sc in cases().items():
+        if name not in STEP_CASES:
+            continue
+        f = S.apply_forces(sc, FORCE, DT)
+        e = S.extrapolate(sc, LAYERS)
+        s2 = sc.copy()
+        s2.u, s2.v, s2.w = f
+        pr = R.project(s2, TOL, MAXIT)
+        assert pr["ok"], name
+        st = S.extrapolate(sc, LAYERS, uvw=(pr["u"], pr["v"], pr["w"]))
+        np.savez_compressed(
+            OUT / f"steps_{name}.npz",
+            dims=np.array([sc.ni, sc.nj, sc.nk]), mat=sc.mat, u=sc.u, v=sc.v, w=sc.w,
+            force=np.array(FORCE), dt=DT, layers=LAYERS, tol=TOL, maxit=MAXIT,
+            u_forced=f[0], v_forced=f[1], w_forced=f[2], u_extrap=e[0], v_extrap=e[1], w_extrap=e[2],
+            p_step=pr["p"], u_step=st[0], v_step=st[1], w_step=st[2])
+        print(f"steps_{name}: forces, {LAYERS}-layer extrapolation, full step")
 
 
 def normal_fixtures(R):
@@ -70,8 +99,10 @@ def main():
     if build_reference() is None:
         raise SystemExit("reference sources not found; cannot regenerate golden vectors")
     R = Reference()
-    normal_fixtures(R)
-    if "--normal-only" in sys.argv:
+    if "--steps-only" not in sys.argv:
+        normal_fixtures(R)
+    step_fixtures(R)
+    if "--normal-only" in sys.argv or "--steps-only" in sys.argv:
         return
     for name, sc in cases().items():
         A = R.assemble(sc)

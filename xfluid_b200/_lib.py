@@ -90,7 +90,8 @@ EXPORTS = [
     "xfp_project_backward_f32", "xfp_debug_stages", "xfp_rhs_inf_noalloc_f64",
     "xfp_project_batch_f32", "xfp_project_batch_f64", "xfp_advect_f64", "xfp_advect_f32",
     "xfp_advect_backward_f64", "xfp_advect_backward_f32", "xfp_box_loss_f64", "xfp_box_loss_f32",
-    "xfp_debug_expire_next_sweep",
+    "xfp_debug_expire_next_sweep", "xfp_apply_forces_f64", "xfp_apply_forces_f32", "xfp_extrapolate_f64",
+    "xfp_extrapolate_f32", "xfp_project_step_f64", "xfp_project_step_f32",
 ]
 
 
@@ -130,6 +131,12 @@ def load() -> C.CDLL:
         getattr(L, "xfp_box_loss_" + sfx).argtypes = [vp, C.c_int, C.c_int, C.c_int] + [vp] * 3 + [
             C.POINTER(C.c_double), C.POINTER(C.c_double)] + [vp] * 3
     L.xfp_debug_expire_next_sweep.argtypes = [vp]
+    d3 = C.POINTER(C.c_double)
+    for sfx in ("f64", "f32"):
+        getattr(L, "xfp_apply_forces_" + sfx).argtypes = [vp, C.c_int, C.c_int, C.c_int] + [vp] * 4 + [d3, C.c_double]
+        getattr(L, "xfp_extrapolate_" + sfx).argtypes = [vp, C.c_int, C.c_int, C.c_int] + [vp] * 4 + [C.c_int]
+        getattr(L, "xfp_project_step_" + sfx).argtypes = ([vp, C.c_int, C.c_int, C.c_int] + [vp] * 8 +
+                                                          [d3, C.c_double, C.c_int, C.POINTER(XfpStats)])
     L.xfp_rhs_inf_noalloc_f64.argtypes = [C.c_int] * 3 + [vp] * 9 + [C.c_char_p, C.c_size_t]
     for name in EXPORTS:
         f = getattr(L, name)

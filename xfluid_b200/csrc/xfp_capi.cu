@@ -466,7 +466,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     double* A[5];
     for (int q = 0; q < 5; ++q) A[q] = ctx->A64[q].as<double>();
     XFP_CUDA(ctx, (assemble<IOT, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
-                                         A[3], A[4], st, ctx->opt.matrix)));
+                                         A[3], A[4], st, ctx->opt.matrix, ctx->force)));
     if (adj_gu) XFP_CUDA(ctx, (apply_pressure_T<IOT, double>(dmat, dwu, dwv, dww, adj_gu, adj_gv, adj_gw, ni, nj,
                                                              nk, lines, A[4], st)));
     ev_record(ctx, 1);
@@ -486,7 +486,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     float* A[5];
     for (int q = 0; q < 5; ++q) A[q] = ctx->A32[q].as<float>();
     XFP_CUDA(ctx, (assemble<IOT, float>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
-                                        A[3], A[4], st, ctx->opt.matrix)));
+                                        A[3], A[4], st, ctx->opt.matrix, ctx->force)));
     if (adj_gu) XFP_CUDA(ctx, (apply_pressure_T<IOT, float>(dmat, dwu, dwv, dww, adj_gu, adj_gv, adj_gw, ni, nj,
                                                             nk, lines, A[4], st)));
     ev_record(ctx, 1);
@@ -507,7 +507,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     double* A[5];
     for (int q = 0; q < 5; ++q) A[q] = ctx->A64[q].as<double>();
     XFP_CUDA(ctx, (assemble<IOT, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
-                                         A[3], A[4], st, ctx->opt.matrix)));
+                                         A[3], A[4], st, ctx->opt.matrix, ctx->force)));
     if (adj_gu) XFP_CUDA(ctx, (apply_pressure_T<IOT, double>(dmat, dwu, dwv, dww, adj_gu, adj_gv, adj_gw, ni, nj,
                                                              nk, lines, A[4], st)));
     float* A32[4];
@@ -683,7 +683,13 @@ int project_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* 
     IOT* mv = const_cast<IOT*>(dv);
     IOT* mw = const_cast<IOT*>(dw);
     XFP_CUDA(ctx, (apply_pressure<IOT, IOT>(dmat, dwu, dwv, dww, dp, ni, nj, nk, mu, mv, mw, ctx->stream,
-                                            ctx->opt.matrix)));
+                                            ctx->opt.matrix, ctx->force)));
+    if (ctx->step_layers > 0) {
+      const size_t nm = (size_t)(ni + 1) * (nj + 1) * (nk + 1);
+      XFP_CUDA(ctx, ctx->xmarker.ensure(nm * sizeof(short)));
+      XFP_CUDA(ctx, extrapolate<IOT>(dmat, ni, nj, nk, mu, mv, mw, ctx->step_layers, ctx->xmarker.as<short>(),
+                                     ctx->stream));
+    }
   }
   ev_record(ctx, 4);
   if (!ctx->opt.device_pointers) {
@@ -902,6 +908,85 @@ int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* c
     if ((rc = dump_dense<VT>(ctx, qv, out[11]))) return rc;
   }
   return XFP_OK;
+}
+
+// ---------------------------------------------------------------- steps either side
+// The force as FluidSimulator::_applyForces forms it (FluidSimulator.cpp:431-438):
+// the summed force times dt, per axis.
+Force3 make_force(const double* force, double dt) {
+  Force3 f;
+  if (!force) return f;
+  f.on = 1;
+  for (int a = 0; a < 3; ++a) f.d[a] = force[a] * dt;
+  return f;
+}
+
+template <typename IOT>
+int forces_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* u, IOT* v, IOT* w,
+                const double* force, double dt) {
+  int rc = check_dims(ctx, ni, nj, nk, mat);
+  if (rc) return rc;
+  if (!u || !v || !w || !force) return fail(ctx, XFP_ERR_ARGS, "NULL array or force");
+  XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  const uint8_t* dmat;
+  const IOT *du_, *dv, *dw;
+  if ((rc = stage_in(ctx, ctx->io_mat, mat, ncells(ni, nj, nk), &dmat))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_u, u, nu(ni, nj, nk), &du_))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_v, v, nv(ni, nj, nk), &dv))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_w, w, nw_(ni, nj, nk), &dw))) return rc;
+  XFP_CUDA(ctx, apply_forces<IOT>(dmat, ni, nj, nk, const_cast<IOT*>(du_), const_cast<IOT*>(dv),
+                                  const_cast<IOT*>(dw), make_force(force, dt), ctx->stream));
+  if (!ctx->opt.device_pointers) {
+    XFP_CUDA(ctx, cudaMemcpyAsync(u, du_, nu(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+    XFP_CUDA(ctx, cudaMemcpyAsync(v, dv, nv(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+    XFP_CUDA(ctx, cudaMemcpyAsync(w, dw, nw_(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XFP_OK;
+}
+
+constexpr int kMaxLayers = 30000;   // the layer marker is 16-bit
+
+template <typename IOT>
+int extrapolate_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* u, IOT* v, IOT* w,
+                     int layers) {
+  int rc = check_dims(ctx, ni, nj, nk, mat);
+  if (rc) return rc;
+  if (!u || !v || !w) return fail(ctx, XFP_ERR_ARGS, "NULL array");
+  if (layers < 0 || layers > kMaxLayers) return fail(ctx, XFP_ERR_ARGS, "layers must be in [0, 30000]");
+  XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  const uint8_t* dmat;
+  const IOT *du_, *dv, *dw;
+  if ((rc = stage_in(ctx, ctx->io_mat, mat, ncells(ni, nj, nk), &dmat))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_u, u, nu(ni, nj, nk), &du_))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_v, v, nv(ni, nj, nk), &dv))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_w, w, nw_(ni, nj, nk), &dw))) return rc;
+  XFP_CUDA(ctx, ctx->xmarker.ensure((size_t)(ni + 1) * (nj + 1) * (nk + 1) * sizeof(short)));
+  XFP_CUDA(ctx, extrapolate<IOT>(dmat, ni, nj, nk, const_cast<IOT*>(du_), const_cast<IOT*>(dv),
+                                 const_cast<IOT*>(dw), layers, ctx->xmarker.as<short>(), ctx->stream));
+  if (!ctx->opt.device_pointers) {
+    XFP_CUDA(ctx, cudaMemcpyAsync(u, du_, nu(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+    XFP_CUDA(ctx, cudaMemcpyAsync(v, dv, nv(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+    XFP_CUDA(ctx, cudaMemcpyAsync(w, dw, nw_(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XFP_OK;
+}
+
+// Force fused into assembly and apply, projection, extrapolation on the
+// projected velocities, one call.
+template <typename IOT>
+int step_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* u, IOT* v, IOT* w, const IOT* wu,
+              const IOT* wv, const IOT* ww, IOT* pressure, const double* force, double dt, int layers,
+              xfp_stats* stats) {
+  if (!ctx) return XFP_ERR_ARGS;
+  if (layers < 0 || layers > kMaxLayers) return fail(ctx, XFP_ERR_ARGS, "layers must be in [0, 30000]");
+  ctx->force = make_force(force, dt);
+  ctx->step_layers = layers;
+  const int rc = project_impl<IOT>(ctx, ni, nj, nk, mat, u, v, w, wu, wv, ww, pressure, stats, true);
+  ctx->force = Force3();
+  ctx->step_layers = 0;
+  return rc;
 }
 
 }  // namespace xfp_host
@@ -1149,4 +1234,31 @@ extern "C" int xfp_debug_expire_next_sweep(xfp_ctx* ctx) {
   if (!ctx) return XFP_ERR_ARGS;
   ctx->expire_next_sweep = true;
   return XFP_OK;
+}
+
+int xfp_apply_forces_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, double* u, double* v,
+                         double* w, const double force[3], double dt) {
+  return forces_impl<double>(ctx, ni, nj, nk, material, u, v, w, force, dt);
+}
+int xfp_apply_forces_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, float* u, float* v,
+                         float* w, const double force[3], double dt) {
+  return forces_impl<float>(ctx, ni, nj, nk, material, u, v, w, force, dt);
+}
+int xfp_extrapolate_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, double* u, double* v,
+                        double* w, int layers) {
+  return extrapolate_impl<double>(ctx, ni, nj, nk, material, u, v, w, layers);
+}
+int xfp_extrapolate_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, float* u, float* v,
+                        float* w, int layers) {
+  return extrapolate_impl<float>(ctx, ni, nj, nk, material, u, v, w, layers);
+}
+int xfp_project_step_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, double* u, double* v,
+                         double* w, const double* wu, const double* wv, const double* ww, double* pressure,
+                         const double force[3], double dt, int layers, xfp_stats* stats) {
+  return step_impl<double>(ctx, ni, nj, nk, material, u, v, w, wu, wv, ww, pressure, force, dt, layers, stats);
+}
+int xfp_project_step_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, float* u, float* v,
+                         float* w, const float* wu, const float* wv, const float* ww, float* pressure,
+                         const double force[3], double dt, int layers, xfp_stats* stats) {
+  return step_impl<float>(ctx, ni, nj, nk, material, u, v, w, wu, wv, ww, pressure, force, dt, layers, stats);
 }

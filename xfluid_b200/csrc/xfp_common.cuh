@@ -34,6 +34,16 @@ struct __align__(16) Line {
   int off, lo, len, nrows;
 };
 
+// Constant body-force velocity increment (force * dt per axis), added to every
+// face that borders a fluid cell, as xFluid's FluidSimulator::_applyForces does
+// (FluidSimulator.cpp:429-499): an axis whose |dv| is not above 1e-10 is left
+// alone.  on = 0: no force.
+struct Force3 {
+  double d[3] = {0.0, 0.0, 0.0};
+  int on = 0;
+  __host__ __device__ bool axis_on(int a) const { return on && (d[a] > 1e-10 || d[a] < -1e-10); }
+};
+
 // Sweep-ordered copy ("sweep layout") of the arrays the triangular solves
 // stream.  For every active tile, compute warp (k) and group g of 4 forward
 // wavefront steps (steps 4g..4g+3) it holds a block of 32 lanes x 4 cells:
@@ -137,6 +147,8 @@ __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
 __device__ __forceinline__ double rsqrt_ref(double x) { return __ddiv_rn(1.0, __dsqrt_rn(x)); }
 __device__ __forceinline__ float rsqrt_ref(float x) { return __fdiv_rn(1.0f, __fsqrt_rn(x)); }
 

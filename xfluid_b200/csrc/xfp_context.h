@@ -68,6 +68,12 @@ struct xfp_ctx {
   // and the copies the solves stream (lx, ly, lz, inv, r, y; 8 bytes per
   // element covers every precision)
   DevBuf swt, tile_pos, sw_perm, sw_l[3], sw_inv, sw_r, sw_y;
+  // xfp_project_step_*: body force fused into assembly and apply, and the
+  // extrapolation layers run after the apply (zero outside such a call);
+  // xmarker is the extrapolation's layer-marker scratch
+  xfp::Force3 force;
+  int step_layers = 0;
+  DevBuf xmarker;
   long long Msw = 0;
   bool tracing = false;
   // sizes of the current layout

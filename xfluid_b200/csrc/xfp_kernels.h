@@ -120,7 +120,7 @@ template <typename FT, typename AT>
 cudaError_t assemble(const uint8_t* mat, const FT* u, const FT* v, const FT* w, const FT* wu,
                      const FT* wv, const FT* ww, int ni, int nj, int nk, const Line* lines,
                      AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st,
-                     int matrix = XFP_MATRIX_VARIATIONAL);
+                     int matrix = XFP_MATRIX_VARIATIONAL, Force3 frc = Force3());
 
 template <typename T>
 cudaError_t scatter_dense(const T* x, const Line* lines, int ni, int nj, int nk, T* dense,
@@ -128,7 +128,16 @@ cudaError_t scatter_dense(const T* x, const Line* lines, int ni, int nj, int nk,
 template <typename FT, typename PT>
 cudaError_t apply_pressure(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
                            const PT* p, int ni, int nj, int nk, FT* u, FT* v, FT* w,
-                           cudaStream_t st, int matrix = XFP_MATRIX_VARIATIONAL);
+                           cudaStream_t st, int matrix = XFP_MATRIX_VARIATIONAL, Force3 frc = Force3());
+// FluidSimulator::_applyForces (FluidSimulator.cpp:429-499) as one pass.
+template <typename FT>
+cudaError_t apply_forces(const uint8_t* mat, int ni, int nj, int nk, FT* u, FT* v, FT* w, Force3 frc,
+                         cudaStream_t st);
+// FluidSimulator::_expolateVelocity(layers, axis) for the three axes
+// (FluidSimulator.cpp:521-650); marker: scratch of (ni+1)*(nj+1)*(nk+1) shorts.
+template <typename FT>
+cudaError_t extrapolate(const uint8_t* mat, int ni, int nj, int nk, FT* u, FT* v, FT* w, int layers,
+                        short* marker, cudaStream_t st);
 template <typename FT, typename PT>
 cudaError_t apply_pressure_T(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
                              const FT* gu, const FT* gv, const FT* gw, int ni, int nj, int nk,

@@ -44,7 +44,7 @@ __global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __res
                                 const FT* __restrict__ ww, int ni, int nj, int nk,
                                 const Line* __restrict__ lines, AT* __restrict__ diag,
                                 AT* __restrict__ ax, AT* __restrict__ ay, AT* __restrict__ az,
-                                AT* __restrict__ b, int matrix) {
+                                AT* __restrict__ b, int matrix, Force3 frc) {
   const int lane = threadIdx.x & 31;
   const long long nlines = (long long)nj * nk;
   const size_t nn = (size_t)ni * nj;
@@ -69,15 +69,17 @@ __global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __res
           if (ii < 0 || jj < 0 || kk < 0 || ii >= ni || jj >= nj || kk >= nk) return false;
           vs = (di + dj + dk) > 0 ? AT(-1) : AT(1);
           const int fi = i + (di > 0), fj = j + (dj > 0), fk = k + (dk > 0);
+          // every face read here borders a fluid cell, so a body force applies
+          // to all of them (added in the I/O type, before the conversion)
           if (di) {
             const size_t f = uix(ni, nj, fi, fj, fk);
-            uf = (AT)u[f]; mf = wu ? (AT)wu[f] : AT(1);
+            uf = (AT)(frc.axis_on(0) ? add_rn(u[f], (FT)frc.d[0]) : u[f]); mf = wu ? (AT)wu[f] : AT(1);
           } else if (dj) {
             const size_t f = vix(ni, nj, fi, fj, fk);
-            uf = (AT)v[f]; mf = wv ? (AT)wv[f] : AT(1);
+            uf = (AT)(frc.axis_on(1) ? add_rn(v[f], (FT)frc.d[1]) : v[f]); mf = wv ? (AT)wv[f] : AT(1);
           } else {
             const size_t f = wix(ni, nj, fi, fj, fk);
-            uf = (AT)w[f]; mf = ww ? (AT)ww[f] : AT(1);
+            uf = (AT)(frc.axis_on(2) ? add_rn(w[f], (FT)frc.d[2]) : w[f]); mf = ww ? (AT)ww[f] : AT(1);
           }
           return true;
         };
@@ -158,31 +160,31 @@ __global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __res
 template <typename FT, typename AT>
 cudaError_t assemble(const uint8_t* mat, const FT* u, const FT* v, const FT* w, const FT* wu,
                      const FT* wv, const FT* ww, int ni, int nj, int nk, const Line* lines,
-                     AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st, int matrix) {
+                     AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st, int matrix, Force3 frc) {
   const long long nlines = (long long)nj * nk;
   long long blocks = (nlines + 7) / 8;
   if (blocks > 65535 * 8) blocks = 65535 * 8;
   ++g_kernel_launches;
   assemble_kernel<FT, AT><<<(unsigned)blocks, 256, 0, st>>>(mat, u, v, w, wu, wv, ww, ni, nj, nk, lines,
-                                                          diag, ax, ay, az, b, matrix);
+                                                          diag, ax, ay, az, b, matrix, frc);
   return cudaGetLastError();
 }
 template cudaError_t assemble<double, double>(const uint8_t*, const double*, const double*,
                                               const double*, const double*, const double*,
                                               const double*, int, int, int, const Line*, double*,
-                                              double*, double*, double*, double*, cudaStream_t, int);
+                                              double*, double*, double*, double*, cudaStream_t, int, Force3);
 template cudaError_t assemble<float, float>(const uint8_t*, const float*, const float*, const float*,
                                             const float*, const float*, const float*, int, int, int,
                                             const Line*, float*, float*, float*, float*, float*,
-                                            cudaStream_t, int);
+                                            cudaStream_t, int, Force3);
 template cudaError_t assemble<float, double>(const uint8_t*, const float*, const float*,
                                              const float*, const float*, const float*, const float*,
                                              int, int, int, const Line*, double*, double*, double*,
-                                             double*, double*, cudaStream_t, int);
+                                             double*, double*, cudaStream_t, int, Force3);
 template cudaError_t assemble<double, float>(const uint8_t*, const double*, const double*,
                                              const double*, const double*, const double*,
                                              const double*, int, int, int, const Line*, float*,
-                                             float*, float*, float*, float*, cudaStream_t, int);
+                                             float*, float*, float*, float*, cudaStream_t, int, Force3);
 
 // ---------------------------------------------------------------------------
 // Compact -> dense pressure grid: every cell written, 0 outside unknowns
@@ -313,46 +315,61 @@ __device__ __forceinline__ bool face_dp_normal(const uint8_t* __restrict__ mat, 
 template <typename FT, typename PT>
 __global__ void apply_kernel(const uint8_t* __restrict__ mat, const FT* __restrict__ wt,
                              const PT* __restrict__ p, int ni, int nj, int nk, int axis,
-                             FT* __restrict__ f, int matrix) {
+                             FT* __restrict__ f, int matrix, Force3 frc) {
   const int si = ni + (axis == 0), sj = nj + (axis == 1), sk = nk + (axis == 2);
   const size_t n = (size_t)si * sj * sk;
   for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(idx % si);
     const int j = (int)((idx / si) % sj);
     const int k = (int)(idx / ((size_t)si * sj));
-    if (matrix == XFP_MATRIX_NORMAL) {
-      PT dp;
-      if (face_dp_normal(mat, p, ni, nj, nk, i - (axis == 0), j - (axis == 1), k - (axis == 2), i, j, k,
-                         (PT)f[idx], dp))
-        f[idx] = sub_rn(f[idx], (FT)mul_rn(PT(1), dp));
-      continue;
+    // a body force first moves every face that borders fluid (_applyForces),
+    // then the pressure update uses the moved value
+    FT fv = f[idx];
+    bool changed = false;
+    if (frc.axis_on(axis)) {
+      const int il = i - (axis == 0), jl = j - (axis == 1), kl = k - (axis == 2);
+      const size_t nn = (size_t)ni * nj;
+      const bool fl = il >= 0 && jl >= 0 && kl >= 0 && mat[(size_t)kl * nn + (size_t)jl * ni + il] == MAT_FLUID;
+      const bool fr = i < ni && j < nj && k < nk && mat[(size_t)k * nn + (size_t)j * ni + i] == MAT_FLUID;
+      if (fl || fr) {
+        fv = add_rn(fv, (FT)frc.d[axis]);
+        changed = true;
+      }
     }
-    if (wt && wt[idx] == FT(0)) continue;
     PT dp;
-    if (face_dp(mat, p, ni, nj, nk, i - (axis == 0), j - (axis == 1), k - (axis == 2), i, j, k, dp)) {
-      f[idx] = sub_rn(f[idx], (FT)mul_rn(PT(1), dp));
+    if (matrix == XFP_MATRIX_NORMAL) {
+      if (face_dp_normal(mat, p, ni, nj, nk, i - (axis == 0), j - (axis == 1), k - (axis == 2), i, j, k,
+                         (PT)fv, dp)) {
+        fv = sub_rn(fv, (FT)mul_rn(PT(1), dp));
+        changed = true;
+      }
+    } else if (!(wt && wt[idx] == FT(0)) &&
+               face_dp(mat, p, ni, nj, nk, i - (axis == 0), j - (axis == 1), k - (axis == 2), i, j, k, dp)) {
+      fv = sub_rn(fv, (FT)mul_rn(PT(1), dp));
+      changed = true;
     }
+    if (changed) f[idx] = fv;
   }
 }
 template <typename FT, typename PT>
 cudaError_t apply_pressure(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
                            const PT* p, int ni, int nj, int nk, FT* u, FT* v, FT* w,
-                           cudaStream_t st, int matrix) {
+                           cudaStream_t st, int matrix, Force3 frc) {
   for (int axis = 0; axis < 3; ++axis) {
     size_t n = (size_t)(ni + (axis == 0)) * (nj + (axis == 1)) * (nk + (axis == 2));
     unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32);
     ++g_kernel_launches;
     apply_kernel<FT, PT><<<blocks, 256, 0, st>>>(mat, axis == 0 ? wu : axis == 1 ? wv : ww, p, ni, nj, nk,
-                                                axis, axis == 0 ? u : axis == 1 ? v : w, matrix);
+                                                axis, axis == 0 ? u : axis == 1 ? v : w, matrix, frc);
   }
   return cudaGetLastError();
 }
 template cudaError_t apply_pressure<double, double>(const uint8_t*, const double*, const double*,
                                                     const double*, const double*, int, int, int,
-                                                    double*, double*, double*, cudaStream_t, int);
+                                                    double*, double*, double*, cudaStream_t, int, Force3);
 template cudaError_t apply_pressure<float, float>(const uint8_t*, const float*, const float*,
                                                   const float*, const float*, int, int, int, float*,
-                                                  float*, float*, cudaStream_t, int);
+                                                  float*, float*, cudaStream_t, int, Force3);
 
 // ---------------------------------------------------------------------------
 // Adjoint of the pressure update: q = G^T g, where applyPressure computes

@@ -146,6 +146,44 @@ class VariationalPressureSolver:
         self.stats = st.as_dict()
         return rc == _lib.XFP_OK
 
+    # ---- the simulator steps either side of the projection (FluidSimulator.cpp) ----
+    def applyForces(self, force, dt: float) -> None:
+        """FluidSimulator::_applyForces (:429-499) on the borrowed velocities:
+        force (the summed constant force, 3 values) * dt on every face that
+        borders fluid."""
+        ni, nj, nk = self._size
+        arrs = [self._mat, self._u, self._v, self._w]
+        self._prep(arrs)
+        f3 = (C.c_double * 3)(*[float(x) for x in force])
+        fn = self._ctx.lib.xfp_apply_forces_f64 if _dtype_name(self._u) == "f64" else self._ctx.lib.xfp_apply_forces_f32
+        self._ctx.check(fn(self._ctx.ptr, ni, nj, nk, *map(_ptr, arrs), f3, float(dt)))
+
+    def extrapolateVelocity(self, layers: int) -> None:
+        """FluidSimulator::_expolateVelocity (:511-650) on the borrowed
+        velocities; the reference uses layers = int(CFL number + 5)."""
+        ni, nj, nk = self._size
+        arrs = [self._mat, self._u, self._v, self._w]
+        self._prep(arrs)
+        fn = self._ctx.lib.xfp_extrapolate_f64 if _dtype_name(self._u) == "f64" else self._ctx.lib.xfp_extrapolate_f32
+        self._ctx.check(fn(self._ctx.ptr, ni, nj, nk, *map(_ptr, arrs), int(layers)))
+
+    def projectStep(self, pressure, force, dt: float, layers: int) -> bool:
+        """applyForces, solve, applyPressure and extrapolateVelocity in one
+        call, the force fused into the assembly and apply kernels; True when
+        the solve converged."""
+        ni, nj, nk = self._size
+        wu, wv, ww = self._weights
+        arrs = [self._mat, self._u, self._v, self._w, wu, wv, ww, pressure]
+        self._prep(arrs)
+        st = XfpStats()
+        f3 = (C.c_double * 3)(*[float(x) for x in force])
+        fn = (self._ctx.lib.xfp_project_step_f64 if _dtype_name(self._u) == "f64"
+              else self._ctx.lib.xfp_project_step_f32)
+        rc = self._ctx.check(fn(self._ctx.ptr, ni, nj, nk, *map(_ptr, arrs), f3, float(dt), int(layers),
+                                C.byref(st)))
+        self.stats = st.as_dict()
+        return rc == _lib.XFP_OK
+
     def applyPressure(self, pressure) -> bool:
         """u,v,w -= grad p on every face that touches fluid."""
         ni, nj, nk = self._size
