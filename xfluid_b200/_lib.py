@@ -147,9 +147,11 @@ def load() -> C.CDLL:
 
 
 def torch_stream(device: int) -> C.c_void_p:
-    """Handle of torch's current CUDA stream on `device`.  A context that is
-    given CUDA tensors runs on it, so the library reads them only after the
-    torch work that produced them and torch sees the results in order."""
+    """Handle of torch's current CUDA stream on `device`.  For a created
+    stream a context given it runs in order with torch's work there.  Torch's
+    default stream has the handle NULL, which the library reads as "no stream
+    given" (the context then makes its own, unordered with torch): callers
+    still wait with sync_torch before the library reads torch's tensors."""
     import torch
     return C.c_void_p(torch.cuda.current_stream(device).cuda_stream)
 

@@ -183,6 +183,41 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
   ctx->M = B->M;
   ctx->ntiles = nt;
   ctx->nlines_all = nlines;
+  // Sweep layout over the merged tile list: spans on the device, offsets
+  // scanned here, the (scene, K, J) -> tile map filled here, then the cell ->
+  // element map scene by scene.
+  ctx->Msw = 0;
+  if (nt > 0) {
+    XFP_CUDA(ctx, ctx->swt.ensure(nt * sizeof(SwTile)));
+    XFP_CUDA(ctx, sw_tiles_build_batch(B->tiles.as<int>(), B->tile_scene.as<int>(), B->segs.as<BatchSeg>(), nt, nw,
+                                       ctx->swt.as<SwTile>(), st));
+    std::vector<SwTile> sw(nt);
+    XFP_CUDA(ctx, cudaMemcpyAsync(sw.data(), ctx->swt.p, nt * sizeof(SwTile), cudaMemcpyDeviceToHost, st));
+    XFP_CUDA(ctx, cudaStreamSynchronize(st));
+    long long off = 0;
+    for (auto& e : sw) {
+      e.off = off;
+      off += (long long)nw * e.ng * 128;
+    }
+    if (off >= (1LL << 31)) return fail(ctx, XFP_ERR_ARGS, "batch too large for the sweep layout");
+    ctx->Msw = off;
+    std::vector<int> tpos(std::max<long long>(ntile_slots, 1), -1);
+    for (int t = 0; t < nt; ++t) {
+      const int sc = tscene[t], J = tiles[t] & 0xffff, K = tiles[t] >> 16;
+      tpos[tile_base[sc] + (long long)K * ((S[sc].nj + 31) / 32) + J] = t;
+    }
+    XFP_CUDA(ctx, ctx->tile_pos.ensure(tpos.size() * sizeof(int)));
+    XFP_CUDA(ctx, cudaMemcpyAsync(ctx->swt.p, sw.data(), nt * sizeof(SwTile), cudaMemcpyHostToDevice, st));
+    XFP_CUDA(ctx, cudaMemcpyAsync(ctx->tile_pos.p, tpos.data(), tpos.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                  st));
+    XFP_CUDA(ctx, ctx->sw_perm.ensure((size_t)(std::max<long long>(B->M, 4) + 8) * sizeof(int)));
+    for (int sc = 0; sc < n; ++sc)
+      XFP_CUDA(ctx, sw_perm_build(ctx->cell_line.as<int>() + base[sc], lines + B->line_base[sc], S[sc].nj, nw,
+                                  (S[sc].nj + 31) / 32, ctx->tile_pos.as<int>() + tile_base[sc],
+                                  ctx->swt.as<SwTile>(), base[sc + 1] - base[sc], ctx->sw_perm.as<int>() + base[sc],
+                                  st, base[sc]));
+    XFP_CUDA(ctx, cudaStreamSynchronize(st));
+  }
   return XFP_OK;
 }
 
@@ -245,6 +280,7 @@ int batch_pcg(xfp_ctx* ctx, BatchState* B, const VT* const A[4], const VT* b, VT
   const int n = B->n;
   const size_t M = (size_t)std::max<long long>(B->M, 1);
   const BatchSeg* segs = B->segs.as<BatchSeg>();
+  int rc0;
   if (tol < 1e-30) tol = 1e-30;
   XFP_CUDA(ctx, cudaMemsetAsync(x, 0, M * sizeof(VT), st));
   XFP_CUDA(ctx, cudaMemsetAsync(dsc, 0, n * sizeof(PcgScalars), st));
@@ -255,24 +291,35 @@ int batch_pcg(xfp_ctx* ctx, BatchState* B, const VT* const A[4], const VT* b, VT
   d.partials = ctx->tpartials.as<double>();
   d.sy = ctx->sy.as<unsigned long long>();
   d.sz = ctx->sz.as<unsigned long long>();
-  const SweepGrid g = batch_grid(ctx, B, dsc);
+  SweepGrid g = batch_grid(ctx, B, dsc);
+  // the solves stream the sweep layout (as single scenes do): factor and r
+  // copied in, z gathered back through perm
+  if ((rc0 = sweep_copies<VT, IT, DT>(ctx, L, inv, r, &g, 1, &d)) != XFP_OK) return rc0;
+  const bool swl = B->ntiles > 0;
+  VT* rsw = swl ? ctx->sw_r.as<VT>() : nullptr;
+  const VT* zsw = swl ? ctx->sw_y.as<VT>() : nullptr;
+  const int* perm = swl ? ctx->sw_perm.as<int>() : nullptr;
   const double* lpart = ctx->tpartials.as<double>();
   // lines of inactive tiles are never written: their partials stay zero
   XFP_CUDA(ctx, cudaMemsetAsync(ctx->tpartials.p, 0, std::max<long long>(ctx->nlines_all, 1) * sizeof(double), st));
   XFP_CUDA(ctx, (batch_sweep<VT, IT, DT>(ctx, B, SWEEP_FWD, g, d)));
   XFP_CUDA(ctx, (batch_sweep<VT, IT, DT>(ctx, B, SWEEP_BWD, g, d)));
   XFP_CUDA(ctx, batch_bwd_reduce<DT>(segs, n, lpart, dsc, 0, st));
-  XFP_CUDA(ctx, copy_vec<VT>(z, s, (long long)M, st));
+  if (swl) {
+    if ((rc0 = sweep_result<VT>(ctx, s)) != XFP_OK) return rc0;
+  } else {
+    XFP_CUDA(ctx, copy_vec<VT>(z, s, (long long)M, st));
+  }
   auto iteration = [&]() -> cudaError_t {
     cudaError_t e;
     if ((e = batch_spmv_dot<VT, VT, DT>(segs, n, B->blocks_cells, A[0], A[1], A[2], A[3], s, z,
                                         ctx->cell_line.as<int>(), dsc, 0, st)))
       return e;
-    if ((e = batch_update_xr<VT>(segs, n, B->blocks_cells, x, r, s, z, dsc, st))) return e;
+    if ((e = batch_update_xr<VT>(segs, n, B->blocks_cells, x, r, s, z, dsc, st, rsw, perm))) return e;
     if ((e = batch_sweep<VT, IT, DT>(ctx, B, SWEEP_FWD, g, d))) return e;
     if ((e = batch_sweep<VT, IT, DT>(ctx, B, SWEEP_BWD, g, d))) return e;
     if ((e = batch_bwd_reduce<DT>(segs, n, lpart, dsc, 1, st))) return e;
-    return batch_update_s<VT>(segs, n, B->blocks_cells, s, z, dsc, st);
+    return batch_update_s<VT>(segs, n, B->blocks_cells, s, z, dsc, st, zsw, perm);
   };
   const int K = ctx->opt.check_every > 0 ? ctx->opt.check_every : 8;
   const int per_iter = B->ntiles > 0 ? 6 : 4;
@@ -505,7 +552,9 @@ int time_sweeps(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<IOT>>& S
   d.partials = ctx->tpartials.as<double>();
   d.sy = ctx->sy.as<unsigned long long>();
   d.sz = ctx->sz.as<unsigned long long>();
-  const SweepGrid g = batch_grid(ctx, B, B->scal.as<PcgScalars>());
+  SweepGrid g = batch_grid(ctx, B, B->scal.as<PcgScalars>());
+  const float* Lf[3] = {F[0], F[1], F[2]};
+  if ((rc = sweep_copies<float, float, float>(ctx, Lf, d.inv, d.r, &g, 1, &d))) return rc;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);

@@ -131,4 +131,45 @@ int check_dims(xfp_ctx* ctx, int ni, int nj, int nk, const void* mat);
 int ensure_compact(xfp_ctx* ctx, int prec);
 int check_sweep_error(xfp_ctx* ctx);
 
+
+// Sweep-layout copies of the factor (after it is final in the solve type)
+// and of r; element slots of lanes without a cell stay zero.
+template <typename VT, typename IT, typename CT>
+int sweep_copies(xfp_ctx* ctx, const VT* const L[3], const IT* inv, const VT* r, xfp::SweepGrid* gs, int ng,
+                 xfp::SweepData<VT, IT, CT>* d) {
+  if (ctx->ntiles == 0) return XFP_OK;
+  const size_t bytes = (size_t)(ctx->Msw + 8) * 8;
+  for (auto& b : ctx->sw_l) XFP_CUDA(ctx, b.ensure(bytes));
+  XFP_CUDA(ctx, ctx->sw_inv.ensure(bytes));
+  XFP_CUDA(ctx, ctx->sw_r.ensure(bytes));
+  XFP_CUDA(ctx, ctx->sw_y.ensure(bytes));
+  cudaStream_t st = ctx->stream;
+  const int* perm = ctx->sw_perm.as<int>();
+  for (int q = 0; q < 3; ++q) {
+    XFP_CUDA(ctx, cudaMemsetAsync(ctx->sw_l[q].p, 0, (size_t)ctx->Msw * sizeof(VT), st));
+    XFP_CUDA(ctx, xfp::sw_permute<VT>(const_cast<VT*>(L[q]), ctx->sw_l[q].as<VT>(), perm, ctx->M, 0, st));
+  }
+  XFP_CUDA(ctx, cudaMemsetAsync(ctx->sw_inv.p, 0, (size_t)ctx->Msw * sizeof(IT), st));
+  XFP_CUDA(ctx, xfp::sw_permute<IT>(const_cast<IT*>(inv), ctx->sw_inv.as<IT>(), perm, ctx->M, 0, st));
+  XFP_CUDA(ctx, cudaMemsetAsync(ctx->sw_r.p, 0, (size_t)ctx->Msw * sizeof(VT), st));
+  XFP_CUDA(ctx, xfp::sw_permute<VT>(const_cast<VT*>(r), ctx->sw_r.as<VT>(), perm, ctx->M, 0, st));
+  d->lxs = ctx->sw_l[0].as<VT>();
+  d->lys = ctx->sw_l[1].as<VT>();
+  d->lzs = ctx->sw_l[2].as<VT>();
+  d->invs = ctx->sw_inv.as<IT>();
+  d->rs = ctx->sw_r.as<VT>();
+  d->ys = ctx->sw_y.as<VT>();
+  for (int q = 0; q < ng; ++q) gs[q].swt = ctx->swt.as<xfp::SwTile>();
+  return XFP_OK;
+}
+
+// Line-layout copy of the sweep-ordered solve result (z, or y after a
+// forward solve alone).
+template <typename VT>
+int sweep_result(xfp_ctx* ctx, VT* out) {
+  if (ctx->ntiles == 0) return XFP_OK;
+  XFP_CUDA(ctx, xfp::sw_permute<VT>(out, ctx->sw_y.as<VT>(), ctx->sw_perm.as<int>(), ctx->M, 1, ctx->stream));
+  return XFP_OK;
+}
+
 }  // namespace xfp_host

@@ -95,9 +95,13 @@ XFP_SWEEP_DECL(float, double, double)
 // and the (K*NJt + J) -> tile position map.
 cudaError_t sw_tiles_build(const Line* lines, const int* tiles, int ntiles, int nj, int nk, int nw, int NJt,
                            SwTile* swt, int* tile_pos, cudaStream_t st);
-// perm[c] = sweep-layout element of stored cell c (c < M).
+// perm[c] = sweep-layout element of stored cell cell_base + c (c < M); the
+// line offsets count from cell 0 of the compact arrays.
 cudaError_t sw_perm_build(const int* cell_line, const Line* lines, int nj, int nw, int NJt, const int* tile_pos,
-                          const SwTile* swt, long long M, int* perm, cudaStream_t st);
+                          const SwTile* swt, long long M, int* perm, cudaStream_t st, long long cell_base = 0);
+// Batch form of sw_tiles_build: spans of the merged tile list (tile t in scene tile_scene[t]).
+cudaError_t sw_tiles_build_batch(const int* tiles, const int* tile_scene, const BatchSeg* segs, int ntiles, int nw,
+                                 SwTile* swt, cudaStream_t st);
 // dir 0: sw[perm[c]] = line[c]; dir 1: line[c] = sw[perm[c]] for the M stored cells.
 template <typename T>
 cudaError_t sw_permute(T* line, T* sw, const int* perm, long long M, int dir, cudaStream_t st);
@@ -182,12 +186,14 @@ template <typename VT, typename AT, typename DT>
 cudaError_t batch_spmv_dot(const BatchSeg* segs, int nseg, int blocks, const AT* diag, const AT* ax,
                            const AT* ay, const AT* az, const VT* s, VT* z, const int* cell_line, PcgScalars* sc,
                            int mode, cudaStream_t st);
+// rsw/perm, zsw/perm (optional): as update_xr / update_s, perm indexed by global cell
 template <typename VT>
 cudaError_t batch_update_xr(const BatchSeg* segs, int nseg, int blocks, VT* x, VT* r, const VT* s,
-                            const VT* z, PcgScalars* sc, cudaStream_t st);
+                            const VT* z, PcgScalars* sc, cudaStream_t st, VT* rsw = nullptr,
+                            const int* perm = nullptr);
 template <typename VT>
 cudaError_t batch_update_s(const BatchSeg* segs, int nseg, int blocks, VT* s, const VT* z, PcgScalars* sc,
-                           cudaStream_t st);
+                           cudaStream_t st, const VT* zsw = nullptr, const int* perm = nullptr);
 // tols/maxits: optional per-scene tolerance and iteration cap (else tol, maxit)
 template <typename VT>
 cudaError_t batch_absmax_init(const BatchSeg* segs, int nseg, int blocks, const VT* b, PcgScalars* sc,

@@ -757,11 +757,12 @@ template <typename VT>
 __global__ void __launch_bounds__(256) batch_update_xr_kernel(const BatchSeg* __restrict__ segs, int nseg,
                                                               VT* __restrict__ x, VT* __restrict__ r,
                                                               const VT* __restrict__ s, const VT* __restrict__ z,
-                                                              PcgScalars* sc) {
+                                                              PcgScalars* sc, VT* __restrict__ rsw,
+                                                              const int* __restrict__ perm) {
   const int q = batch_scene_of(segs, nseg, false);
   const BatchSeg& S = segs[q];
   update_xr_body<VT>(blockIdx.x - S.blk_cells_start, S.blk_cells, x + S.base, r + S.base, s + S.base,
-                     z + S.base, S.M, sc + q, S.partials);
+                     z + S.base, S.M, sc + q, S.partials, rsw, perm ? perm + S.base : nullptr);
 }
 template <typename VT, typename DT>
 cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgScalars* sc,
@@ -797,10 +798,12 @@ __global__ void update_s_kernel(VT* __restrict__ s, const VT* __restrict__ z, lo
 }
 template <typename VT>
 __global__ void batch_update_s_kernel(const BatchSeg* __restrict__ segs, int nseg, VT* __restrict__ s,
-                                      const VT* __restrict__ z, PcgScalars* sc) {
+                                      const VT* __restrict__ z, PcgScalars* sc, const VT* __restrict__ zsw,
+                                      const int* __restrict__ perm) {
   const int q = batch_scene_of(segs, nseg, false);
   const BatchSeg& S = segs[q];
-  update_s_body<VT>(blockIdx.x - S.blk_cells_start, S.blk_cells, s + S.base, z + S.base, S.M, sc + q);
+  update_s_body<VT>(blockIdx.x - S.blk_cells_start, S.blk_cells, s + S.base, z + S.base, S.M, sc + q, zsw,
+                    perm ? perm + S.base : nullptr);
 }
 template <typename VT>
 cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st, const VT* zsw,
@@ -1023,27 +1026,27 @@ cudaError_t build_cell_line(const Line* lines, long long nlines, int* cell_line,
 
 template <typename VT>
 cudaError_t batch_update_xr(const BatchSeg* segs, int nseg, int blocks, VT* x, VT* r, const VT* s,
-                            const VT* z, PcgScalars* sc, cudaStream_t st) {
+                            const VT* z, PcgScalars* sc, cudaStream_t st, VT* rsw, const int* perm) {
   ++g_kernel_launches;
-  batch_update_xr_kernel<VT><<<blocks, 256, 0, st>>>(segs, nseg, x, r, s, z, sc);
+  batch_update_xr_kernel<VT><<<blocks, 256, 0, st>>>(segs, nseg, x, r, s, z, sc, rsw, perm);
   return cudaGetLastError();
 }
 template cudaError_t batch_update_xr<double>(const BatchSeg*, int, int, double*, double*, const double*,
-                                             const double*, PcgScalars*, cudaStream_t);
+                                             const double*, PcgScalars*, cudaStream_t, double*, const int*);
 template cudaError_t batch_update_xr<float>(const BatchSeg*, int, int, float*, float*, const float*,
-                                            const float*, PcgScalars*, cudaStream_t);
+                                            const float*, PcgScalars*, cudaStream_t, float*, const int*);
 
 template <typename VT>
 cudaError_t batch_update_s(const BatchSeg* segs, int nseg, int blocks, VT* s, const VT* z, PcgScalars* sc,
-                           cudaStream_t st) {
+                           cudaStream_t st, const VT* zsw, const int* perm) {
   ++g_kernel_launches;
-  batch_update_s_kernel<VT><<<blocks, 256, 0, st>>>(segs, nseg, s, z, sc);
+  batch_update_s_kernel<VT><<<blocks, 256, 0, st>>>(segs, nseg, s, z, sc, zsw, perm);
   return cudaGetLastError();
 }
 template cudaError_t batch_update_s<double>(const BatchSeg*, int, int, double*, const double*, PcgScalars*,
-                                            cudaStream_t);
+                                            cudaStream_t, const double*, const int*);
 template cudaError_t batch_update_s<float>(const BatchSeg*, int, int, float*, const float*, PcgScalars*,
-                                           cudaStream_t);
+                                           cudaStream_t, const float*, const int*);
 
 template <typename VT>
 cudaError_t batch_absmax_init(const BatchSeg* segs, int nseg, int blocks, const VT* b, PcgScalars* sc,

@@ -32,9 +32,14 @@ class Rollout:
         o = _lib.default_options()
         o.precision = _lib.PREC[precision]
         o.tol, o.max_iter, o.device, o.device_pointers = tol, max_iter, device, 1
-        # torch produces and consumes every tensor this class passes: order the
-        # library's kernels on torch's stream
+        # torch produces and consumes every tensor this class passes.  The
+        # library runs on torch's current stream when that is a created stream;
+        # torch's default stream has the handle NULL, which gives the context a
+        # stream of its own that is not ordered after torch's work, so every
+        # library call below first waits for torch's stream (_wait_torch).  Each
+        # call returns only after its own kernels are done.
         o.stream = _lib.torch_stream(device)
+        self.device = device
         self._ctx = Context(o)
         self.mat = mat
         self.nk, self.nj, self.ni = mat.shape
@@ -56,10 +61,15 @@ class Rollout:
     def _P(x):
         return None if x is None else C.c_void_p(x.data_ptr())
 
+    def _wait_torch(self):
+        _lib.sync_torch(self.device)
+
     def step(self, u, v, w):
         """advect then project; returns new tensors."""
         P = self._P
         ou, ov, ow = (a.clone() for a in (u, v, w))
+        # the clones (torch) must land before the advection overwrites them
+        self._wait_torch()
         self._ctx.check(self._fn("xfp_advect", u)(self._ctx.ptr, self.ni, self.nj, self.nk, P(u), P(v), P(w),
                                                   P(ou), P(ov), P(ow), self.c))
         st = XfpStats()
@@ -75,6 +85,7 @@ class Rollout:
         P = self._P
         u, v, w = state
         pu, pv, pw = (torch_empty_like(a) for a in g)
+        self._wait_torch()
         st = XfpStats()
         rc = self._fn("xfp_project_backward", u)(self._ctx.ptr, self.ni, self.nj, self.nk, P(self.mat),
                                                  *map(P, self.weights), P(g[0]), P(g[1]), P(g[2]), P(pu), P(pv),
@@ -91,6 +102,7 @@ class Rollout:
         P = self._P
         out = C.c_double(0.0)
         g = tuple(torch_empty_like(a) for a in (u, v, w)) if grad else (None, None, None)
+        self._wait_torch()
         self._ctx.check(self._fn("xfp_box_loss", u)(self._ctx.ptr, self.ni, self.nj, self.nk, P(u), P(v), P(w),
                                                     self.box, C.byref(out), *map(P, g)))
         return (out.value, g) if grad else out.value
