@@ -216,8 +216,12 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
         gi = min(max(gi, T.g0), T.g0 + T.ng - 1);
         return wbase + (long long)(gi - T.g0) * 128;
       };
+      // A lane whose group lies outside its line loads nothing: every use of
+      // such a group's values is masked by `in`, so the buffer may keep an
+      // older group's values (masked lanes fetch no sectors).
       auto load_grp = [&](Grp& G, int c4, long long si) {
-        const int cc = c4 >= 0 ? c4 : 0;
+        if (c4 < 0) return;
+        const int cc = c4;
         if constexpr (OP == SWEEP_FWD) {
           if (swl) ldg(G.r, d.rs + si);
           else ldg(G.r, d.r + cc);
@@ -328,17 +332,16 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           if (tau >= tileLo && tau <= tileHi) yb[e] = step(tau, G, e, in, cc + e);
         }
         // with a sweep layout y (forward) and z (backward, in place) go to
-        // the sweep-ordered copy, the whole block (zeros where a lane has no
-        // cell); otherwise to the line layout
-        if (swl) stg(d.ys + si, yb);
-        else if (in) stg(d.y + c4, yb);
+        // the sweep-ordered copy, otherwise to the line layout; lanes without
+        // a cell in this group store nothing (no solve reads those slots)
+        if (in) stg(swl ? d.ys + si : d.y + c4, yb);
       };
       // Groups are loaded into registers one group ahead (two buffers), or two
       // groups ahead (three buffers) where the register budget allows: the
       // height-8 tile has 10 warps, i.e. about 170 registers per thread (FP32
       // values; FP64 groups are twice the size and stay double-buffered).
       if constexpr (NW <= 8 && sizeof(VT) == 4) {
-        Grp GA, GB, GC;
+        Grp GA{}, GB{}, GC{};
         int cA = group_c4(base0), cB = group_c4(base0 + GS);
         long long sA = sw_at(base0), sB = sw_at(base0 + GS);
         load_grp(GA, cA, sA);
@@ -360,7 +363,7 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           run_group(gb + 2 * GS, GC, cC, sC);
         }
       } else {
-      Grp GA, GB;
+      Grp GA{}, GB{};
       int cA = group_c4(base0);
       long long sA = sw_at(base0);
       load_grp(GA, cA, sA);
