@@ -257,6 +257,55 @@ int xfp_project_step_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* ma
                          float* w, const float* wu, const float* wv, const float* ww, float* pressure,
                          const double force[3], double dt, int layers, xfp_stats* stats);
 
+/* ---- Particle steps (FLIP/PIC) around the projection ----
+ * One particle is xFluid's struct Particle {Vec3d p; Vec3d v;} (particle.h:5-15):
+ * position then velocity, six doubles, so a std::vector<Particle>'s data()
+ * is passed as it is.  Positions are in the simulator's units (cell width dx,
+ * grid origin 0).  Grids, material and pointers follow the projection's rules
+ * (host arrays, or device arrays with options.device_pointers).  All FP64.
+ *
+ * xfp_advect_particles_f64 replaces FluidSimulator::_advectParticles steps
+ *   a-b (FluidSimulator.cpp:652-723): each particle's velocity becomes
+ *   (1-ratio) PIC + ratio FLIP from the current faces (u,v,w) and those saved
+ *   before the forces (_saveVelocity, :1095-1100); the particle moves by RK4
+ *   through (u,v,w) over dt (:895-906), and a particle that would enter a solid
+ *   cell is resolved as the reference does (collision.cpp:293-440).  As in the
+ *   reference, whose six worker chunks of n/6 skip the remainder, the last
+ *   n mod 6 particles are left unchanged.  Bit-identical to the reference,
+ *   except where it reads outside its arrays: a collision point in a cell
+ *   outside the grid leaves the particle in place.
+ * xfp_particles_to_grid_f64 replaces _updateVelocityByParticles (:909-1085):
+ *   every face of u,v,w becomes the kernel-weighted mean of the particles'
+ *   velocity component (radius 1.5 dx), or 0 where the weight is <= 1e-7.
+ *   The same contributions as the reference, summed in a fixed order other
+ *   than its particle order: equal to FP64 rounding.
+ * xfp_update_material replaces _updateMaterial (:402-427): non-solid cells
+ *   become air, then every cell holding a particle becomes fluid.  Bit-identical.
+ * xfp_distance_field_f64 replaces DirectedDistanceField::updateFeild
+ *   (directeddistancefield.cpp:122-165): phi on the (ni*subdiv+1) x
+ *   (nj*subdiv+1) x (nk*subdiv+1) vertex grid (may be NULL when only the
+ *   material is wanted), and, when material is given, the material part of
+ *   updateSurfaceInfo (:167-215): non-solid cells classified fluid or air by
+ *   phi >= threshold.  phi equals the reference's to FP64 rounding (summation
+ *   order); the classification follows phi exactly.  FluidSimulator uses
+ *   subdiv 2, radius 3x its particle radius, threshold 0.4 (:207-213). */
+typedef struct {
+  double p[3];
+  double v[3];
+} xfp_particle;
+
+int xfp_advect_particles_f64(xfp_ctx* ctx, int ni, int nj, int nk, double dx, const uint8_t* material,
+                             const double* u, const double* v, const double* w, const double* u_saved,
+                             const double* v_saved, const double* w_saved, double ratio_flip, double dt,
+                             long long n, xfp_particle* particles);
+int xfp_particles_to_grid_f64(xfp_ctx* ctx, int ni, int nj, int nk, double dx, long long n,
+                              const xfp_particle* particles, double* u, double* v, double* w);
+int xfp_update_material(xfp_ctx* ctx, int ni, int nj, int nk, double dx, long long n,
+                        const xfp_particle* particles, uint8_t* material);
+int xfp_distance_field_f64(xfp_ctx* ctx, int ni, int nj, int nk, double dx, int subdiv, double radius,
+                           double threshold, long long n, const xfp_particle* particles, double* phi,
+                           uint8_t* material);
+
 /* Diagnostics: runs the internal stages on one scene and returns them on the
  * dense grid (ni*nj*nk doubles each; any output may be NULL), in the
  * context's precision.  Exposes, for verification against the reference:

@@ -14,6 +14,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ORACLE_SRC = HERE / "xfp_oracle.c"
+ORACLE_SRCS = [ORACLE_SRC, HERE / "xfp_particles_oracle.c"]
 ORACLE_LIB = HERE / "_build" / "libxfp_oracle.so"
 REF_LIB = HERE / "_ref" / "libxfref.so"
 SIM_LIB = HERE / "_ref" / "libxfsim.so"
@@ -22,14 +23,20 @@ _dp = C.POINTER(C.c_double)
 _u8 = C.POINTER(C.c_uint8)
 
 
+def _parts(a) -> np.ndarray:
+    """Particles as xFluid's struct Particle {Vec3d p; Vec3d v;}: (n, 6) FP64."""
+    return np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1, 6))
+
+
 def build_oracle(force: bool = False) -> Path:
     """Compile the C restatement (gcc, -O2, no FP contraction)."""
-    if ORACLE_LIB.exists() and not force and ORACLE_LIB.stat().st_mtime >= ORACLE_SRC.stat().st_mtime:
+    if ORACLE_LIB.exists() and not force and \
+            ORACLE_LIB.stat().st_mtime >= max(f.stat().st_mtime for f in ORACLE_SRCS):
         return ORACLE_LIB
     ORACLE_LIB.parent.mkdir(parents=True, exist_ok=True)
     tmp = ORACLE_LIB.with_suffix(".so.tmp")
     subprocess.check_call(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off",
-                           "-fno-fast-math", str(ORACLE_SRC), "-lm", "-o", str(tmp)])
+                           "-fno-fast-math", *map(str, ORACLE_SRCS), "-lm", "-o", str(tmp)])
     os.replace(tmp, ORACLE_LIB)
     return ORACLE_LIB
 
@@ -106,6 +113,12 @@ class Oracle(_Lib):
                                         C.POINTER(C.c_int), _dp])
         L.xo_project_normal.restype = C.c_int
         L.xo_apply_forces.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_double] * 4
+        L.xo_advect_particles.argtypes = ([C.c_int] * 3 + [C.c_double, _u8] + [_dp] * 6 +
+                                          [C.c_double, C.c_double, C.c_longlong, _dp, C.POINTER(C.c_int)])
+        L.xo_p2g.argtypes = [C.c_int] * 3 + [C.c_double, C.c_longlong] + [_dp] * 4
+        L.xo_update_material.argtypes = [C.c_int] * 3 + [C.c_double, C.c_longlong, _dp, _u8]
+        L.xo_distance_field.argtypes = ([C.c_int] * 3 + [C.c_double, C.c_int, C.c_double, C.c_double,
+                                        C.c_longlong, _dp, _dp, _u8])
         L.xo_extrapolate.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_int]
 
     @staticmethod
@@ -207,6 +220,42 @@ class Oracle(_Lib):
         u, v, w = (np.array(a, dtype=np.float64) for a in (uvw or (sc.u, sc.v, sc.w)))
         self.lib.xo_extrapolate(*self._dims(sc), _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w), int(layers))
         return u, v, w
+
+    # ---- particle steps (oracle/xfp_particles_oracle.c) ----
+    def advect_particles(self, sc, saved, parts, ratio, dt, dx, status=False):
+        """_advectParticles steps a, b on the faces of sc (current) and `saved`;
+        with status=True also the per-particle outcome (xo_advect_particles)."""
+        out = _parts(parts).copy()
+        g = [_f64(a) for a in (sc.u, sc.v, sc.w, *saved)]
+        st = np.zeros(len(out), np.int32)
+        self.lib.xo_advect_particles(*self._dims(sc), float(dx), _p(np.ascontiguousarray(sc.mat, np.uint8)),
+                                     *map(_p, g), float(ratio), float(dt), len(out), _p(out),
+                                     st.ctypes.data_as(C.POINTER(C.c_int)))
+        return (out, st) if status else out
+
+    def p2g(self, dims, dx, parts):
+        ni, nj, nk = dims
+        P = _parts(parts)
+        u, v, w = np.zeros((nk, nj, ni + 1)), np.zeros((nk, nj + 1, ni)), np.zeros((nk + 1, nj, ni))
+        self.lib.xo_p2g(ni, nj, nk, float(dx), len(P), _p(P), _p(u), _p(v), _p(w))
+        return u, v, w
+
+    def update_material(self, mat, dx, parts):
+        nk, nj, ni = mat.shape
+        P = _parts(parts)
+        m = np.array(mat, np.uint8)
+        self.lib.xo_update_material(ni, nj, nk, float(dx), len(P), _p(P), _p(m))
+        return m
+
+    def distance_field(self, mat, dx, subdiv, radius, threshold, parts):
+        nk, nj, ni = mat.shape
+        P = _parts(parts)
+        s = int(subdiv)
+        phi = np.zeros((nk * s + 1, nj * s + 1, ni * s + 1))
+        m = np.array(mat, np.uint8)
+        self.lib.xo_distance_field(ni, nj, nk, float(dx), s, float(radius), float(threshold), len(P), _p(P),
+                                   _p(phi), _p(m))
+        return phi, m
 
     # ---- NormalPressureSolver (classic Poisson matrix) ----
     def assemble_normal(self, sc):
@@ -412,6 +461,11 @@ class RefSteps(_Lib):
         L = self.lib
         L.xfsim_apply_forces.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_double] * 4
         L.xfsim_extrapolate.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_int]
+        L.xfsim_advect_particles.argtypes = ([C.c_int] * 3 + [C.c_double, _u8] + [_dp] * 6 +
+                                             [C.c_double, C.c_double, C.c_longlong, _dp] + [_dp] * 3)
+        L.xfsim_p2g.argtypes = [C.c_int] * 3 + [C.c_double, C.c_longlong] + [_dp] * 4
+        L.xfsim_material.argtypes = ([C.c_int] * 3 + [C.c_double, C.c_int, C.c_double, C.c_double,
+                                     C.c_longlong, _dp, _u8, _dp, _u8, _u8])
 
     def apply_forces(self, sc, force, dt, uvw=None):
         u, v, w = (np.array(a, dtype=np.float64) for a in (uvw or (sc.u, sc.v, sc.w)))
@@ -424,3 +478,33 @@ class RefSteps(_Lib):
         self.lib.xfsim_extrapolate(sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(u), _p(v), _p(w),
                                    int(layers))
         return u, v, w
+
+    def advect_particles(self, sc, saved, parts, ratio, dt, dx, grids=False):
+        """The reference's _advectParticles(dt) (steps a, b, then its own P2G);
+        returns the particles, and with grids=True also the faces after P2G."""
+        out = _parts(parts).copy()
+        g = [_f64(a) for a in (sc.u, sc.v, sc.w, *saved)]
+        u, v, w = (np.zeros_like(a) for a in g[:3])
+        self.lib.xfsim_advect_particles(sc.ni, sc.nj, sc.nk, float(dx), _p(np.ascontiguousarray(sc.mat, np.uint8)),
+                                        *map(_p, g), float(ratio), float(dt), len(out), _p(out), _p(u), _p(v), _p(w))
+        return (out, (u, v, w)) if grids else out
+
+    def p2g(self, dims, dx, parts):
+        ni, nj, nk = dims
+        P = _parts(parts)
+        u, v, w = np.zeros((nk, nj, ni + 1)), np.zeros((nk, nj + 1, ni)), np.zeros((nk + 1, nj, ni))
+        self.lib.xfsim_p2g(ni, nj, nk, float(dx), len(P), _p(P), _p(u), _p(v), _p(w))
+        return u, v, w
+
+    def material(self, mat, dx, subdiv, radius, threshold, parts):
+        """updateFeild + updateSurfaceInfo, then _updateMaterial: (phi, material
+        after updateSurfaceInfo, material after _updateMaterial)."""
+        nk, nj, ni = mat.shape
+        P = _parts(parts)
+        s = int(subdiv)
+        phi = np.zeros((nk * s + 1, nj * s + 1, ni * s + 1))
+        m0 = np.ascontiguousarray(mat, np.uint8)
+        ms, mf = np.zeros_like(m0), np.zeros_like(m0)
+        self.lib.xfsim_material(ni, nj, nk, float(dx), s, float(radius), float(threshold), len(P), _p(P), _p(m0),
+                                _p(phi), _p(ms), _p(mf))
+        return phi, ms, mf

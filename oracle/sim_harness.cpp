@@ -215,4 +215,89 @@ void xfsim_extrapolate(int ni, int nj, int nk, const uint8_t* mat, double* u, do
   f.out(u, v, w);
 }
 
+namespace {
+void set_particles(FluidSimulator& fs, long long n, const double* P) {
+  fs._particles.clear();
+  for (long long q = 0; q < n; ++q)
+    fs._particles.push_back(Particle(Vec3d(P[6 * q], P[6 * q + 1], P[6 * q + 2]),
+                                     Vec3d(P[6 * q + 3], P[6 * q + 4], P[6 * q + 5])));
+}
+void get_particles(const FluidSimulator& fs, double* P) {
+  for (size_t q = 0; q < fs._particles.size(); ++q) {
+    const Particle& a = fs._particles[q];
+    const double x[6] = {a.p.x, a.p.y, a.p.z, a.v.x, a.v.y, a.v.z};
+    for (int e = 0; e < 6; ++e) P[6 * q + e] = x[e];
+  }
+}
+}  // namespace
+
+// _advectParticles(dt) (FluidSimulator.cpp:652-728): FLIP/PIC update from
+// (u,v,w) and the saved (us,vs,ws), RK4 advection with solid collisions, then
+// the reference's own particle-to-grid transfer into (uo,vo,wo).  No fluid
+// sources (_applyFluidSource is then a no-op).
+void xfsim_advect_particles(int ni, int nj, int nk, double dx, const uint8_t* mat, const double* u, const double* v,
+                            const double* w, const double* us, const double* vs, const double* ws, double ratio,
+                            double dt, long long n, double* parts, double* uo, double* vo, double* wo) {
+  MuteCout mute;
+  Fields f(ni, nj, nk, mat, us, vs, ws);
+  f.fs._dx = dx;
+  f.fs._usaved = f.fs._u;
+  f.fs._vsaved = f.fs._v;
+  f.fs._wsaved = f.fs._w;
+  Fields::fill(f.fs._u, u);
+  Fields::fill(f.fs._v, v);
+  Fields::fill(f.fs._w, w);
+  f.fs._ratioFLIP = ratio;
+  f.fs._fluidSources.clear();
+  set_particles(f.fs, n, parts);
+  f.fs._advectParticles(dt);
+  get_particles(f.fs, parts);
+  f.out(uo, vo, wo);
+}
+
+// _updateVelocityByParticles (FluidSimulator.cpp:909-1085) on given particles.
+void xfsim_p2g(int ni, int nj, int nk, double dx, long long n, const double* parts, double* u, double* v, double* w) {
+  MuteCout mute;
+  std::vector<uint8_t> mat((size_t)ni * nj * nk, 0);
+  Fields f(ni, nj, nk, mat.data(), u, v, w);
+  f.fs._dx = dx;
+  set_particles(f.fs, n, parts);
+  f.fs._updateVelocityByParticles();
+  f.out(u, v, w);
+}
+
+// The material update of timeStep (FluidSimulator.cpp:274-276):
+// DirectedDistanceField::updateFeild and updateSurfaceInfo(material) with the
+// field set up as init does (:207-213, with the given subdivision, radius and
+// threshold), then _updateMaterial.  Writes phi, the material after
+// updateSurfaceInfo (ms) and after _updateMaterial (mf).
+void xfsim_material(int ni, int nj, int nk, double dx, int subdiv, double radius, double threshold, long long n,
+                    const double* parts, const uint8_t* mat, double* phi, uint8_t* ms, uint8_t* mf) {
+  MuteCout mute;
+  std::vector<double> zu((size_t)(ni + 1) * nj * nk), zv((size_t)ni * (nj + 1) * nk), zw((size_t)ni * nj * (nk + 1));
+  Fields f(ni, nj, nk, mat, zu.data(), zv.data(), zw.data());
+  f.fs._dx = dx;
+  set_particles(f.fs, n, parts);
+  DirectedDistanceField& d = f.fs._dis_field;
+  d.setSize(ni, nj, nk);
+  d.setParticleVector(&f.fs._particles);
+  d.setSubDivisionLevel(subdiv);
+  d.setParticleRadius(radius);
+  d.setDx(dx);
+  d.setThreshold(threshold);
+  d.initField();
+  d.updateFeild();
+  d.updateSurfaceInfo(f.fs._material);
+  dump(d._phi, phi);
+  auto dump_mat = [&](uint8_t* dst) {
+    for (int k = 0; k < nk; ++k)
+      for (int j = 0; j < nj; ++j)
+        for (int i = 0; i < ni; ++i)
+          dst[(size_t)k * ni * nj + (size_t)j * ni + i] = static_cast<uint8_t>(f.fs._material(i, j, k));
+  };
+  dump_mat(ms);
+  f.fs._updateMaterial();
+  dump_mat(mf);
+}
+
 }  // extern "C"

@@ -19,7 +19,8 @@ NormalPressureSolver (pressuresolver.cpp, the classic Poisson matrix): its
 assembly (diag, ax, ay, az, b), its PCG pressure at tol 1e-6 (iterations,
 residual) and the velocities after its applyPressure.  ``--normal-only``
 writes just those (and the step fixtures); ``--steps-only`` writes only the
-``steps_<case>.npz`` fixtures (see step_fixtures).
+``steps_<case>.npz`` fixtures (see step_fixtures); ``--particles-only`` writes
+only the ``particles_<case>.npz`` fixtures (see particle_fixtures).
 """
 from __future__ import annotations
 
@@ -78,6 +79,51 @@ def step_fixtures(R):
         print(f"steps_{name}: forces, {LAYERS}-layer extrapolation, full step")
 
 
+PARTICLE_CASES = {"dam17x13x11": dict(dims=(17, 13, 11), seed=2, dt=0.2, vel=2.0),
+                  "dam19x15x13": dict(dims=(19, 15, 13), seed=3, dt=0.05, vel=4.0)}
+RATIO_FLIP, SUBDIV, THRESHOLD = 0.95, 2, 0.4
+
+
+def particle_fixtures():
+    """``particles_<case>.npz``: the particle steps around the projection, run
+    by the reference's own code (oracle/sim_harness.cpp) on xFluid-seeded
+    particles (scenes.seed_particles, jitter dx/5 so particles cross faces)
+    with random velocities, and one particle dropped so n is not a multiple of
+    six:
+      - _advectParticles(dt) (FluidSimulator.cpp:652-728) with ratio 0.95 on
+        the scene's faces and a perturbed saved copy: particles_out, and the
+        faces after its own particle-to-grid transfer (u_p2g_adv, ...);
+      - _updateVelocityByParticles on the input particles (u_p2g, ...);
+      - updateFeild + updateSurfaceInfo (subdivision 2, radius 3 x the
+        simulator's particle radius, threshold 0.4, FluidSimulator.cpp:207-213):
+        phi, mat_surface; then _updateMaterial: mat_final.
+    `ub` marks the particles whose collision point lies in a cell outside the
+    grid: the reference reads the material out of bounds there (:714), so those
+    particles are not compared (the oracle's status 2)."""
+    from oracle import Oracle, RefSteps  # noqa: E402
+    S, O = RefSteps(), Oracle()
+    for name, cfg in PARTICLE_CASES.items():
+        ni, nj, nk = cfg["dims"]
+        sc = scenes.dam_break(dims=cfg["dims"], seed=cfg["seed"], noise=0.4)
+        dx = 1.0 / ni
+        P = scenes.seed_particles(sc.mat, dx, seed=cfg["seed"], jitter=0.2 * dx, vel_scale=cfg["vel"])[:-1]
+        rng = np.random.default_rng(cfg["seed"])
+        saved = [a + 0.1 * rng.standard_normal(a.shape) for a in (sc.u, sc.v, sc.w)]
+        out, g = S.advect_particles(sc, saved, P, RATIO_FLIP, cfg["dt"], dx, grids=True)
+        _, st = O.advect_particles(sc, saved, P, RATIO_FLIP, cfg["dt"], dx, status=True)
+        p2g = S.p2g((ni, nj, nk), dx, P)
+        radius = 3.0 * (3 * (dx * dx * dx / 8.0) / (4 * 3.141592653)) ** (1.0 / 3.0)
+        phi, ms, mf = S.material(sc.mat, dx, SUBDIV, radius, THRESHOLD, P)
+        np.savez_compressed(
+            OUT / f"particles_{name}.npz",
+            dims=np.array([ni, nj, nk]), dx=dx, mat=sc.mat, u=sc.u, v=sc.v, w=sc.w,
+            us=saved[0], vs=saved[1], ws=saved[2], ratio=RATIO_FLIP, dt=cfg["dt"], parts_in=P,
+            parts_out=out, ub=(st == 2), u_p2g_adv=g[0], v_p2g_adv=g[1], w_p2g_adv=g[2],
+            u_p2g=p2g[0], v_p2g=p2g[1], w_p2g=p2g[2], subdiv=SUBDIV, radius=radius, threshold=THRESHOLD,
+            phi=phi, mat_surface=ms, mat_final=mf)
+        print(f"particles_{name}: {len(P)} particles, status counts {np.bincount(st, minlength=5).tolist()}")
+
+
 def normal_fixtures(R):
     for name, sc in cases().items():
         if name not in NORMAL_CASES:
@@ -99,6 +145,9 @@ def main():
     if build_reference() is None:
         raise SystemExit("reference sources not found; cannot regenerate golden vectors")
     R = Reference()
+    if "--particles-only" in sys.argv:
+        particle_fixtures()
+        return
     if "--steps-only" not in sys.argv:
         normal_fixtures(R)
     step_fixtures(R)

@@ -64,6 +64,9 @@ struct xfp_ctx {
   DevBuf x64, r64, x32, r32, s32, z32, s64, z64, dense;
   // control
   DevBuf ctl, scal, scal2, partials, tpartials, sy, sz, trace;
+  // particle steps (xfp_particles.cu): staged particles and field, bin keys,
+  // indices, boxes, positions, bin starts, box spans, sort/scan scratch
+  DevBuf part_io, phi_io, part_key, part_idx, part_box, part_pos, part_start, part_span, part_tmp;
   // sweep layout (SwTile): tile table, (K,J) -> tile map, cell -> element map
   // and the copies the solves stream (lx, ly, lz, inv, r, y; 8 bytes per
   // element covers every precision)
@@ -126,6 +129,10 @@ int stage_in(xfp_ctx* ctx, DevBuf& buf, const T* src, size_t n, const T** dev) {
 }
 
 // xfp_capi.cu
+size_t ncells(int ni, int nj, int nk);
+size_t nu(int ni, int nj, int nk);
+size_t nv(int ni, int nj, int nk);
+size_t nw_(int ni, int nj, int nk);
 long long spin_limit(const xfp_ctx* ctx);
 int check_dims(xfp_ctx* ctx, int ni, int nj, int nk, const void* mat);
 int ensure_compact(xfp_ctx* ctx, int prec);

@@ -264,3 +264,26 @@ def active_mask(mat: np.ndarray) -> np.ndarray:
     adj[:, 1:] |= fl[:, :-1]; adj[:, :-1] |= fl[:, 1:]
     adj[:, :, 1:] |= fl[:, :, :-1]; adj[:, :, :-1] |= fl[:, :, 1:]
     return fl | ((mat == SOLID) & adj)
+
+
+# xFluid's eight seeding points per fluid cell (FluidSimulator::_addParticle,
+# FluidSimulator.cpp:347-370): cell centre +- dx/4 on each axis, in this order
+_SEED_OFFSETS = np.array([(-1, -1, -1), (1, -1, -1), (1, -1, 1), (-1, -1, 1),
+                          (-1, 1, -1), (1, 1, -1), (1, 1, 1), (-1, 1, 1)], np.float64)
+
+
+def seed_particles(mat: np.ndarray, dx: float, seed: int = 0, jitter: float = 0.01, vel_scale: float = 1.0,
+                   vel=None) -> np.ndarray:
+    """Particles in every fluid cell of `mat` as xFluid seeds them: eight per
+    cell at the centre +- dx/4 with a U[-jitter, jitter] offset (the reference's
+    scale 0.01, FluidSimulator.cpp:364-369).  Velocities are U[-vel_scale,
+    vel_scale] (the reference starts at rest; random velocities exercise the
+    transfers), or `vel` (n, 3) when given.  Returns (n, 6) FP64 rows laid out
+    as struct Particle {Vec3d p; Vec3d v;} (particle.h:5-15)."""
+    rng = np.random.default_rng(seed)
+    k, j, i = np.nonzero(mat == 1)
+    c = (np.stack([i, j, k], 1).astype(np.float64) + 0.5) * dx
+    p = (c[:, None, :] + 0.25 * dx * _SEED_OFFSETS[None]).reshape(-1, 3)
+    p = p + rng.uniform(-jitter, jitter, p.shape)
+    v = rng.uniform(-vel_scale, vel_scale, p.shape) if vel is None else np.asarray(vel, np.float64)
+    return np.ascontiguousarray(np.concatenate([p, v], 1))
