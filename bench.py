@@ -420,6 +420,8 @@ def ours(args, rank, world):
 
     # ---------------- differentiable rollout (C5) beside the headline ----------------
     rollout = None if args.no_batch else rollout_leg(stream, barrier, max_over_ranks)
+    particles = None if args.no_batch else particles_leg(stream, barrier, max_over_ranks,
+                                                         cpu=(rank == 0 and not args.no_cpu))
 
     # ---------------- CPU baseline (rank 0, N=1 only) ----------------
     cpu = None
@@ -439,7 +441,7 @@ def ours(args, rank, world):
                            parallelism="replicas" if world > 1 else "single GPU",
                            tile_k=int(last.get("tile_k", 0))),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk.summary(), "accuracy": accs, "forms": forms, "batch": batch, "rollout": rollout}
+            "clocks": clk.summary(), "accuracy": accs, "forms": forms, "batch": batch, "rollout": rollout, "particles": particles}
     if rank == 0:
         print(json.dumps(line), flush=True)
     for c in (ctx, ctx_h, ctx64):
@@ -583,6 +585,105 @@ def rollout_leg(stream, barrier, max_over_ranks):
                 "pcg_iterations": dict(r.iterations), "loss": loss, "grad_norm": gn}
     finally:
         r.close()
+
+
+def particles_leg(stream, barrier, max_over_ranks, cpu=True):
+    """The particle steps around the projection on the 128^3 dam break: eight
+    particles per fluid cell seeded as xFluid seeds them (jitter dx/5),
+    velocities U[-1,1] (seed 11), faces from the scene, saved faces perturbed,
+    dt 0.01, ratio 0.95; the distance field at FluidSimulator's settings
+    (subdivision 2, radius 3x the particle radius, threshold 0.4).  Device-
+    resident FP64; each step is one blocking library call timed with CUDA
+    events on the launching stream (mean of 5 after a warm-up, particles
+    restored before each advection).  The CPU figure is the oracle (the
+    reference's operation order, one thread) on the 64^3 version of the scene."""
+    import ctypes as C
+    import time
+
+    import torch
+    from xfluid_b200 import _lib, scenes
+
+    def setup(n):
+        sc = scenes.dam_break(n, seed=1)
+        dx = 1.0 / n
+        P = scenes.seed_particles(sc.mat, dx, seed=11, jitter=0.2 * dx, vel_scale=1.0)
+        rng = np.random.default_rng(11)
+        saved = [a + 0.05 * rng.standard_normal(a.shape) for a in (sc.u, sc.v, sc.w)]
+        return sc, dx, P, saved
+
+    n = 128
+    sc, dx, P, saved = setup(n)
+    radius = 3.0 * (3 * (dx ** 3 / 8.0) / (4 * 3.141592653)) ** (1.0 / 3.0)
+    o = _lib.default_options()
+    o.device_pointers = 1
+    o.stream = C.c_void_p(stream.cuda_stream)
+    ctx = _lib.Context(o)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()   # noqa: E731
+    P0, Pd = t(P), t(P)
+    mat = t(np.asarray(sc.mat, np.uint8))
+    uvw = [t(np.asarray(a, np.float64)) for a in (sc.u, sc.v, sc.w)]
+    sv = [t(a) for a in saved]
+    gf = [torch.zeros_like(a) for a in uvw]
+    phi = torch.zeros((n * 2 + 1,) * 3, dtype=torch.float64, device="cuda")
+    m2 = mat.clone()
+    ptr = lambda a: C.c_void_p(a.data_ptr())   # noqa: E731
+    L, N = ctx.lib, len(P)
+    steps = {
+        "advect": lambda: L.xfp_advect_particles_f64(ctx.ptr, n, n, n, dx, ptr(mat), *map(ptr, uvw), *map(ptr, sv),
+                                                     0.95, 0.01, N, ptr(Pd)),
+        "particles_to_grid": lambda: L.xfp_particles_to_grid_f64(ctx.ptr, n, n, n, dx, N, ptr(Pd), *map(ptr, gf)),
+        "update_material": lambda: L.xfp_update_material(ctx.ptr, n, n, n, dx, N, ptr(Pd), ptr(m2)),
+        "distance_field": lambda: L.xfp_distance_field_f64(ctx.ptr, n, n, n, dx, 2, radius, 0.4, N, ptr(Pd), ptr(phi),
+                                                           ptr(m2)),
+    }
+    out = {"workload": f"dam break {n}^3, {N} particles (8 per fluid cell, xFluid's seeding, jitter dx/5), "
+                       "velocities U[-1,1], dt 0.01, ratio 0.95; field subdivision 2, radius 3x particle radius, "
+                       "threshold 0.4; FP64, device-resident",
+           "particles": N, "ms": {}, "particles_per_s": {}}
+    try:
+        for name, fn in steps.items():
+            reps = []
+            for rep in range(6):
+                if name == "advect":
+                    Pd.copy_(P0)
+                barrier()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ctx.check(fn())
+                e1.record(stream)
+                torch.cuda.synchronize()
+                if rep > 0:
+                    reps.append(e0.elapsed_time(e1))
+            ms = max_over_ranks(float(np.mean(reps)))
+            out["ms"][name] = ms
+            out["particles_per_s"][name] = N / (ms * 1e-3)
+        # algorithmic bytes of the advection: particles read + written (96 B),
+        # the faces and material it samples are L2-resident at this size
+        out["advect_gbs"] = N * 96 / (out["ms"]["advect"] * 1e-3) / 1e9
+    finally:
+        ctx.close()
+    if cpu:
+        import oracle   # the checker, timed here as the CPU baseline only
+        scs, dxs, Ps, saveds = setup(64)
+        O = oracle.Oracle()
+        c = {}
+        t0 = time.perf_counter()
+        Pa = O.advect_particles(scs, saveds, Ps, 0.95, 0.01, dxs)
+        c["advect"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        O.p2g((64, 64, 64), dxs, Pa)
+        c["particles_to_grid"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        O.update_material(scs.mat, dxs, Pa)
+        c["update_material"] = time.perf_counter() - t0
+        rs = 3.0 * (3 * (dxs ** 3 / 8.0) / (4 * 3.141592653)) ** (1.0 / 3.0)
+        t0 = time.perf_counter()
+        O.distance_field(scs.mat, dxs, 2, rs, 0.4, Pa)
+        c["distance_field"] = time.perf_counter() - t0
+        out["cpu_baseline"] = {"kind": "port", "cores": 1, "sample": f"the 64^3 scene ({len(Ps)} particles)",
+                               "particles_per_s": {k: len(Ps) / v for k, v in c.items()}}
+    return out
 
 
 def main():
