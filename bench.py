@@ -590,7 +590,9 @@ def rollout_leg(stream, barrier, max_over_ranks):
 def particles_leg(stream, barrier, max_over_ranks, cpu=True):
     """The particle steps around the projection on the 128^3 dam break: eight
     particles per fluid cell seeded as xFluid seeds them (jitter dx/5),
-    velocities U[-1,1] (seed 11), faces from the scene, saved faces perturbed,
+    velocities U[-1,1] (seed 11), the scene's faces (gravity impulse) with
+    U[-0.5,0.5] noise on every face (particles move and hit the walls), saved
+    faces perturbed,
     dt 0.01, ratio 0.95; the distance field at FluidSimulator's settings
     (subdivision 2, radius 3x the particle radius, threshold 0.4).  Device-
     resident FP64; each step is one blocking library call timed with CUDA
@@ -604,7 +606,7 @@ def particles_leg(stream, barrier, max_over_ranks, cpu=True):
     from xfluid_b200 import _lib, scenes
 
     def setup(n):
-        sc = scenes.dam_break(n, seed=1)
+        sc = scenes.dam_break(n, seed=1, noise=0.5)
         dx = 1.0 / n
         P = scenes.seed_particles(sc.mat, dx, seed=11, jitter=0.2 * dx, vel_scale=1.0)
         rng = np.random.default_rng(11)
@@ -637,7 +639,7 @@ def particles_leg(stream, barrier, max_over_ranks, cpu=True):
                                                            ptr(m2)),
     }
     out = {"workload": f"dam break {n}^3, {N} particles (8 per fluid cell, xFluid's seeding, jitter dx/5), "
-                       "velocities U[-1,1], dt 0.01, ratio 0.95; field subdivision 2, radius 3x particle radius, "
+                       "velocities U[-1,1], faces with U[-0.5,0.5] noise, dt 0.01, ratio 0.95; field subdivision 2, radius 3x particle radius, "
                        "threshold 0.4; FP64, device-resident",
            "particles": N, "ms": {}, "particles_per_s": {}}
     try:
@@ -695,10 +697,18 @@ def main():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-scenes leg")
+    ap.add_argument("--particles-case", action="store_true",
+                    help="only run the particle-steps leg (128^3 dam break, no CPU baseline), print its JSON and "
+                         "exit: the case the ncu captures of the particle kernels use")
     ap.add_argument("--profile-case", type=int, default=0, metavar="N",
                     help="only project the N^3 blob scene twice (mixed, device-resident) and exit: "
                          "the small case the ncu captures of the sweep kernels use")
     args = ap.parse_args()
+    if args.particles_case:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps(particles_leg(torch.cuda.current_stream(), lambda: None, lambda x: x, cpu=False)))
+        return
     if args.profile_case:
         profile_case(args.profile_case)
         return

@@ -66,7 +66,8 @@ struct xfp_ctx {
   DevBuf ctl, scal, scal2, partials, tpartials, sy, sz, trace;
   // particle steps (xfp_particles.cu): staged particles and field, bin keys,
   // indices, boxes, positions, bin starts, box spans, sort/scan scratch
-  DevBuf part_io, phi_io, part_key, part_idx, part_box, part_pos, part_start, part_span, part_tmp;
+  DevBuf part_io, phi_io, part_key, part_idx, part_box, part_pos, part_sbox, part_spos, part_start, part_span,
+      part_tmp;
   // sweep layout (SwTile): tile table, (K,J) -> tile map, cell -> element map
   // and the copies the solves stream (lx, ly, lz, inv, r, y; 8 bytes per
   // element covers every precision)

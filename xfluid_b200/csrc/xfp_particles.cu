@@ -350,15 +350,15 @@ __global__ void bin_count_kernel(const unsigned* __restrict__ key, long long n, 
 // component for the transfer, unused for the field)
 __global__ void bin_gather_kernel(const int* __restrict__ sidx, long long n, const int* __restrict__ box,
                                   const double* __restrict__ pos, const double* __restrict__ parts, int vcomp,
-                                  int* __restrict__ sbox, double* __restrict__ spos) {
+                                  int4* __restrict__ sbox_xy, int2* __restrict__ sbox_z,
+                                  double2* __restrict__ spos) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     const int o = sidx[q];
-#pragma unroll
-    for (int e = 0; e < 6; ++e) sbox[6 * q + e] = box[6 * (size_t)o + e];
-    spos[4 * q] = pos[3 * (size_t)o];
-    spos[4 * q + 1] = pos[3 * (size_t)o + 1];
-    spos[4 * q + 2] = pos[3 * (size_t)o + 2];
-    spos[4 * q + 3] = vcomp >= 0 ? parts[6 * (size_t)o + 3 + vcomp] : 0.0;
+    const int* b = box + 6 * (size_t)o;
+    sbox_xy[q] = make_int4(b[0], b[1], b[2], b[3]);
+    sbox_z[q] = make_int2(b[4], b[5]);
+    spos[2 * q] = make_double2(pos[3 * (size_t)o], pos[3 * (size_t)o + 1]);
+    spos[2 * q + 1] = make_double2(pos[3 * (size_t)o + 2], vcomp >= 0 ? parts[6 * (size_t)o + 3 + vcomp] : 0.0);
   }
 }
 
@@ -379,8 +379,9 @@ __device__ __forceinline__ double poly_w(const Poly& W, double rs) {
 // (:1010-1027).  Field: out = weight sum.
 template <bool FIELD>
 __global__ void gather_kernel(int e0, int e1, int e2, int s, double unit, int nb0, int nb1, int nb2, int sp0, int sp1,
-                              int sp2, const int* __restrict__ start, const int* __restrict__ sbox,
-                              const double* __restrict__ spos, Poly W, double* __restrict__ out) {
+                              int sp2, const int* __restrict__ start, const int4* __restrict__ sbox_xy,
+                              const int2* __restrict__ sbox_z, const double2* __restrict__ spos, Poly W,
+                              double* __restrict__ out) {
   const long long total = (long long)e0 * e1 * e2;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
@@ -396,16 +397,16 @@ __global__ void gather_kernel(int e0, int e1, int e2, int s, double unit, int nb
         const long long row = ((long long)ck * nb1 + cj) * nb0;
         const int qa = __ldg(&start[row + i0]), qb = __ldg(&start[row + bi + 1]);
         for (int q = qa; q < qb; ++q) {
-          const int* bx = sbox + 6 * (size_t)q;
-          if (i < __ldg(&bx[0]) || i > __ldg(&bx[1]) || j < __ldg(&bx[2]) || j > __ldg(&bx[3]) ||
-              k < __ldg(&bx[4]) || k > __ldg(&bx[5]))
-            continue;
-          const V3 p = v3(__ldg(&spos[4 * (size_t)q]), __ldg(&spos[4 * (size_t)q + 1]), __ldg(&spos[4 * (size_t)q + 2]));
+          const int4 bxy = __ldg(&sbox_xy[q]);
+          const int2 bz = __ldg(&sbox_z[q]);
+          if (i < bxy.x || i > bxy.y || j < bxy.z || j > bxy.w || k < bz.x || k > bz.y) continue;
+          const double2 pxy = __ldg(&spos[2 * (size_t)q]), pzv = __ldg(&spos[2 * (size_t)q + 1]);
+          const V3 p = v3(pxy.x, pxy.y, pzv.x);
           // transfer: curR = p - idx2Pos (:960); field: gp - p (:296)
           const V3 d = FIELD ? vsub(g, p) : vsub(p, g);
           const double cw = poly_w(W, vdot(d, d));
           wsum = add_rn(wsum, cw);
-          if (!FIELD) vsum = add_rn(vsum, mul_rn(__ldg(&spos[4 * (size_t)q + 3]), cw));
+          if (!FIELD) vsum = add_rn(vsum, mul_rn(pzv.y, cw));
         }
       }
     if (FIELD) out[t] = wsum;
@@ -499,17 +500,22 @@ int bin_and_gather(xfp_ctx* ctx, const double* dparts, long long n, const BoxSpe
   const size_t nn = (size_t)std::max<long long>(n, 1);
   XFP_CUDA(ctx, ctx->part_key.ensure(nn * 2 * sizeof(unsigned)));
   XFP_CUDA(ctx, ctx->part_idx.ensure(nn * 2 * sizeof(int)));
-  XFP_CUDA(ctx, ctx->part_box.ensure(nn * 12 * sizeof(int)));
-  XFP_CUDA(ctx, ctx->part_pos.ensure(nn * 7 * sizeof(double)));
+  XFP_CUDA(ctx, ctx->part_box.ensure(nn * 6 * sizeof(int)));
+  XFP_CUDA(ctx, ctx->part_pos.ensure(nn * 3 * sizeof(double)));
+  XFP_CUDA(ctx, ctx->part_sbox.ensure(nn * (sizeof(int4) + sizeof(int2))));
+  XFP_CUDA(ctx, ctx->part_spos.ensure(nn * 2 * sizeof(double2)));
   XFP_CUDA(ctx, ctx->part_start.ensure((size_t)(nbins + 2) * sizeof(int) * 2 + 16));
   unsigned* key = ctx->part_key.as<unsigned>();
   unsigned* key2 = key + nn;
   int* idx = ctx->part_idx.as<int>();
   int* idx2 = idx + nn;
   int* box = ctx->part_box.as<int>();
-  int* sbox = box + 6 * nn;
   double* pos = ctx->part_pos.as<double>();
-  double* spos = pos + 3 * nn;
+  // sorted copies for the gather: box as int4 (x, y) + int2 (z), position and
+  // carried value as two double2 -- four vector loads per candidate
+  int4* sbox_xy = ctx->part_sbox.as<int4>();
+  int2* sbox_z = reinterpret_cast<int2*>(sbox_xy + nn);
+  double2* spos = ctx->part_spos.as<double2>();
   int* count = ctx->part_start.as<int>();
   int* start = count + (nbins + 2);
   XFP_CUDA(ctx, ctx->part_span.ensure(4 * sizeof(int)));
@@ -541,7 +547,7 @@ int bin_and_gather(xfp_ctx* ctx, const double* dparts, long long n, const BoxSpe
     XFP_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->part_tmp.p, tmp2, count, start, (int)(nbins + 1), st));
     g_kernel_launches += 2;
     ++g_kernel_launches;
-    bin_gather_kernel<<<pgrid(n), 256, 0, st>>>(idx2, n, box, pos, dparts, vcomp, sbox, spos);
+    bin_gather_kernel<<<pgrid(n), 256, 0, st>>>(idx2, n, box, pos, dparts, vcomp, sbox_xy, sbox_z, spos);
     XFP_CUDA(ctx, cudaGetLastError());
   }
   int span[4] = {0, 0, 0, 0};
@@ -549,7 +555,7 @@ int bin_and_gather(xfp_ctx* ctx, const double* dparts, long long n, const BoxSpe
   XFP_CUDA(ctx, cudaStreamSynchronize(st));
   ++g_kernel_launches;
   gather_kernel<FIELD><<<pgrid(total), 256, 0, st>>>(B.ext[0], B.ext[1], B.ext[2], B.s, unit, nb0, nb1, nb2, span[0],
-                                                     span[1], span[2], start, sbox, spos, W, out);
+                                                     span[1], span[2], start, sbox_xy, sbox_z, spos, W, out);
   XFP_CUDA(ctx, cudaGetLastError());
   return XFP_OK;
 }
