@@ -61,3 +61,69 @@ def test_cpp_dropin_matches_python_mirror(shim, tmp_path):
     assert np.array_equal(np.fromfile(tmp_path / "p.f64").reshape(p.shape), p)
     for name, ref in (("u", u), ("v", v), ("w", w)):
         assert np.array_equal(np.fromfile(tmp_path / f"{name}_out.f64").reshape(ref.shape), ref), name
+
+
+# ---- the particle steps (include/xfp_particles.hpp) ----
+@pytest.fixture(scope="module")
+def particles_shim(tmp_path_factory):
+    from xfluid_b200 import build
+    lib = build.build()
+    out = tmp_path_factory.mktemp("pshim") / "particles_main"
+    cxx = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
+    subprocess.run([cxx, "-std=c++17", "-O1", "-Wall", "-Werror", f"-I{ROOT / 'include'}",
+                    str(ROOT / "tests" / "cpp" / "particles_main.cpp"), str(lib), f"-Wl,-rpath,{lib.parent}",
+                    "-o", str(out)], check=True)
+    return out
+
+
+def _particle_case(d: Path):
+    from xfluid_b200 import scenes
+    sc = scenes.dam_break(dims=(26, 22, 18), seed=4, noise=0.5)
+    dx = 1.0 / 26
+    P = scenes.seed_particles(sc.mat, dx, seed=4, jitter=0.2 * dx, vel_scale=2.0)[:-2]
+    rng = np.random.default_rng(4)
+    saved = [a + 0.05 * rng.standard_normal(a.shape) for a in (sc.u, sc.v, sc.w)]
+    _write_scene(d, sc)
+    for name, a in zip(("us", "vs", "ws"), saved):
+        np.ascontiguousarray(a, np.float64).tofile(d / f"{name}.f64")
+    P.tofile(d / "parts.f64")
+    radius = 3.0 * (3 * (dx ** 3 / 8.0) / (4 * 3.141592653)) ** (1.0 / 3.0)
+    args = [sc.ni, sc.nj, sc.nk, len(P), dx, 0.02, 0.95, 2, radius, 0.4]
+    return sc, dx, P, saved, radius, [repr(float(x)) if isinstance(x, float) else str(x) for x in args]
+
+
+def test_particles_header_compiles_and_fails_cleanly_without_gpu(particles_shim, tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    _, _, _, _, _, args = _particle_case(tmp_path)
+    r = subprocess.run([str(particles_shim), str(tmp_path), *args], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 3 and "xfp_create failed" in r.stderr
+
+
+@pytest.mark.gpu
+def test_cpp_particle_steps_match_python_mirror(particles_shim, tmp_path):
+    """The header driven as FluidSimulator::timeStep would call it gives the
+    same bits as the Python mirror (both over libxfp)."""
+    from xfluid_b200.particles import ParticleSteps
+    sc, dx, P, saved, radius, args = _particle_case(tmp_path)
+    r = subprocess.run([str(particles_shim), str(tmp_path), *args], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    s = ParticleSteps(dx)
+    try:
+        mat = np.array(sc.mat, np.uint8)
+        phi = s.updateField(P, mat, subdiv=2, radius=radius, threshold=0.4)
+        surface = mat.copy()
+        s.updateMaterial(P, mat)
+        uvw = [np.array(a, np.float64) for a in (sc.u, sc.v, sc.w)]
+        Pp = np.array(P)
+        s.advectParticles(Pp, mat, uvw, [np.ascontiguousarray(a) for a in saved], 0.02, 0.95)
+        s.updateVelocityByParticles(Pp, uvw)
+    finally:
+        s.close()
+    assert np.array_equal(np.fromfile(tmp_path / "phi.f64").reshape(phi.shape), phi)
+    assert np.array_equal(np.fromfile(tmp_path / "mat_surface.u8", np.uint8).reshape(mat.shape), surface)
+    assert np.array_equal(np.fromfile(tmp_path / "mat_final.u8", np.uint8).reshape(mat.shape), mat)
+    assert np.array_equal(np.fromfile(tmp_path / "parts_out.f64").reshape(Pp.shape), Pp)
+    for name, a in zip(("u_out", "v_out", "w_out"), uvw):
+        assert np.array_equal(np.fromfile(tmp_path / f"{name}.f64").reshape(a.shape), a), name

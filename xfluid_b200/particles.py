@@ -86,6 +86,7 @@ class ParticleSteps:
         stay unchanged, as in the reference."""
         dims = self._dims(mat)
         _check(parts, "float64", (parts.shape[0], 6), "particles")
+        _check(mat, "uint8", mat.shape, "material")
         self._faces(dims, uvw, "")
         self._faces(dims, saved, "saved ")
         ctx = self._context([parts, mat, *uvw, *saved])
@@ -131,6 +132,7 @@ class ParticleSteps:
                 phi = np.zeros(shape)
         _check(phi, "float64", shape, "phi")
         _check(parts, "float64", (parts.shape[0], 6), "particles")
+        _check(mat, "uint8", mat.shape, "material")
         ctx = self._context([parts, mat, phi])
         ctx.check(ctx.lib.xfp_distance_field_f64(ctx.ptr, ni, nj, nk, self.dx, s, float(radius), float(threshold),
                                                  int(parts.shape[0]), _ptr(parts), _ptr(phi),
