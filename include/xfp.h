@@ -257,6 +257,19 @@ int xfp_project_step_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* ma
                          float* w, const float* wu, const float* wv, const float* ww, float* pressure,
                          const double force[3], double dt, int layers, xfp_stats* stats);
 
+/* The reference solver's divergence diagnostic, VariationalPressureSolver::
+ * _calculate_divergience (variationalpressure/variational_pressuresolver.cpp:
+ * 526-597): for every fluid cell, +u(i)-u(i+1)+v(j)-v(j+1)+w(k)-w(k+1) over the
+ * faces whose neighbour cell is not solid (outside the grid counts as solid),
+ * unit weights; 0 for other cells.  div is ni*nj*nk in the cell layout.  The
+ * projection zeroes the weighted form of this quantity (solid faces at 0.5),
+ * which equals b - A p; this is the reference's unweighted diagnostic.  FP64
+ * results are bit-identical to the reference. */
+int xfp_divergence_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const double* u,
+                       const double* v, const double* w, double* div);
+int xfp_divergence_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const float* u,
+                       const float* v, const float* w, float* div);
+
 /* ---- Particle steps (FLIP/PIC) around the projection ----
  * One particle is xFluid's struct Particle {Vec3d p; Vec3d v;} (particle.h:5-15):
  * position then velocity, six doubles, so a std::vector<Particle>'s data()

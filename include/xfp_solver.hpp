@@ -90,6 +90,15 @@ class VariationalPressureSolver {
     return check(rc);
   }
 
+  // ---- the reference's divergence diagnostic (variational_pressuresolver.cpp:526-597) ----
+  // _calculate_divergience into div (resized to ni x nj x nk).
+  template <class Grid>
+  bool calculateDivergence(Grid& div) {
+    if (!ready()) return false;
+    div.resize(ni_, nj_, nk_);
+    return check(xfp_divergence_f64(ctx_, ni_, nj_, nk_, mat_(), u_(), v_(), w_(), &div(0)));
+  }
+
   // ---- extensions ----
   // PCGSolver::set_solver_parameters (pcg_solver.h:234-241).
   void set_solver_parameters(double tol, int max_iter, double omega = 0.97, double min_diag_ratio = 0.25) {

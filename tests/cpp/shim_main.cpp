@@ -4,7 +4,8 @@
 //
 //   shim_main DIR ni nj nk
 // reads DIR/{mat.u8,u.f64,v.f64,w.f64}, runs setDt -> solve -> applyPressure
-// and writes DIR/{p.f64,u_out.f64,v_out.f64,w_out.f64}.  Exit status: 0 solved
+// then the divergence diagnostic of the projected velocities, and writes
+// DIR/{p.f64,u_out.f64,v_out.f64,w_out.f64,div.f64}.  Exit status: 0 solved
 // and applied, 3 solve() returned false (message on stderr), 2 I/O error.
 #include <cstdio>
 #include <string>
@@ -79,8 +80,11 @@ int main(int argc, char** argv) {
   if (!solver.solve(pressure)) return 3;
   if (!solver.applyPressure(pressure)) return 3;
   std::printf("iterations %d rows %lld\n", solver.stats().iterations, solver.stats().rows);
+  // the reference's divergence diagnostic of the projected velocities
+  Grid<double> div;
+  if (!solver.calculateDivergence(div)) return 3;
   if (!write_from(dir + "/p.f64", pressure) || !write_from(dir + "/u_out.f64", u) ||
-      !write_from(dir + "/v_out.f64", v) || !write_from(dir + "/w_out.f64", w))
+      !write_from(dir + "/v_out.f64", v) || !write_from(dir + "/w_out.f64", w) || !write_from(dir + "/div.f64", div))
     return 2;
   return 0;
 }

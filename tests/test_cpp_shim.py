@@ -56,11 +56,14 @@ def test_cpp_dropin_matches_python_mirror(shim, tmp_path):
     s.setMaterial(np.ascontiguousarray(sc.mat, np.uint8))
     s.setVelocityField(u, v, w)
     assert s.solve(p) and s.applyPressure(p)
+    div = np.zeros_like(p)
+    s.calculateDivergence(div)
     s.close()
     # same library, same options, FP64: identical bits
     assert np.array_equal(np.fromfile(tmp_path / "p.f64").reshape(p.shape), p)
     for name, ref in (("u", u), ("v", v), ("w", w)):
         assert np.array_equal(np.fromfile(tmp_path / f"{name}_out.f64").reshape(ref.shape), ref), name
+    assert np.array_equal(np.fromfile(tmp_path / "div.f64").reshape(p.shape), div)
 
 
 # ---- the particle steps (include/xfp_particles.hpp) ----

@@ -140,6 +140,32 @@ def test_ragged_shapes(ctx64, oracle_lib, dims):
     assert bits_equal(d["z"], oracle_lib.precond(sc, F, r))
 
 
+@pytest.mark.parametrize("name", CASES)
+def test_divergence_diagnostic_matches_reference(ctx64, name):
+    """xfp_divergence (VariationalPressureSolver::_calculate_divergience,
+    variational_pressuresolver.cpp:526-597) of the reference's projected
+    velocities is the reference's own diagnostic bit for bit in FP64; FP32
+    agrees with it to FP32 rounding: six face values rounded, five additions
+    of partial sums up to six times the face scale (at most 33 ulp of it)."""
+    import ctypes as C
+    sc, g = load(name)
+    mat = np.ascontiguousarray(sc.mat, np.uint8)
+    uvw = [np.ascontiguousarray(g[k], np.float64) for k in ("u_out", "v_out", "w_out")]
+    div = np.full((sc.nk, sc.nj, sc.ni), 5.0)
+    p = lambda a: C.c_void_p(a.ctypes.data)   # noqa: E731
+    ctx64.check(ctx64.lib.xfp_divergence_f64(ctx64.ptr, sc.ni, sc.nj, sc.nk, p(mat), *map(p, uvw), p(div)))
+    assert bits_equal(div, g["div"])
+    c32 = make_ctx("f32")
+    try:
+        u32 = [a.astype(np.float32) for a in uvw]
+        d32 = np.zeros((sc.nk, sc.nj, sc.ni), np.float32)
+        c32.check(c32.lib.xfp_divergence_f32(c32.ptr, sc.ni, sc.nj, sc.nk, p(mat), *map(p, u32), p(d32)))
+    finally:
+        c32.close()
+    scale = max(float(np.abs(np.concatenate([a.ravel() for a in uvw])).max()), 1e-30)
+    assert float(np.abs(d32 - g["div"]).max()) <= 33 * 2.0 ** -24 * scale
+
+
 def test_empty_scene(ctx64):
     sc = scenes.dam_break(dims=(12, 10, 8))
     sc.mat[:] = scenes.AIR

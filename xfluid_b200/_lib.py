@@ -92,7 +92,8 @@ EXPORTS = [
     "xfp_advect_backward_f64", "xfp_advect_backward_f32", "xfp_box_loss_f64", "xfp_box_loss_f32",
     "xfp_debug_expire_next_sweep", "xfp_apply_forces_f64", "xfp_apply_forces_f32", "xfp_extrapolate_f64",
     "xfp_extrapolate_f32", "xfp_project_step_f64", "xfp_project_step_f32", "xfp_advect_particles_f64",
-    "xfp_particles_to_grid_f64", "xfp_update_material", "xfp_distance_field_f64",
+    "xfp_particles_to_grid_f64", "xfp_update_material", "xfp_distance_field_f64", "xfp_divergence_f64",
+    "xfp_divergence_f32",
 ]
 
 
@@ -139,6 +140,8 @@ def load() -> C.CDLL:
         getattr(L, "xfp_project_step_" + sfx).argtypes = ([vp, C.c_int, C.c_int, C.c_int] + [vp] * 8 +
                                                           [d3, C.c_double, C.c_int, C.POINTER(XfpStats)])
     L.xfp_rhs_inf_noalloc_f64.argtypes = [C.c_int] * 3 + [vp] * 9 + [C.c_char_p, C.c_size_t]
+    for sfx in ("f64", "f32"):
+        getattr(L, "xfp_divergence_" + sfx).argtypes = [vp, C.c_int, C.c_int, C.c_int] + [vp] * 5
     g = [vp, C.c_int, C.c_int, C.c_int, C.c_double]
     L.xfp_advect_particles_f64.argtypes = g + [vp] * 7 + [C.c_double, C.c_double, C.c_longlong, vp]
     L.xfp_particles_to_grid_f64.argtypes = g + [C.c_longlong] + [vp] * 4

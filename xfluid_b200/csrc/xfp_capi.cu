@@ -934,6 +934,32 @@ int extrapolate_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, I
   return XFP_OK;
 }
 
+// VariationalPressureSolver::_calculate_divergience on the device.
+template <typename IOT>
+int divergence_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, const IOT* u, const IOT* v,
+                    const IOT* w, IOT* div) {
+  int rc = check_dims(ctx, ni, nj, nk, mat);
+  if (rc) return rc;
+  if (!u || !v || !w || !div) return fail(ctx, XFP_ERR_ARGS, "NULL array");
+  XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  const uint8_t* dmat;
+  const IOT *du_, *dv, *dw;
+  if ((rc = stage_in(ctx, ctx->io_mat, mat, ncells(ni, nj, nk), &dmat))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_u, u, nu(ni, nj, nk), &du_))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_v, v, nv(ni, nj, nk), &dv))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_w, w, nw_(ni, nj, nk), &dw))) return rc;
+  IOT* dd = div;
+  if (!ctx->opt.device_pointers) {
+    XFP_CUDA(ctx, ctx->io_p.ensure(ncells(ni, nj, nk) * sizeof(IOT)));
+    dd = ctx->io_p.as<IOT>();
+  }
+  XFP_CUDA(ctx, divergence<IOT>(dmat, ni, nj, nk, du_, dv, dw, dd, ctx->stream));
+  if (!ctx->opt.device_pointers)
+    XFP_CUDA(ctx, cudaMemcpyAsync(div, dd, ncells(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return XFP_OK;
+}
+
 // Force fused into assembly and apply, projection, extrapolation on the
 // projected velocities, one call.
 template <typename IOT>
@@ -1212,6 +1238,17 @@ int xfp_extrapolate_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat
 int xfp_extrapolate_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, float* u, float* v,
                         float* w, int layers) {
   return extrapolate_impl<float>(ctx, ni, nj, nk, material, u, v, w, layers);
+}
+
+int xfp_divergence_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const double* u, const double* v,
+                       const double* w, double* div) {
+  if (!ctx) return XFP_ERR_ARGS;
+  return divergence_impl<double>(ctx, ni, nj, nk, material, u, v, w, div);
+}
+int xfp_divergence_f32(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, const float* u, const float* v,
+                       const float* w, float* div) {
+  if (!ctx) return XFP_ERR_ARGS;
+  return divergence_impl<float>(ctx, ni, nj, nk, material, u, v, w, div);
 }
 int xfp_project_step_f64(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* material, double* u, double* v,
                          double* w, const double* wu, const double* wv, const double* ww, double* pressure,

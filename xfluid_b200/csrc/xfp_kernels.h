@@ -142,6 +142,9 @@ cudaError_t apply_forces(const uint8_t* mat, int ni, int nj, int nk, FT* u, FT* 
 template <typename FT>
 cudaError_t extrapolate(const uint8_t* mat, int ni, int nj, int nk, FT* u, FT* v, FT* w, int layers,
                         short* marker, cudaStream_t st);
+template <typename FT>
+cudaError_t divergence(const uint8_t* mat, int ni, int nj, int nk, const FT* u, const FT* v, const FT* w, FT* div,
+                       cudaStream_t st);
 template <typename FT, typename PT>
 cudaError_t apply_pressure_T(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
                              const FT* gu, const FT* gv, const FT* gw, int ni, int nj, int nk,

@@ -85,9 +85,52 @@ __global__ void xlayer_kernel(short* __restrict__ mk, FT* __restrict__ f, int si
   }
 }
 
+// VariationalPressureSolver::_calculate_divergience
+// (variationalpressure/variational_pressuresolver.cpp:526-597): per fluid cell
+// the sum of +u(low face) - u(high face) over the axes, a face counted only when
+// the cell across it is not solid (outside the grid counts as solid); 0 for
+// other cells.  Six additions from 0 in the reference's order.
+template <typename FT>
+__global__ void divergence_kernel(const uint8_t* __restrict__ mat, int ni, int nj, int nk, const FT* __restrict__ u,
+                                  const FT* __restrict__ v, const FT* __restrict__ w, FT* __restrict__ div) {
+  const size_t n = (size_t)ni * nj * nk;
+  auto solid_at = [&](int i, int j, int k) {
+    return !(i >= 0 && j >= 0 && k >= 0 && i < ni && j < nj && k < nk) ||
+           mat[(size_t)k * ni * nj + (size_t)j * ni + i] == MAT_SOLID;
+  };
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % ni), j = (int)((c / ni) % nj), k = (int)(c / ((size_t)ni * nj));
+    FT d = FT(0);
+    if (mat[c] == MAT_FLUID) {
+      const size_t uu = (size_t)k * (ni + 1) * nj + (size_t)j * (ni + 1) + i;
+      const size_t vv = (size_t)k * ni * (nj + 1) + (size_t)j * ni + i;
+      const size_t ww = c;
+      if (!solid_at(i - 1, j, k)) d = add_rn(d, u[uu]);
+      if (!solid_at(i + 1, j, k)) d = sub_rn(d, u[uu + 1]);
+      if (!solid_at(i, j - 1, k)) d = add_rn(d, v[vv]);
+      if (!solid_at(i, j + 1, k)) d = sub_rn(d, v[vv + ni]);
+      if (!solid_at(i, j, k - 1)) d = add_rn(d, w[ww]);
+      if (!solid_at(i, j, k + 1)) d = sub_rn(d, w[ww + (size_t)ni * nj]);
+    }
+    div[c] = d;
+  }
+}
+
 unsigned grid_for(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 32); }
 
 }  // namespace
+
+template <typename FT>
+cudaError_t divergence(const uint8_t* mat, int ni, int nj, int nk, const FT* u, const FT* v, const FT* w, FT* div,
+                       cudaStream_t st) {
+  ++g_kernel_launches;
+  divergence_kernel<FT><<<grid_for((size_t)ni * nj * nk), 256, 0, st>>>(mat, ni, nj, nk, u, v, w, div);
+  return cudaGetLastError();
+}
+template cudaError_t divergence<double>(const uint8_t*, int, int, int, const double*, const double*, const double*,
+                                        double*, cudaStream_t);
+template cudaError_t divergence<float>(const uint8_t*, int, int, int, const float*, const float*, const float*, float*,
+                                       cudaStream_t);
 
 template <typename FT>
 cudaError_t apply_forces(const uint8_t* mat, int ni, int nj, int nk, FT* u, FT* v, FT* w, Force3 frc,

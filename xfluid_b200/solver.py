@@ -167,6 +167,17 @@ class VariationalPressureSolver:
         fn = self._ctx.lib.xfp_extrapolate_f64 if _dtype_name(self._u) == "f64" else self._ctx.lib.xfp_extrapolate_f32
         self._ctx.check(fn(self._ctx.ptr, ni, nj, nk, *map(_ptr, arrs), int(layers)))
 
+    def calculateDivergence(self, div) -> None:
+        """VariationalPressureSolver::_calculate_divergience (variational_
+        pressuresolver.cpp:526-597) of the borrowed velocities into `div`
+        (ni*nj*nk, the velocities' dtype): per fluid cell the unit-weight sum
+        over faces whose neighbour is not solid, 0 elsewhere."""
+        ni, nj, nk = self._size
+        arrs = [self._mat, self._u, self._v, self._w, div]
+        self._prep(arrs)
+        fn = self._ctx.lib.xfp_divergence_f64 if _dtype_name(self._u) == "f64" else self._ctx.lib.xfp_divergence_f32
+        self._ctx.check(fn(self._ctx.ptr, ni, nj, nk, *map(_ptr, arrs)))
+
     def projectStep(self, pressure, force, dt: float, layers: int) -> bool:
         """applyForces, solve, applyPressure and extrapolateVelocity in one
         call, the force fused into the assembly and apply kernels; True when
