@@ -117,14 +117,36 @@ def cpu_project_seconds(sc):
     s64 = sc.astype(np.float64)
     if oracle.reference_available():
         R = oracle.Reference()
-        t = time.perf_counter()
-        R.project(s64.reference_mode(), tol=TOL, maxit=MAXIT)
-        return time.perf_counter() - t, "reference"
+        before = R.set_threads(1)   # the single-core figure: applyPressure's OpenMP loop on one thread
+        try:
+            t = time.perf_counter()
+            R.project(s64.reference_mode(), tol=TOL, maxit=MAXIT)
+            return time.perf_counter() - t, "reference"
+        finally:
+            R.set_threads(before)
     oracle.build_oracle()
     O = oracle.Oracle()
     t = time.perf_counter()
     O.project(s64, tol=TOL, maxit=MAXIT)
     return time.perf_counter() - t, "port"
+
+
+def cpu_apply_pressure(sc):
+    """xFluid's own applyPressure (its OpenMP loop over i,
+    variational_pressuresolver.cpp:120-220) on all host cores and on one,
+    mean of 2 calls each on the scene with a zero pressure field (the work does
+    not depend on the values).  None when the reference was not built."""
+    import oracle
+    if not oracle.reference_available():
+        return None
+    R = oracle.Reference()
+    s64 = sc.astype(np.float64).reference_mode()
+    p = np.zeros((sc.nk, sc.nj, sc.ni))
+    cores = os.cpu_count() or 1
+    ms_all = 1e3 * R.time_apply(s64, p, cores, 2)
+    ms_one = 1e3 * R.time_apply(s64, p, 1, 2)
+    return {"kind": "reference", "threads": cores, "ms_all_threads": ms_all, "ms_1_thread": ms_one,
+            "sample": f"applyPressure alone on the {sc.ni}^3 scene, OpenMP on {cores} threads and on 1"}
 
 
 def _ref_worker(conn, n):
@@ -432,6 +454,10 @@ def ours(args, rank, world):
                           "applyPressure, single-threaded as xFluid's PCG is"
                           + ("; same scene without fractional face weights (xFluid has none)" if kind == "reference"
                              else "; oracle C port, same scene"))}
+        try:
+            cpu["apply_pressure"] = cpu_apply_pressure(sc)
+        except Exception as e:   # a reported extra: never lose the line over it
+            cpu["apply_pressure"] = {"error": repr(e)[:200]}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,

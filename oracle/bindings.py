@@ -301,6 +301,10 @@ class Reference(_Lib):
         L.xfref_project.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 3 + [C.c_double, C.c_int, _dp]
         L.xfref_project.restype = C.c_int
         L.xfref_apply.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 4
+        L.xfref_set_threads.argtypes = [C.c_int]
+        L.xfref_set_threads.restype = C.c_int
+        L.xfref_time_apply.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 4 + [C.c_int, C.c_int]
+        L.xfref_time_apply.restype = C.c_double
         L.xfref_assemble.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 8
         L.xfref_assemble.restype = C.c_int
         L.xfref_factor.argtypes = [C.c_int] * 3 + [_u8] + [_dp] * 7
@@ -355,6 +359,17 @@ class Reference(_Lib):
         ok = self.lib.xfref_project(sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat)), _p(u),
                                     _p(v), _p(w), tol, maxit, _p(p))
         return dict(ok=bool(ok), p=p, u=u, v=v, w=w)
+
+    def set_threads(self, n: int) -> int:
+        """OpenMP threads for the reference's parallel loops; returns the
+        previous count (1 for a build without OpenMP)."""
+        return int(self.lib.xfref_set_threads(int(n)))
+
+    def time_apply(self, sc, p, threads: int, reps: int = 3) -> float:
+        """Mean seconds of the reference's applyPressure on `threads` threads."""
+        u, v, w = (np.array(a, dtype=np.float64) for a in (sc.u, sc.v, sc.w))
+        return float(self.lib.xfref_time_apply(sc.ni, sc.nj, sc.nk, _p(np.ascontiguousarray(sc.mat, np.uint8)),
+                                               _p(_f64(p)), _p(u), _p(v), _p(w), int(threads), int(reps)))
 
     def apply(self, sc, p):
         u, v, w = (np.array(a, dtype=np.float64) for a in (sc.u, sc.v, sc.w))

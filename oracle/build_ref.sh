@@ -10,6 +10,9 @@
 # UINT_MAX and the math functions without including their headers (the
 # reference targets MSVC).  FP contraction is off so the x86-64 build rounds
 # every multiply and add separately, as the reference's own build does.
+# OpenMP is on, as in the reference's project (its applyPressure loop is an
+# omp parallel for); the loop's iterations are independent, so results do not
+# depend on the thread count.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REF="${XFLUID_REF:-/root/reference}"
@@ -22,7 +25,7 @@ fi
 mkdir -p "$OUT"
 # The system g++ (not $CXX): the library must share the process's libstdc++.
 CXX="${XFREF_CXX:-/usr/bin/g++}"
-"$CXX" -std=c++17 -O2 -fPIC -shared -ffp-contract=off -fno-fast-math -w \
+"$CXX" -std=c++17 -O2 -fPIC -shared -ffp-contract=off -fno-fast-math -fopenmp -w \
   -include climits -include cmath \
   -I"$SRC" -I"$SRC/variationalpressure" \
   "$SRC/variationalpressure/variational_pressuresolver.cpp" \

@@ -23,6 +23,7 @@
 // (variational_pressuresolver.cpp:74-75,113); the harness mutes std::cout
 // around each call.
 
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdint>
@@ -31,6 +32,9 @@
 #include <map>
 #include <sstream>
 #include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #define private public
 #define protected public
@@ -152,6 +156,40 @@ int xfref_project(int ni, int nj, int nk, const uint8_t* mat, double* u,
 }
 
 // Reference applyPressure on (u,v,w) in place, given a pressure grid.
+// OpenMP threads the reference's parallel loops use (applyPressure's loop over
+// i, variational_pressuresolver.cpp:134); returns the count in effect before
+// (1 when the build has no OpenMP).
+int xfref_set_threads(int n) {
+#ifdef _OPENMP
+  const int before = omp_get_max_threads();
+  if (n > 0) omp_set_num_threads(n);
+  return before;
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+// applyPressure alone (:120-220) on `threads` threads: the solver is wired once
+// and the call repeated `reps` times after one untimed call; returns the mean
+// seconds per call (u, v, w are updated in place each time).
+double xfref_time_apply(int ni, int nj, int nk, const uint8_t* mat, const double* p, double* u, double* v, double* w,
+                        int threads, int reps) {
+  MuteCout mute;
+  const int before = xfref_set_threads(threads);
+  Scene sc(ni, nj, nk, mat, u, v, w);
+  VariationalPressureSolver s;
+  sc.wire(s);
+  Array3d<double> pg(ni, nj, nk);
+  Scene::fill(pg, p);
+  s.applyPressure(pg);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int r = 0; r < reps; ++r) s.applyPressure(pg);
+  const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  xfref_set_threads(before);
+  return sec / (reps > 0 ? reps : 1);
+}
+
 void xfref_apply(int ni, int nj, int nk, const uint8_t* mat, const double* p,
                  double* u, double* v, double* w) {
   MuteCout mute;
