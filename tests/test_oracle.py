@@ -140,3 +140,28 @@ def test_adjoint_matches_finite_differences(oracle_lib):
         fd = (loss(sp_) - loss(sm_)) / (2 * eps)
         an = float((bu * eu).sum() + (bv * ev).sum() + (bw * ew).sum())
         assert abs(fd - an) <= 1e-7 * max(1.0, abs(an))
+
+
+def test_reference_apply_does_not_depend_on_its_thread_count():
+    """oracle/_ref is built with OpenMP, as xFluid's project is: applyPressure's
+    loop over i (variational_pressuresolver.cpp:134) runs in parallel.  Its
+    iterations write disjoint faces, so one thread and all host threads give the
+    same bits (the golden vectors do not depend on the build's thread count)."""
+    import os
+
+    import oracle
+    if not oracle.reference_available():
+        pytest.skip("reference build absent (oracle/_ref)")
+    R = oracle.Reference()
+    sc = scenes.dam_break(dims=(40, 34, 30), seed=4, noise=0.5)
+    p = np.random.default_rng(4).standard_normal((sc.nk, sc.nj, sc.ni))
+    before = R.set_threads(1)
+    try:
+        one = R.apply(sc, p)
+        R.set_threads(max(2, os.cpu_count() or 2))
+        many = R.apply(sc, p)
+    finally:
+        R.set_threads(before)
+    for a, b in zip(one, many):
+        assert np.array_equal(a, b)
+    assert R.time_apply(sc, p, 1, 1) > 0.0
