@@ -94,6 +94,40 @@ def test_oracle_particles_match_reference_build(seed, dims, dt):
         assert np.array_equal(O.update_material(m_s, dx, P), m_f)
 
 
+@pytest.mark.skipif(not oracle.sim_available(), reason="reference simulator build absent (oracle/_ref)")
+def test_oracle_particles_match_reference_on_lattice_and_edge_positions():
+    """Particles exactly on cell faces and centres (the half-cell lattice), just
+    below zero (where C's truncation and floor differ: pos2Index gives 0 and
+    the particle counts as inside), and just inside the far wall, with fast
+    velocities so many collide: the oracle equals the reference everywhere the
+    reference reads inside its arrays."""
+    sc = scenes.dam_break(dims=(14, 12, 10), seed=5, noise=0.6)
+    ni, nj, nk = sc.ni, sc.nj, sc.nk
+    dx = 1.0 / ni
+    rng = np.random.default_rng(5)
+    n = 3000
+    lat = np.stack([rng.integers(0, 2 * m, n) for m in (ni, nj, nk)], 1) * (0.5 * dx)
+    lat[:300, 0] = -rng.uniform(0, 0.9, 300) * dx
+    lat[300:600, 1] = -rng.uniform(0, 0.9, 300) * dx
+    lat[600:900, 2] = (nk - rng.uniform(0.001, 0.5, 300)) * dx
+    P = np.concatenate([lat, rng.uniform(-3, 3, (n, 3))], 1)
+    saved = [a + 0.1 * rng.standard_normal(a.shape) for a in (sc.u, sc.v, sc.w)]
+    O, R = oracle.Oracle(), oracle.RefSteps()
+    for dt in (0.005, 0.3):
+        po, st = O.advect_particles(sc, saved, P, 0.9, dt, dx, status=True)
+        pr = R.advect_particles(sc, saved, P, 0.9, dt, dx)
+        keep = st != 2
+        assert (st == 1).sum() > 0 and keep.sum() > 0.95 * n
+        assert np.array_equal(po[keep], pr[keep])
+    for a, b in zip(O.p2g((ni, nj, nk), dx, P), R.p2g((ni, nj, nk), dx, P)):
+        assert np.array_equal(a, b)
+    for s, rad in ((2, 0.93 * dx), (1, 1.0 * dx), (3, 0.5 * dx)):
+        phi_o, m_o = O.distance_field(sc.mat, dx, s, rad, 0.4, P)
+        phi_r, m_s, m_f = R.material(sc.mat, dx, s, rad, 0.4, P)
+        assert np.array_equal(phi_o, phi_r) and np.array_equal(m_o, m_s)
+        assert np.array_equal(O.update_material(m_s, dx, P), m_f)
+
+
 def test_seed_particles_follow_the_reference_layout():
     mat = np.zeros((3, 3, 3), np.uint8)
     mat[1, 2, 0] = 1
