@@ -128,6 +128,52 @@ def test_oracle_particles_match_reference_on_lattice_and_edge_positions():
         assert np.array_equal(O.update_material(m_s, dx, P), m_f)
 
 
+def _trunc_div(x, dx):
+    """C's (int)(x / dx): truncation toward zero."""
+    return np.trunc(x / dx).astype(np.int64)
+
+
+@pytest.mark.parametrize("spec", ["faces0", "faces1", "faces2", "field2", "field3", "field1"])
+def test_gather_bin_windows_cover_every_box(spec):
+    """The binning of xfp_particles.cu restated in integers: a particle's key is
+    the bin of its box's low corner, clamped to [0, nb-1]; an output at index t
+    scans bins [b(t) - span, b(t)] per axis, b(t) = min(t/s, nb-1), span = the
+    widest box.  Every output inside a particle's box must scan the particle's
+    bin (that is what makes the gather see exactly the reference's
+    contributions).  Checked on random, lattice and out-of-domain positions."""
+    ni, nj, nk, dx = 13, 9, 11, 0.07
+    rng = np.random.default_rng(8)
+    n = 20000
+    lo_b, hi_b = np.array([-2.0, -2.0, -2.0]), np.array([ni + 2.0, nj + 2.0, nk + 2.0])
+    pos = rng.uniform(lo_b, hi_b, (n, 3)) * dx
+    pos[: n // 4] = rng.integers(-4, 2 * max(ni, nj, nk) + 4, (n // 4, 3)) * (0.5 * dx)   # lattice
+    if spec.startswith("faces"):
+        a = int(spec[-1])
+        s, r = 1, 1.5 * dx
+        sh = np.zeros(3)
+        sh[a] = 0.5 * dx
+        ext = np.array([ni, nj, nk]) + (np.arange(3) == a)
+    else:
+        s, r = int(spec[-1]), 0.93 * dx * (1 + (spec == "field1"))
+        sh = np.zeros(3)
+        ext = np.array([ni, nj, nk]) * s + 1
+    p = pos + sh
+    g0 = _trunc_div((-r) + p, dx)
+    g1 = _trunc_div(p + r, dx)
+    lo, hi = (g0, g1) if s == 1 else (g0 * s, (g1 + 1) * s)
+    nb = (ext + s - 1) // s
+    hits = np.all((hi >= 0) & (lo <= ext - 1), axis=1)
+    assert hits.sum() > n // 2 and (~hits).sum() > 0
+    bc = np.minimum(np.maximum(lo, 0) // s, nb - 1)
+    span = (np.minimum(hi, ext - 1) // s - bc)[hits].max(axis=0)
+    assert (span >= 0).all()
+    lo_t, hi_t = np.maximum(lo, 0)[hits], np.minimum(hi, ext - 1)[hits]
+    b = lambda t: np.minimum(t // s, nb - 1)   # noqa: E731
+    # b is monotone: the window condition at both ends of the covered range
+    assert (bc[hits] <= b(lo_t)).all()
+    assert (bc[hits] >= b(hi_t) - span).all()
+
+
 def test_seed_particles_follow_the_reference_layout():
     mat = np.zeros((3, 3, 3), np.uint8)
     mat[1, 2, 0] = 1
