@@ -57,6 +57,30 @@ def test_null_context_is_rejected(lib):
     assert rc == _lib.XFP_ERR_ARGS
 
 
+def test_particle_and_diagnostic_entry_points_reject_a_null_context(lib):
+    """The particle steps and the divergence diagnostic check their context
+    before touching CUDA (no GPU needed)."""
+    from xfluid_b200 import _lib
+    E = _lib.XFP_ERR_ARGS
+    assert lib.xfp_advect_particles_f64(None, 4, 4, 4, 0.25, *[None] * 7, 0.95, 0.01, 0, None) == E
+    assert lib.xfp_particles_to_grid_f64(None, 4, 4, 4, 0.25, 0, None, None, None, None) == E
+    assert lib.xfp_update_material(None, 4, 4, 4, 0.25, 0, None, None) == E
+    assert lib.xfp_distance_field_f64(None, 4, 4, 4, 0.25, 2, 0.2, 0.4, 0, None, None, None) == E
+    assert lib.xfp_divergence_f64(None, 4, 4, 4, None, None, None, None, None) == E
+    assert lib.xfp_divergence_f32(None, 4, 4, 4, None, None, None, None, None) == E
+
+
+def test_particle_record_is_the_reference_layout():
+    """xfp_particle is xFluid's struct Particle {Vec3d p; Vec3d v;}: six
+    doubles, p first (particle.h:5-15), as include/xfp.h declares it."""
+    src = (ROOT / "include" / "xfp.h").read_text()
+    assert "typedef struct {\n  double p[3];\n  double v[3];\n} xfp_particle;" in src
+
+    class Particle(C.Structure):
+        _fields_ = [("p", C.c_double * 3), ("v", C.c_double * 3)]
+    assert C.sizeof(Particle) == 48 and Particle.v.offset == 24
+
+
 def test_scene_generators_are_seeded_and_shaped():
     from xfluid_b200 import scenes
     a = scenes.blob_scene(dims=(20, 18, 16), seed=4)
