@@ -561,8 +561,20 @@ __device__ __forceinline__ double block_max(double v, double* sh) {
   __syncthreads();
   return t;
 }
-// Returns true in thread 0 of the last of nblk blocks to finish (a batch runs
-// one such group of blocks per scene, each with its own counter).
+// The last block's max over the nblk per-block partials, read by all its
+// threads (partial b by thread b mod blockDim, then the block tree).  A max is
+// exact in any order, so this equals the sequential max bit for bit; it replaces
+// one thread walking every partial (up to NBLK_MAX dependent L2 reads).  Call
+// from every thread of the block; the result is valid in thread 0.
+__device__ __forceinline__ double partials_max(const double* partials, unsigned nblk, double* sh) {
+  double m = 0.0;
+  for (unsigned b = threadIdx.x; b < nblk; b += blockDim.x) m = fmax(m, ((volatile const double*)partials)[b]);
+  return block_max(m, sh);
+}
+
+// Returns true, in every thread of the block, in the last of nblk blocks to
+// finish (a batch runs one such group of blocks per scene, each with its own
+// counter).
 __device__ __forceinline__ bool last_block(PcgScalars* sc, unsigned nblk) {
   __shared__ bool s_last;
   __syncthreads();
@@ -730,9 +742,9 @@ __device__ __forceinline__ void update_xr_body(unsigned bid, unsigned nblk, VT* 
   }
   double t = block_max(m, sh);
   if (threadIdx.x == 0) partials[bid] = t;
-  if (last_block(sc, nblk) && threadIdx.x == 0) {
-    double tot = 0.0;
-    for (unsigned b = 0; b < nblk; ++b) tot = fmax(tot, ((volatile double*)partials)[b]);
+  if (!last_block(sc, nblk)) return;   // uniform over the block
+  const double tot = partials_max(partials, nblk, sh);
+  if (threadIdx.x == 0) {
     sc->res = tot;
     sc->iters += 1;
     if (tot <= sc->tolabs) {
@@ -830,9 +842,9 @@ __device__ __forceinline__ void absmax_init_body(unsigned bid, unsigned nblk, co
     m = fmax(m, (double)fabs(b[c]));
   double t = block_max(m, sh);
   if (threadIdx.x == 0) partials[bid] = t;
-  if (last_block(sc, nblk) && threadIdx.x == 0) {
-    double tot = 0.0;
-    for (unsigned q = 0; q < nblk; ++q) tot = fmax(tot, ((volatile double*)partials)[q]);
+  if (!last_block(sc, nblk)) return;   // uniform over the block
+  const double tot = partials_max(partials, nblk, sh);
+  if (threadIdx.x == 0) {
     sc->bnorm = tot;
     sc->res = tot;
     sc->tolabs = tol * tot;
@@ -942,9 +954,9 @@ __device__ __forceinline__ void residual64_body(
   }
   double t = block_max(m, sh);
   if (threadIdx.x == 0) partials[bid] = t;
-  if (last_block(sc, nblk) && threadIdx.x == 0) {
-    double tot = 0.0;
-    for (unsigned q = 0; q < nblk; ++q) tot = fmax(tot, ((volatile double*)partials)[q]);
+  if (!last_block(sc, nblk)) return;   // uniform over the block
+  const double tot = partials_max(partials, nblk, sh);
+  if (threadIdx.x == 0) {
     sc->res = tot;
     sc->red_count = 0;
   }
