@@ -442,8 +442,17 @@ def ours(args, rank, world):
 
     # ---------------- differentiable rollout (C5) beside the headline ----------------
     rollout = None if args.no_batch else rollout_leg(stream, barrier, max_over_ranks)
-    particles = None if args.no_batch else particles_leg(stream, barrier, max_over_ranks,
-                                                         cpu=(rank == 0 and not args.no_cpu))
+    particles = None
+    if not args.no_batch:
+        if world == 1:
+            # an extra beside the headline: at one rank, never lose the line over it
+            # (with more ranks every rank must take the same barrier sequence)
+            try:
+                particles = particles_leg(stream, barrier, max_over_ranks, cpu=not args.no_cpu)
+            except Exception as e:
+                particles = {"error": repr(e)[:300]}
+        else:
+            particles = particles_leg(stream, barrier, max_over_ranks, cpu=(rank == 0 and not args.no_cpu))
 
     # ---------------- CPU baseline (rank 0, N=1 only) ----------------
     cpu = None
