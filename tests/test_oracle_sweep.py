@@ -4,8 +4,9 @@ reference's assembly relies on (its neighbour lookup has no bounds check,
 variational_pressuresolver.cpp:292), thin and ragged dimensions down to 3
 cells, velocities of several scales.  Every stage of both matrix modes must be
 bit-identical: assembly, MIC(0) factor, preconditioner, PCG (iterations,
-residual, pressure), applyPressure and the divergence diagnostic, and
-NormalPressureSolver's assembly, solve and apply.  Needs oracle/_ref."""
+residual, pressure), applyPressure and the divergence diagnostic,
+NormalPressureSolver's assembly, solve and apply, and the simulator's forces and
+velocity extrapolation.  Needs oracle/_ref."""
 import numpy as np
 import pytest
 
@@ -73,4 +74,23 @@ def test_normal_solver_matches_reference_bitwise(libs, seed):
         assert po["iters"] == pr["iters"] and np.array_equal(po["p"], pr["p"])
     p = np.random.default_rng(seed).standard_normal(sc.mat.shape)
     for x, y in zip(O.apply_normal(sc, p), R.normal_apply(sc, p)):
+        assert np.array_equal(x, y)
+
+
+@pytest.mark.skipif(not oracle.sim_available(), reason="reference simulator build absent (oracle/_ref)")
+@pytest.mark.parametrize("seed", SEEDS[:6])
+def test_simulator_steps_match_reference_bitwise(libs, seed):
+    """_applyForces with random forces (a component below the reference's
+    1e-10 cut-off included) and _expolateVelocity with random layer counts on
+    the same random scenes, against the reference's own simulator code."""
+    O, _ = libs
+    S = oracle.RefSteps()
+    sc = _random_scene(seed)
+    rng = np.random.default_rng(2000 + seed)
+    force = rng.standard_normal(3) * 10.0
+    force[rng.integers(0, 3)] = 3e-11 / 0.02   # |force*dt| = 3e-11: below the cut-off
+    for x, y in zip(O.apply_forces(sc, force, 0.02), S.apply_forces(sc, force, 0.02)):
+        assert np.array_equal(x, y)
+    layers = int(rng.integers(0, 9))
+    for x, y in zip(O.extrapolate(sc, layers), S.extrapolate(sc, layers)):
         assert np.array_equal(x, y)
