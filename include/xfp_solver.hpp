@@ -99,6 +99,30 @@ class VariationalPressureSolver {
     return check(xfp_divergence_f64(ctx_, ni_, nj_, nk_, mat_(), u_(), v_(), w_(), &div(0)));
   }
 
+  // ---- the simulator steps either side of the projection ----
+  // FluidSimulator::_applyForces (FluidSimulator.cpp:429-499): force*dt on every
+  // face next to fluid (an axis with |force*dt| <= 1e-10 is left alone), on the
+  // borrowed velocities.
+  bool applyForces(const double force[3], double dt) {
+    if (!ready()) return false;
+    return check(xfp_apply_forces_f64(ctx_, ni_, nj_, nk_, mat_(), u_(), v_(), w_(), force, dt));
+  }
+  // FluidSimulator::_expolateVelocity (:511-650); the reference passes
+  // layers = int(CFL number + 5).
+  bool extrapolateVelocity(int layers) {
+    if (!ready()) return false;
+    return check(xfp_extrapolate_f64(ctx_, ni_, nj_, nk_, mat_(), u_(), v_(), w_(), layers));
+  }
+  // applyForces, solve, applyPressure and extrapolateVelocity in one call, the
+  // force fused into the assembly and apply kernels (timeStep :310-322).
+  template <class Grid>
+  bool projectStep(Grid& pressureGrid, const double force[3], double dt, int layers) {
+    if (!ready()) return false;
+    pressureGrid.resize(ni_, nj_, nk_);
+    return check(xfp_project_step_f64(ctx_, ni_, nj_, nk_, mat_(), u_(), v_(), w_(), nullptr, nullptr, nullptr,
+                                      &pressureGrid(0), force, dt, layers, &stats_));
+  }
+
   // ---- extensions ----
   // PCGSolver::set_solver_parameters (pcg_solver.h:234-241).
   void set_solver_parameters(double tol, int max_iter, double omega = 0.97, double min_diag_ratio = 0.25) {

@@ -130,3 +130,49 @@ def test_cpp_particle_steps_match_python_mirror(particles_shim, tmp_path):
     assert np.array_equal(np.fromfile(tmp_path / "parts_out.f64").reshape(Pp.shape), Pp)
     for name, a in zip(("u_out", "v_out", "w_out"), uvw):
         assert np.array_equal(np.fromfile(tmp_path / f"{name}.f64").reshape(a.shape), a), name
+
+
+def test_every_header_template_instantiates(tmp_path):
+    """Every method of both C++ drop-ins, templates included, instantiated with
+    an Array3d-like grid and xFluid's Particle/Material types (compile only)."""
+    src = tmp_path / "inst.cpp"
+    src.write_text(r"""
+#include <vector>
+#include "xfp_solver.hpp"
+#include "xfp_particles.hpp"
+enum class Material : char { air = 0, fluid = 1, solid = 2 };
+struct Vec3d { double x, y, z; };
+struct Particle { Vec3d p; Vec3d v; };
+template <class T> struct Grid {
+  void resize(int i, int j, int k) { n[0] = i; n[1] = j; n[2] = k; d.resize((size_t)i * j * k); }
+  T& operator()(int f) { return d[f]; }
+  int sizei() const { return n[0]; }
+  int sizej() const { return n[1]; }
+  int sizek() const { return n[2]; }
+  int n[3] = {0, 0, 0};
+  std::vector<T> d;
+};
+bool all_methods() {
+  Grid<double> u, v, w, p, div, phi;
+  Grid<Material> m;
+  std::vector<Particle> parts;
+  const double g[3] = {0.0, -9.8, 0.0};
+  xfp::VariationalPressureSolver s;
+  xfp::NormalPressureSolver ns;
+  int disfield = 0;
+  s.setSize(4, 4, 4); s.setMaterial(&m); s.setVelocityField(&u, &v, &w); s.setDisField(&disfield);
+  s.setDensity(1.0); s.setDt(0.1); s.setDx(0.25); s.set_solver_parameters(1e-6, 100);
+  ns.setSize(4, 4, 4); ns.setMaterial(&m); ns.setVelocityField(&u, &v, &w);
+  bool ok = s.solve(p) && s.applyPressure(p) && s.calculateDivergence(div) && s.applyForces(g, 0.1) &&
+            s.extrapolateVelocity(5) && s.projectStep(p, g, 0.1, 5) && ns.solve(p) && ns.applyPressure(p);
+  xfp::ParticleSteps ps;
+  ok = ok && ps.updateField(parts, phi, &m, 0.25, 2, 0.2, 0.4) && ps.updateMaterial(parts, m, 0.25) &&
+       ps.advectParticles(parts, m, u, v, w, u, v, w, 0.25, 0.1, 0.95) &&
+       ps.updateVelocityByParticles(parts, u, v, w, 0.25);
+  return ok && s.stats().iterations >= 0 && s.last_error().empty() && ps.last_error().empty();
+}
+""")
+    cxx = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
+    r = subprocess.run([cxx, "-std=c++17", "-fsyntax-only", "-Wall", "-Werror", f"-I{ROOT / 'include'}", str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
