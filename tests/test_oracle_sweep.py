@@ -94,3 +94,39 @@ def test_simulator_steps_match_reference_bitwise(libs, seed):
     layers = int(rng.integers(0, 9))
     for x, y in zip(O.extrapolate(sc, layers), S.extrapolate(sc, layers)):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.skipif(not oracle.sim_available(), reason="reference simulator build absent (oracle/_ref)")
+@pytest.mark.parametrize("seed", SEEDS[:8])
+def test_particle_steps_match_reference_on_random_masks(libs, seed):
+    """The particle steps on the random masks, whose solids sit inside the
+    domain too: collisions walk through interior solid voxels and hit their
+    boxes from every side.  Particles are seeded in the fluid cells as xFluid
+    seeds them, plus some anywhere in the box (solid cells included), with
+    velocities fast enough to cross cells.  Bit-identical where the reference
+    reads inside its arrays (the oracle's status 2 marks the rest)."""
+    O, _ = libs
+    S = oracle.RefSteps()
+    sc = _random_scene(seed)
+    rng = np.random.default_rng(3000 + seed)
+    dx = 1.0 / max(sc.ni, sc.nj, sc.nk)
+    P = scenes.seed_particles(sc.mat, dx, seed=seed, jitter=0.3 * dx, vel_scale=4.0)
+    extra = np.concatenate([rng.uniform(0, 1, (200, 3)) * np.array([sc.ni, sc.nj, sc.nk]) * dx,
+                            rng.uniform(-4, 4, (200, 3))], 1)
+    P = np.concatenate([P, extra])[: len(P) + 200 - (seed % 5)]
+    uvw = [np.clip(a, -50.0, 50.0) for a in (sc.u, sc.v, sc.w)]
+    sc = scenes.Scene(sc.ni, sc.nj, sc.nk, sc.mat, *uvw)
+    saved = [a + 0.1 * rng.standard_normal(a.shape) for a in uvw]
+    for dt in (0.01, 0.08):
+        po, st = O.advect_particles(sc, saved, P, 0.95, dt, dx, status=True)
+        pr = S.advect_particles(sc, saved, P, 0.95, dt, dx)
+        keep = st != 2
+        assert np.array_equal(po[keep], pr[keep])
+    dims = (sc.ni, sc.nj, sc.nk)
+    for a, b in zip(O.p2g(dims, dx, P), S.p2g(dims, dx, P)):
+        assert np.array_equal(a, b)
+    radius = 3.0 * (3 * (dx ** 3 / 8.0) / (4 * 3.141592653)) ** (1.0 / 3.0)
+    phi_o, m_o = O.distance_field(sc.mat, dx, 2, radius, 0.4, P)
+    phi_r, m_s, m_f = S.material(sc.mat, dx, 2, radius, 0.4, P)
+    assert np.array_equal(phi_o, phi_r) and np.array_equal(m_o, m_s)
+    assert np.array_equal(O.update_material(m_s, dx, P), m_f)
