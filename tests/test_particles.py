@@ -389,3 +389,42 @@ def test_python_particle_steps_on_cuda_tensors_match_host_arrays():
         assert np.array_equal(a.cpu().numpy(), b)
     assert np.array_equal(mat_d.cpu().numpy(), mat_h)
     assert np.array_equal(phi_d.cpu().numpy(), phi_h)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [0, 2, 6])
+def test_gpu_particle_steps_on_random_masks_with_interior_solids(seed):
+    """The random fluid/air/solid masks of the oracle sweep (interior solids,
+    collision-heavy): advection and the material update bitwise against the
+    oracle on every particle, the transfers to 1e-12."""
+    import sys
+    sys.path.insert(0, str(Path(__file__).parent))
+    from test_oracle_sweep import _random_scene
+    sc = _random_scene(seed)
+    rng = np.random.default_rng(3000 + seed)
+    dx = 1.0 / max(sc.ni, sc.nj, sc.nk)
+    P = scenes.seed_particles(sc.mat, dx, seed=seed, jitter=0.3 * dx, vel_scale=4.0)
+    extra = np.concatenate([rng.uniform(0, 1, (200, 3)) * np.array([sc.ni, sc.nj, sc.nk]) * dx,
+                            rng.uniform(-4, 4, (200, 3))], 1)
+    P = np.concatenate([P, extra])
+    uvw = [np.clip(a, -50.0, 50.0) for a in (sc.u, sc.v, sc.w)]
+    sc = scenes.Scene(sc.ni, sc.nj, sc.nk, sc.mat, *uvw)
+    saved = [a + 0.1 * rng.standard_normal(a.shape) for a in uvw]
+    O = oracle.Oracle()
+    ref, st = O.advect_particles(sc, saved, P, 0.95, 0.08, dx, status=True)
+    assert (st == 1).sum() + (st == 3).sum() > len(P) // 10
+    ctx = _ctx()
+    try:
+        out = _gpu_advect(ctx, sc, saved, P, 0.95, 0.08, dx)
+        assert np.array_equal(out, ref)
+        for a, b in zip(_gpu_p2g(ctx, (sc.ni, sc.nj, sc.nk), dx, out), O.p2g((sc.ni, sc.nj, sc.nk), dx, out)):
+            assert _maxrel(a, b) <= TRANSFER_TOL
+        radius = 3.0 * (3 * (dx ** 3 / 8.0) / (4 * 3.141592653)) ** (1.0 / 3.0)
+        phi, m = _gpu_field(ctx, sc.mat, dx, 2, radius, 0.4, out)
+        phi_o, m_o = O.distance_field(sc.mat, dx, 2, radius, 0.4, out)
+        assert _maxrel(phi, phi_o) <= TRANSFER_TOL and _classification_equal(m, m_o, phi_o, 2, 0.4)
+        mm = np.array(sc.mat)
+        ctx.check(ctx.lib.xfp_update_material(ctx.ptr, sc.ni, sc.nj, sc.nk, dx, len(out), _p(out), _p(mm)))
+        assert np.array_equal(mm, O.update_material(sc.mat, dx, out))
+    finally:
+        ctx.close()
