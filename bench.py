@@ -524,7 +524,7 @@ def batch_leg(args, rank, world, stream, barrier, max_over_ranks):
         return best, out
 
     o = _lib.default_options()
-    o.precision, o.tol, o.max_iter, o.device_pointers, o.tile_k = _lib.PREC["mixed"], TOL, MAXIT, 1, 8
+    o.precision, o.tol, o.max_iter, o.device_pointers, o.tile_k = _lib.PREC["mixed"], TOL, MAXIT, 1, tile_k
     o.stream = C.c_void_p(stream.cuda_stream)
     ctx = _lib.Context(o)
     P = lambda x: None if x is None else C.c_void_p(x.data_ptr())
@@ -560,14 +560,14 @@ def batch_leg(args, rank, world, stream, barrier, max_over_ranks):
             "sharding": f"LPT over {world} rank(s)"}
 
 
-def profile_case(n):
+def profile_case(n, tile_k=8):
     """Two mixed-precision projections of the n^3 blob scene, inputs on the device."""
     import ctypes as C
     import torch
     from xfluid_b200 import _lib, scenes
     sc = scenes.blob_scene(n, seed=SEED, dtype=np.float32)
     o = _lib.default_options()
-    o.precision, o.tol, o.max_iter, o.device_pointers, o.tile_k = _lib.PREC["mixed"], TOL, MAXIT, 1, 8
+    o.precision, o.tol, o.max_iter, o.device_pointers, o.tile_k = _lib.PREC["mixed"], TOL, MAXIT, 1, tile_k
     ctx = _lib.Context(o)
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     P = lambda x: C.c_void_p(x.data_ptr())
@@ -738,6 +738,7 @@ def main():
     ap.add_argument("--profile-case", type=int, default=0, metavar="N",
                     help="only project the N^3 blob scene twice (mixed, device-resident) and exit: "
                          "the small case the ncu captures of the sweep kernels use")
+    ap.add_argument("--tile-k", type=int, default=8, help="sweep tile height of --profile-case (8, 15 or 16)")
     args = ap.parse_args()
     if args.particles_case:
         import torch
@@ -745,7 +746,7 @@ def main():
         print(json.dumps(particles_leg(torch.cuda.current_stream(), lambda: None, lambda x: x, cpu=False)))
         return
     if args.profile_case:
-        profile_case(args.profile_case)
+        profile_case(args.profile_case, args.tile_k)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -208,6 +208,39 @@ def test_python_particle_steps_check_arguments_before_the_library():
     assert s._ctx == {}
 
 
+class _FakeCudaTensor:
+    """Stands in for a CUDA tensor on a CPU-only host: shape, dtype, layout and
+    device are all the argument checks look at."""
+
+    def __init__(self, shape, dtype, contiguous=True, index=0):
+        self.shape, self.dtype, self._contig = tuple(shape), dtype, contiguous
+        self.is_cuda = True
+        self.device = type("Dev", (), {"index": index, "__str__": lambda d: f"cuda:{d.index}"})()
+
+    def is_contiguous(self):
+        return self._contig
+
+
+def test_python_particle_steps_reject_strided_and_foreign_device_tensors():
+    """A strided view such as x[:, :6] of an (n, 8) tensor has the right shape
+    and dtype, but the kernels would read and write 6n contiguous doubles from
+    its data pointer; a tensor on another GPU would be dereferenced from the
+    context's device.  Both are refused before any library call."""
+    from xfluid_b200.particles import ParticleSteps
+    s = ParticleSteps(0.1, device=0)
+    mat = _FakeCudaTensor((4, 5, 6), "torch.uint8")
+    sliced = _FakeCudaTensor((10, 6), "torch.float64", contiguous=False)
+    with pytest.raises(ValueError, match="contiguous"):
+        s.updateMaterial(sliced, mat)
+    other = _FakeCudaTensor((10, 6), "torch.float64", index=1)
+    with pytest.raises(ValueError, match="cuda:1"):
+        s.updateMaterial(other, mat)
+    with pytest.raises(ValueError, match="contiguous"):
+        s.updateMaterial(_FakeCudaTensor((10, 6), "torch.float64"),
+                         _FakeCudaTensor((4, 5, 6), "torch.uint8", contiguous=False))
+    assert s._ctx == {}
+
+
 # ------------------------------------------------------------------ GPU: the C ABI
 def _ctx(**kw):
     from gpu_util import make_ctx

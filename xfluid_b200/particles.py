@@ -62,6 +62,18 @@ class ParticleSteps:
             raise ValueError("pass either all numpy arrays or all CUDA tensors")
         on_dev = bool(dev) and dev[0]
         if on_dev:
+            # the kernels read and write len(a) contiguous elements from data_ptr()
+            # on the context's device: a strided view (x[:, :6] of an (n, 8)
+            # tensor) would have memory outside the view overwritten, and a
+            # tensor on another GPU would be dereferenced from this one
+            for a in arrays:
+                if a is None:
+                    continue
+                if not a.is_contiguous():
+                    raise ValueError("CUDA tensors must be contiguous")
+                if a.device.index != self.device:
+                    raise ValueError(f"CUDA tensor on {a.device}, expected cuda:{self.device}")
+        if on_dev:
             _lib.sync_torch(self.device)
         if on_dev not in self._ctx:
             o = _lib.default_options()
