@@ -21,6 +21,9 @@ residual) and the velocities after its applyPressure.  ``--normal-only``
 writes just those (and the step fixtures); ``--steps-only`` writes only the
 ``steps_<case>.npz`` fixtures (see step_fixtures); ``--particles-only`` writes
 only the ``particles_<case>.npz`` fixtures (see particle_fixtures).
+
+``full_blob256.npz`` (``--full-only``; about two minutes on one core) pins the
+reference on the full-size 256^3 blob scene (see full_size_fixture).
 """
 from __future__ import annotations
 
@@ -124,6 +127,64 @@ def particle_fixtures():
         print(f"particles_{name}: {len(P)} particles, status counts {np.bincount(st, minlength=5).tolist()}")
 
 
+def scene_digest(sc) -> str:
+    """sha256 over the scene's material bytes and its FP32 face velocities, as
+    generated: the full-size test checks it before comparing results."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in (sc.mat, sc.u, sc.v, sc.w):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+FULL_N, FULL_SEED, FULL_MAXIT = 256, 3, 20000
+
+
+def full_size_fixture(R):
+    """``full_blob256.npz``: xFluid's own solver on the 256^3 blob scene
+    (scenes.blob_scene(256, seed=3), reference mode: the same mask, obstacle
+    and FP32 faces without fractional weights), single-threaded:
+      - solve to tol 1e-6 (iterations, residual) and to tol 1e-12 (the exact
+        solution the convergence error is measured against);
+      - the full-field L2 norms of both pressures and of their difference;
+      - a fixed sample of the pressures (every 97th unknown row, flat indices
+        stored) and of the velocities after applyPressure (every 389th face
+        that borders fluid);
+      - the reference's own divergence diagnostic's L-inf after the projection.
+    The whole fields (16.7M cells) are too large to commit; the sample pins the
+    live reference run the GPU test makes beside it."""
+    sc32 = scenes.blob_scene(FULL_N, seed=FULL_SEED, dtype=np.float32)
+    sc = sc32.astype(np.float64).reference_mode()
+    before = R.set_threads(1)
+    try:
+        sol = R.solve(sc, TOL, FULL_MAXIT)
+        ex = R.solve(sc, 1e-12, FULL_MAXIT)
+        assert sol["ok"] and ex["ok"]
+        u2, v2, w2 = R.apply(sc, sol["p"])
+        div = R.divergence(sc, u2, v2, w2)
+    finally:
+        R.set_threads(before)
+    fl = sc.mat == scenes.FLUID
+    nb = np.zeros_like(fl)
+    nb[1:] |= fl[:-1]; nb[:-1] |= fl[1:]
+    nb[:, 1:] |= fl[:, :-1]; nb[:, :-1] |= fl[:, 1:]
+    nb[:, :, 1:] |= fl[:, :, :-1]; nb[:, :, :-1] |= fl[:, :, 1:]
+    rows = np.flatnonzero(fl | ((sc.mat == scenes.SOLID) & nb))
+    prow = rows[::97].astype(np.int64)
+    mu, mv, mw = scenes.fluid_adjacent_faces(sc.mat)
+    fu, fv, fw = (np.flatnonzero(m)[::389].astype(np.int64) for m in (mu, mv, mw))
+    p, pe = sol["p"].ravel(), ex["p"].ravel()
+    np.savez_compressed(
+        OUT / "full_blob256.npz", n=FULL_N, seed=FULL_SEED, digest=scene_digest(sc32), tol=TOL,
+        maxit=FULL_MAXIT, rows=len(rows), iters=sol["iters"], resid=sol["resid"], iters_exact=ex["iters"],
+        p_l2=np.linalg.norm(p), pe_l2=np.linalg.norm(pe), p_minus_pe_l2=np.linalg.norm(p - pe),
+        idx_p=prow, p=p[prow], pe=pe[prow], idx_u=fu, idx_v=fv, idx_w=fw,
+        u_out=u2.ravel()[fu], v_out=v2.ravel()[fv], w_out=w2.ravel()[fw],
+        div_inf=np.abs(div).max())
+    print(f"full_blob256: {len(rows)} rows, {sol['iters']} iterations (exact: {ex['iters']}), "
+          f"reference vs exact rel L2 {np.linalg.norm(p - pe) / np.linalg.norm(pe):.3e}")
+
+
 def normal_fixtures(R):
     for name, sc in cases().items():
         if name not in NORMAL_CASES:
@@ -145,6 +206,9 @@ def main():
     if build_reference() is None:
         raise SystemExit("reference sources not found; cannot regenerate golden vectors")
     R = Reference()
+    if "--full-only" in sys.argv:
+        full_size_fixture(R)
+        return
     if "--particles-only" in sys.argv:
         particle_fixtures()
         return

@@ -7,8 +7,10 @@ import numpy as np
 from xfluid_b200.scenes import Scene
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-# the variational solver's cases (normal_*.npz belong to test_normal.py, steps_*.npz to test_steps.py, particles_*.npz to test_particles.py)
-CASES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("normal_", "steps_", "particles_")))
+# the variational solver's cases (normal_*.npz belong to test_normal.py, steps_*.npz to test_steps.py,
+# particles_*.npz to test_particles.py, full_*.npz to the full-size test in test_gpu_parity.py)
+CASES = sorted(p.stem for p in GOLDEN.glob("*.npz")
+               if not p.stem.startswith(("normal_", "steps_", "particles_", "full_")))
 
 
 def load(name):

@@ -165,3 +165,26 @@ def test_reference_apply_does_not_depend_on_its_thread_count():
     for a, b in zip(one, many):
         assert np.array_equal(a, b)
     assert R.time_apply(sc, p, 1, 1) > 0.0
+
+
+def test_full_size_fixture_matches_the_seeded_scene():
+    """The 256^3 fixture (xFluid's own solver on the benchmark scene) was made
+    on the scene scenes.blob_scene(256, seed=3) generates here, and its sample
+    indices are unknown rows of that scene."""
+    import hashlib
+    from golden_io import GOLDEN
+    g = dict(np.load(GOLDEN / "full_blob256.npz"))
+    sc = scenes.blob_scene(int(g["n"]), seed=int(g["seed"]), dtype=np.float32)
+    h = hashlib.sha256()
+    for a in (sc.mat, sc.u, sc.v, sc.w):
+        h.update(np.ascontiguousarray(a).tobytes())
+    assert h.hexdigest() == str(g["digest"])
+    fl = sc.mat == scenes.FLUID
+    nb = np.zeros_like(fl)
+    nb[1:] |= fl[:-1]; nb[:-1] |= fl[1:]
+    nb[:, 1:] |= fl[:, :-1]; nb[:, :-1] |= fl[:, 1:]
+    nb[:, :, 1:] |= fl[:, :, :-1]; nb[:, :, :-1] |= fl[:, :, 1:]
+    rows = fl | ((sc.mat == scenes.SOLID) & nb)
+    assert int(rows.sum()) == int(g["rows"])
+    assert rows.ravel()[g["idx_p"]].all()
+    assert int(g["iters"]) < int(g["iters_exact"]) and g["p_minus_pe_l2"] < 1e-4 * g["pe_l2"]
