@@ -74,8 +74,13 @@ class VariationalPressureSolver {
   void setDx(double dx) { dx_ = dx; }
 
   // ---- solve / apply (variational_pressuresolver.cpp:50-220) ----
+  // stats() and last_error() describe the most recent solve; a solve that
+  // cannot start (arguments missing, no CUDA device) leaves stats().status at
+  // XFP_ERR_ARGS or XFP_ERR_CUDA.
   template <class Grid>
   bool solve(Grid& pressureGrid) {
+    stats_ = xfp_stats{};
+    err_.clear();
     if (!ready()) return false;
     pressureGrid.resize(ni_, nj_, nk_);
     const int rc = xfp_solve_f64(ctx_, ni_, nj_, nk_, mat_(), u_(), v_(), w_(), nullptr, nullptr, nullptr,
@@ -117,6 +122,8 @@ class VariationalPressureSolver {
   // force fused into the assembly and apply kernels (timeStep :310-322).
   template <class Grid>
   bool projectStep(Grid& pressureGrid, const double force[3], double dt, int layers) {
+    stats_ = xfp_stats{};
+    err_.clear();
     if (!ready()) return false;
     pressureGrid.resize(ni_, nj_, nk_);
     return check(xfp_project_step_f64(ctx_, ni_, nj_, nk_, mat_(), u_(), v_(), w_(), nullptr, nullptr, nullptr,
@@ -147,12 +154,14 @@ class VariationalPressureSolver {
   bool ready() {
     if (!mat_ || !u_ || !v_ || !w_ || ni_ < 1 || nj_ < 1 || nk_ < 1) {
       err_ = "setSize, setMaterial and setVelocityField must be called first";
+      stats_.status = XFP_ERR_ARGS;
       std::fprintf(stderr, "xfp: %s\n", err_.c_str());
       return false;
     }
     if (!ctx_ && xfp_create(&ctx_, &opt_) != XFP_OK) {
       ctx_ = nullptr;
       err_ = "xfp_create failed (no CUDA device?)";
+      stats_.status = XFP_ERR_CUDA;
       std::fprintf(stderr, "xfp: %s\n", err_.c_str());
       return false;
     }

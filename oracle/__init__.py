@@ -13,6 +13,6 @@ Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
 this package, and only as the checker or the timed CPU baseline.  The CUDA
 product path never imports it.
 """
-from .bindings import (ORACLE_LIB, REF_LIB, SIM_LIB, Oracle, Reference, RefSim, RefSteps,  # noqa: F401
-                       build_oracle, build_reference, oracle_available, reference_available,
-                       sim_available)
+from .bindings import (DROPIN_LIB, ORACLE_LIB, REF_LIB, SIM_LIB, Oracle, Reference, RefSim,  # noqa: F401
+                       RefSimDropIn, RefSteps, build_oracle, build_reference, dropin_available,
+                       oracle_available, reference_available, seed_rand, sim_available)

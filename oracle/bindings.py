@@ -18,6 +18,7 @@ ORACLE_SRCS = [ORACLE_SRC, HERE / "xfp_particles_oracle.c"]
 ORACLE_LIB = HERE / "_build" / "libxfp_oracle.so"
 REF_LIB = HERE / "_ref" / "libxfref.so"
 SIM_LIB = HERE / "_ref" / "libxfsim.so"
+DROPIN_LIB = HERE / "_ref" / "libxfsim_dropin.so"
 
 _dp = C.POINTER(C.c_double)
 _u8 = C.POINTER(C.c_uint8)
@@ -46,7 +47,8 @@ def build_reference(ref_root: str | None = None) -> Path | None:
     env = dict(os.environ)
     if ref_root:
         env["XFLUID_REF"] = ref_root
-    root = Path(env.get("XFLUID_REF", "/root/reference"))
+    # XFLUID_REF, else a checkout named `reference` beside this repository
+    root = Path(env.get("XFLUID_REF", str(HERE.parent.parent / "reference")))
     if not (root / "xFluid" / "xFluid" / "variationalpressure").is_dir():
         return None
     subprocess.check_call(["bash", str(HERE / "build_ref.sh")], env=env,
@@ -58,6 +60,17 @@ def build_reference(ref_root: str | None = None) -> Path | None:
 
 def sim_available() -> bool:
     return SIM_LIB.exists()
+
+
+def dropin_available() -> bool:
+    return DROPIN_LIB.exists()
+
+
+def seed_rand(seed: int) -> None:
+    """srand() of the process's C library: xFluid's FluidSimulator::init
+    jitters its particles with rand() (xfluidutil.cpp:67-70), so two simulators
+    seeded alike start from the same particles."""
+    C.CDLL(None).srand(C.c_uint(seed))
 
 
 def oracle_available() -> bool:
@@ -425,6 +438,9 @@ class RefSim(_Lib):
         L.xfsim_end_step.argtypes = [C.c_void_p]
         L.xfsim_fluid_cells.argtypes = [C.c_void_p]
         L.xfsim_fluid_cells.restype = C.c_int
+        L.xfsim_particle_count.argtypes = [C.c_void_p]
+        L.xfsim_particle_count.restype = C.c_longlong
+        L.xfsim_particles.argtypes = [C.c_void_p, _dp]
         self.n = n
         self.h = L.xfsim_create(n, cfl, gravity, tol, maxit)
         for lo, hi in (boxes if boxes is not None else [((0.0, 0.0, 0.0), (0.4, 0.5, 1.0))]):
@@ -465,6 +481,65 @@ class RefSim(_Lib):
 
     def fluid_cells(self):
         return self.lib.xfsim_fluid_cells(self.h)
+
+    def particles(self):
+        P = np.zeros((self.lib.xfsim_particle_count(self.h), 6))
+        self.lib.xfsim_particles(self.h, _p(P))
+        return P
+
+
+class RefSimDropIn(_Lib):
+    """xFluid's own FluidSimulator built with this project's solver class as
+    its pressure-solver member (oracle/_ref/libxfsim_dropin.so,
+    oracle/sim_dropin_harness.cpp): the dam break, stepped as RefSim steps the
+    stock build, with the simulator's own _solvePressure calling the library."""
+
+    def __init__(self, n=64, cfl=5.0, gravity=-9.8, tol=1e-6, maxit=200):
+        super().__init__(DROPIN_LIB)
+        L = self.lib
+        L.xfsd_solver_type.restype = C.c_char_p
+        L.xfsd_create_dam.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int]
+        L.xfsd_create_dam.restype = C.c_void_p
+        L.xfsd_destroy.argtypes = [C.c_void_p]
+        L.xfsd_begin_step.argtypes = [C.c_void_p, C.c_double, _u8, _dp, _dp, _dp]
+        L.xfsd_begin_step.restype = C.c_double
+        L.xfsd_project.argtypes = [C.c_void_p, _dp, _dp, _dp, C.POINTER(C.c_int)]
+        L.xfsd_project.restype = C.c_int
+        L.xfsd_end_step.argtypes = [C.c_void_p]
+        L.xfsd_particle_count.argtypes = [C.c_void_p]
+        L.xfsd_particle_count.restype = C.c_longlong
+        L.xfsd_particles.argtypes = [C.c_void_p, _dp]
+        self.n = n
+        self.solver_type = L.xfsd_solver_type().decode()
+        self.h = L.xfsd_create_dam(n, cfl, gravity, tol, maxit)
+
+    def close(self):
+        if self.h:
+            self.lib.xfsd_destroy(self.h)
+            self.h = None
+
+    def begin_step(self, max_dt=1.0 / 30.0):
+        n = self.n
+        mat = np.zeros((n, n, n), np.uint8)
+        u, v, w = np.zeros((n, n, n + 1)), np.zeros((n, n + 1, n)), np.zeros((n + 1, n, n))
+        dt = self.lib.xfsd_begin_step(self.h, max_dt, _p(mat), _p(u), _p(v), _p(w))
+        return dt, mat, u, v, w
+
+    def project(self):
+        """The simulator's _solvePressure through the library: (status, u, v, w, iterations)."""
+        n = self.n
+        u, v, w = np.zeros((n, n, n + 1)), np.zeros((n, n + 1, n)), np.zeros((n + 1, n, n))
+        it = C.c_int(-1)
+        rc = self.lib.xfsd_project(self.h, _p(u), _p(v), _p(w), C.byref(it))
+        return rc, u, v, w, it.value
+
+    def end_step(self):
+        self.lib.xfsd_end_step(self.h)
+
+    def particles(self):
+        P = np.zeros((self.lib.xfsd_particle_count(self.h), 6))
+        self.lib.xfsd_particles(self.h, _p(P))
+        return P
 
 
 class RefSteps(_Lib):

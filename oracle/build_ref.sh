@@ -4,7 +4,8 @@
 # into oracle/_ref/libxfref.so, together with oracle/ref_harness.cpp (the test
 # harness that binds it).  TEST INFRASTRUCTURE ONLY.
 #
-#   XFLUID_REF  root of the reference checkout (default /root/reference)
+#   XFLUID_REF  root of the reference checkout (default: a checkout named
+#               `reference` beside this repository)
 #
 # g++ needs <climits>/<cmath> force-included: variationalpressure/util.h uses
 # UINT_MAX and the math functions without including their headers (the
@@ -15,7 +16,7 @@
 # depend on the thread count.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${XFLUID_REF:-/root/reference}"
+REF="${XFLUID_REF:-$HERE/../../reference}"
 SRC="$REF/xFluid/xFluid"
 OUT="$HERE/_ref"
 if [ ! -f "$SRC/variationalpressure/variational_pressuresolver.cpp" ]; then

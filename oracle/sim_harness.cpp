@@ -165,6 +165,18 @@ void xfsim_end_step(void* h) {
 
 int xfsim_fluid_cells(void* h) { return static_cast<Sim*>(h)->fs._countFluidCell(); }
 
+long long xfsim_particle_count(void* h) { return (long long)static_cast<Sim*>(h)->fs._particles.size(); }
+
+// The simulator's particles as (p, v) rows of 6 doubles.
+void xfsim_particles(void* h, double* P) {
+  const FluidSimulator& f = static_cast<Sim*>(h)->fs;
+  for (size_t q = 0; q < f._particles.size(); ++q) {
+    const Particle& a = f._particles[q];
+    const double x[6] = {a.p.x, a.p.y, a.p.z, a.v.x, a.v.y, a.v.z};
+    for (int e = 0; e < 6; ++e) P[6 * q + e] = x[e];
+  }
+}
+
 // The two steps either side of the projection on given arrays, through a
 // simulator of the grid's size (FluidSimulator(ni,nj,nk) only sizes its grids,
 // FluidSimulator.cpp:26-31): material and faces are filled in, the step runs,

@@ -7,6 +7,8 @@ from pathlib import Path
 import numpy as np
 import pytest
 
+import oracle
+
 ROOT = Path(__file__).resolve().parents[1]
 
 
@@ -176,3 +178,24 @@ bool all_methods() {
     r = subprocess.run([cxx, "-std=c++17", "-fsyntax-only", "-Wall", "-Werror", f"-I{ROOT / 'include'}", str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.skipif(not oracle.dropin_available(), reason="drop-in simulator build absent")
+def test_dropin_build_wires_the_library_class_and_fails_loudly_without_a_gpu():
+    """Host-only check of the drop-in build (no GPU here): the simulator
+    constructs and runs its init wiring against the library class, steps up
+    to the projection, and its _solvePressure then reports an error status
+    from the library instead of a silent CPU fallback."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: the GPU test covers the build")
+    oracle.seed_rand(1)
+    sim = oracle.RefSimDropIn(16, cfl=5.0, gravity=-9.8, tol=1e-6, maxit=200)
+    try:
+        assert sim.solver_type == "xfp::VariationalPressureSolver"
+        dt, mat, u, v, w = sim.begin_step()
+        assert dt > 0 and (mat == 1).any()
+        rc, *_ = sim.project()
+        assert rc < 0
+    finally:
+        sim.close()

@@ -154,3 +154,46 @@ def test_pool_drop_128_mixed_vs_fp64_oracle_per_step():
         # the refined residual meets the tolerance, up to the rounding of the
         # FP32 output faces (six faces per cell, half an ulp each)
         assert r["div"] <= 1.01e-6 * r["b_inf"] + 6 * 2.0 ** -24 * r["umax"], msg
+
+
+@pytest.mark.skipif(not (oracle.sim_available() and oracle.dropin_available()),
+                    reason="reference simulator builds absent (oracle/_ref/libxfsim.so, libxfsim_dropin.so)")
+def test_dam_break_30_steps_with_the_library_inside_xfluids_own_build():
+    """The drop-in as INTEGRATION.md describes it: xFluid's own FluidSimulator
+    compiled with its pressure-solver member (FluidSimulator.h:215) declared as
+    xfp::VariationalPressureSolver and FluidSimulator.cpp unchanged, so the
+    simulator's own wiring (:216-221) and _solvePressure (:501-509) drive the
+    library (FP64).  It runs the plain dam break (64^3, CFL 5, tol 1e-6, at
+    most 200 iterations) side by side with the stock build from the same seed.
+    Per step: the same time step, the same material, the projected velocities
+    within 1e-9 relative of the stock build's, iterations within 5%; after 30
+    steps the particles agree to 1e-9 of the domain.  (The builds differ only
+    in the dot products' summation order, so the two runs drift apart at
+    round-off level.)"""
+    oracle.seed_rand(1)
+    stock = oracle.RefSim(64, cfl=5.0, gravity=-9.8, tol=1e-6, maxit=200)
+    oracle.seed_rand(1)
+    ours = oracle.RefSimDropIn(64, cfl=5.0, gravity=-9.8, tol=1e-6, maxit=200)
+    assert ours.solver_type == "xfp::VariationalPressureSolver"
+    try:
+        assert np.array_equal(stock.particles(), ours.particles())
+        worst = 0.0
+        for step in range(STEPS):
+            dt_s, mat_s, *_ = stock.begin_step()
+            dt_o, mat_o, *_ = ours.begin_step()
+            assert abs(dt_s - dt_o) <= 1e-12 * dt_s, (step, dt_s, dt_o)
+            assert np.array_equal(mat_s, mat_o), step
+            ok, _, us, vs, ws, its = stock.project()
+            rc, uo, vo, wo, ito = ours.project()
+            assert ok and rc == 0, (step, ok, rc)
+            assert abs(ito - its) <= max(1, int(np.ceil(0.05 * its))), (step, ito, its)
+            for a, b in ((uo, us), (vo, vs), (wo, ws)):
+                e = _rel(a, b)
+                worst = max(worst, e)
+                assert e <= 1e-9, (step, e)
+            stock.end_step()
+            ours.end_step()
+        assert np.abs(stock.particles() - ours.particles()).max() <= 1e-9
+    finally:
+        stock.close()
+        ours.close()
