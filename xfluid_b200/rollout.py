@@ -49,6 +49,10 @@ class Rollout:
         self._ck: dict = {}
         self._final = None
         self.iterations = {"forward": 0, "backward": 0}
+        # |G^T g|_inf of every adjoint projection (the right-hand side of its
+        # MIC(0)-PCG solve), in the order the reverse pass runs them: zero when
+        # the loss's sensitivity has not reached a face next to fluid
+        self.adjoint_rhs_inf: list[float] = []
 
     def close(self) -> None:
         self._ctx.close()
@@ -93,6 +97,7 @@ class Rollout:
         if self._ctx.check(rc) != _lib.XFP_OK:
             raise _lib.XfpError(rc, "adjoint projection did not converge")
         self.iterations["backward"] += st.iterations
+        self.adjoint_rhs_inf.append(float(st.b_inf))
         du, dv, dw = (torch_empty_like(a) for a in g)
         self._ctx.check(self._fn("xfp_advect_backward", u)(self._ctx.ptr, self.ni, self.nj, self.nk, P(u), P(v),
                                                            P(w), P(pu), P(pv), P(pw), P(du), P(dv), P(dw), self.c))
@@ -122,6 +127,7 @@ class Rollout:
         if self._final is None:
             raise RuntimeError("forward() first")
         _, g = self.loss(*self._final, grad=True)
+        self.adjoint_rhs_inf = []
         for s0 in sorted(self._ck, reverse=True):
             states = []
             u, v, w = self._ck[s0]
