@@ -98,6 +98,7 @@ typedef struct xfp_stats {
   int sweeps;            /* triangular-solve sweep launches timed in ms_sweeps */
   long long launches;    /* device kernels launched by this call */
   int tile_k;            /* sweep tile height the call used (k-lines) */
+  int graph;             /* 1: the PCG iterations ran as a CUDA graph; 0: launched one by one */
 } xfp_stats;
 
 /* Fills opt with defaults: tol 1e-5, max_iter 100, omega 0.97, ratio 0.25 --
@@ -313,6 +314,12 @@ int xfp_advect_particles_f64(xfp_ctx* ctx, int ni, int nj, int nk, double dx, co
                              long long n, xfp_particle* particles);
 int xfp_particles_to_grid_f64(xfp_ctx* ctx, int ni, int nj, int nk, double dx, long long n,
                               const xfp_particle* particles, double* u, double* v, double* w);
+/* Replaces FluidSimulator::_maxVelocity (FluidSimulator.cpp:387-400), the
+ * speed frameStep divides the CFL distance by to pick each substep's dt
+ * (:228-241): the square root of the largest v.v over the particles, v.v
+ * rounded as the reference forms it (array3d.h:33-36), so the result -- and
+ * the dt -- are the reference's bits.  0 for no particles.  Synchronous. */
+int xfp_max_speed_f64(xfp_ctx* ctx, long long n, const xfp_particle* particles, double* max_speed);
 int xfp_update_material(xfp_ctx* ctx, int ni, int nj, int nk, double dx, long long n,
                         const xfp_particle* particles, uint8_t* material);
 int xfp_distance_field_f64(xfp_ctx* ctx, int ni, int nj, int nk, double dx, int subdiv, double radius,
@@ -337,13 +344,19 @@ int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* materi
                      double* b, double* inv, double* lx, double* ly, double* lz,
                      double* y, double* z, double* q);
 
-/* |b|_inf of the pressure system's right-hand side -- the same value
- * xfp_solve_f64 reports as stats.b_inf -- computed without allocating any
- * device memory.  This entry point has no counterpart in the reference.  It is
- * for callers that must not call cudaMalloc/cudaFree: a real-time loop that
- * cannot afford cudaFree's device-wide synchronisation, or an application
- * whose own allocator has reserved the device's memory.  No context is
- * needed.
+/* |b|_inf of the pressure system's right-hand side, computed without
+ * allocating any device memory.  This entry point has no counterpart in the
+ * reference.  It is for callers that must not call cudaMalloc/cudaFree: a
+ * real-time loop that cannot afford cudaFree's device-wide synchronisation, or
+ * an application whose own allocator has reserved the device's memory.  No
+ * context is needed.
+ *
+ * b is the variational matrix's right-hand side with no body force: the value
+ * equals, bit for bit, stats.b_inf of an FP64 solve or projection with
+ * options.matrix = XFP_MATRIX_VARIATIONAL (xfp_solve_f64, xfp_project_f64).
+ * It differs from the b of an XFP_MATRIX_NORMAL solve (which drops solid rows
+ * and solid faces) and of xfp_project_step_* (which adds force*dt first).  A
+ * NaN in the inputs that reaches b gives a NaN result.
  *
  * All arrays, including the output b_inf (one double), are device (or managed)
  * memory on the current device; host pointers are rejected.  The kernel runs
@@ -353,10 +366,11 @@ int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* materi
  * loaded on that GPU until the process exits), so grids above 268,435,456
  * cells are rejected with XFP_ERR_ARGS.  Calls share that array: calls whose
  * kernels may overlap on the GPU (different streams or threads) race and must
- * be serialised by the caller.  The first call on a device looks up the
- * array's device address and clears it synchronously; make that first call
- * before any stream capture begins.  On error a message goes to err (up to
- * err_len bytes, may be NULL). */
+ * be serialised by the caller.  Every call looks up the array's address in the
+ * current context (so a context re-created by cudaDeviceReset is handled); the
+ * first call on a device also loads the library's device code there, so make
+ * that first call before any stream capture begins.  On error a message goes
+ * to err (up to err_len bytes, may be NULL). */
 int xfp_rhs_inf_noalloc_f64(int ni, int nj, int nk, const uint8_t* material,
                             const double* u, const double* v, const double* w,
                             const double* wu, const double* wv, const double* ww,

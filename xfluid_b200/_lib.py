@@ -74,6 +74,7 @@ class XfpStats(C.Structure):
         ("sweeps", C.c_int),
         ("launches", C.c_longlong),
         ("tile_k", C.c_int),
+        ("graph", C.c_int),
     ]
 
     def as_dict(self) -> dict:
@@ -93,7 +94,7 @@ EXPORTS = [
     "xfp_debug_expire_next_sweep", "xfp_apply_forces_f64", "xfp_apply_forces_f32", "xfp_extrapolate_f64",
     "xfp_extrapolate_f32", "xfp_project_step_f64", "xfp_project_step_f32", "xfp_advect_particles_f64",
     "xfp_particles_to_grid_f64", "xfp_update_material", "xfp_distance_field_f64", "xfp_divergence_f64",
-    "xfp_divergence_f32",
+    "xfp_divergence_f32", "xfp_max_speed_f64",
 ]
 
 
@@ -147,6 +148,7 @@ def load() -> C.CDLL:
     L.xfp_particles_to_grid_f64.argtypes = g + [C.c_longlong] + [vp] * 4
     L.xfp_update_material.argtypes = g + [C.c_longlong, vp, vp]
     L.xfp_distance_field_f64.argtypes = g + [C.c_int, C.c_double, C.c_double, C.c_longlong, vp, vp, vp]
+    L.xfp_max_speed_f64.argtypes = [vp, C.c_longlong, vp, C.POINTER(C.c_double)]
     for name in EXPORTS:
         f = getattr(L, name)
         if name not in ("xfp_default_options", "xfp_last_error", "xfp_version"):

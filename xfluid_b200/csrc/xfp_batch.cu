@@ -37,7 +37,7 @@ struct BatchState {
   DevBuf io, pdense;
   std::vector<BatchSeg> hsegs;
   std::vector<long long> line_base, rows, nlines_act;
-  int n = 0, nw = 0, ntiles = 0, blocks_lines = 0, blocks_cells = 0;
+  int n = 0, nw = 0, ntiles = 0, blocks_lines = 0, blocks_cells = 0, blocks_groups = 0;
   long long M = 0;
   std::map<std::string, int> tuned;   // batch shape -> sweep tile height
   std::string layout_key;             // shape + tile height of the layout built last
@@ -115,9 +115,10 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
     XFP_CUDA(ctx, offset_lines(lines + B->line_base[s], B->line_base[s + 1] - B->line_base[s], base[s], st));
   // cell -> line index (line numbers local to each scene's table; cells global)
   XFP_CUDA(ctx, ctx->cell_line.ensure((std::max<long long>(base[n], 4) + 8) * sizeof(int)));
+  XFP_CUDA(ctx, ctx->group_line.ensure((std::max<long long>(base[n], 4) / 4 + 8) * sizeof(int)));
   for (int s = 0; s < n; ++s)
     XFP_CUDA(ctx, build_cell_line(lines + B->line_base[s], B->line_base[s + 1] - B->line_base[s],
-                                  ctx->cell_line.as<int>(), st));
+                                  ctx->cell_line.as<int>(), ctx->group_line.as<int>(), st));
   // merge the scenes' tile lists by wavefront level (each list is already in
   // its own topological order, which the merge keeps)
   std::vector<int> all_tiles(ntile_slots > 0 ? ntile_slots : 1);
@@ -146,7 +147,7 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
   // per-scene block decomposition of the vector kernels (as a single launch)
   B->hsegs.assign(n, BatchSeg{});
   XFP_CUDA(ctx, B->part.ensure((size_t)n * NBLK_MAX * sizeof(double)));
-  int bl = 0, bc = 0;
+  int bl = 0, bc = 0, bg = 0;
   for (int s = 0; s < n; ++s) {
     BatchSeg& g = B->hsegs[s];
     const long long nl = (long long)S[s].nj * S[s].nk, Ms = cnt[4 * s];
@@ -155,6 +156,8 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
     g.blk_lines_start = bl;
     g.blk_cells = (int)std::max<long long>(1, std::min<long long>((Ms + 255) / 256, NBLK_MAX));
     g.blk_cells_start = bc;
+    g.blk_groups = (int)spmv_block_count(Ms, NBLK_MAX);
+    g.blk_groups_start = bg;
     g.pad = 0;
     g.base = base[s];
     g.M = Ms;
@@ -163,9 +166,11 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
     g.line_base = B->line_base[s];
     bl += g.blk_lines;
     bc += g.blk_cells;
+    bg += g.blk_groups;
   }
   B->blocks_lines = bl;
   B->blocks_cells = bc;
+  B->blocks_groups = bg;
   XFP_CUDA(ctx, B->segs.ensure(n * sizeof(BatchSeg)));
   XFP_CUDA(ctx, B->tiles.ensure(tiles.size() * sizeof(int)));
   XFP_CUDA(ctx, B->tile_scene.ensure(tscene.size() * sizeof(int)));
@@ -312,8 +317,8 @@ int batch_pcg(xfp_ctx* ctx, BatchState* B, const VT* const A[4], const VT* b, VT
   }
   auto iteration = [&]() -> cudaError_t {
     cudaError_t e;
-    if ((e = batch_spmv_dot<VT, VT, DT>(segs, n, B->blocks_cells, A[0], A[1], A[2], A[3], s, z,
-                                        ctx->cell_line.as<int>(), dsc, 0, st)))
+    if ((e = batch_spmv_dot<VT, VT, DT>(segs, n, B->blocks_groups, A[0], A[1], A[2], A[3], s, z,
+                                        ctx->group_line.as<int>(), dsc, 0, st)))
       return e;
     if ((e = batch_update_xr<VT>(segs, n, B->blocks_cells, x, r, s, z, dsc, st, rsw, perm))) return e;
     if ((e = batch_sweep<VT, IT, DT>(ctx, B, SWEEP_FWD, g, d))) return e;
@@ -445,6 +450,8 @@ int batch_solve(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<IOT>>& S
   const double* Ac[4] = {A[0], A[1], A[2], A[3]};
   if ((rc = batch_factor<float, double, double>(ctx, B, Ac, F, ctx->inv64.as<double>(), omega, ratio))) return rc;
   for (int q = 0; q < 3; ++q) XFP_CUDA(ctx, (convert<double, float>(F[q], ctx->L32[q].as<float>(), M, st)));
+  // FP64 pivots, streamed by the FP32 solves rounded to FP32 (as a single scene's mixed solve)
+  XFP_CUDA(ctx, (convert<double, float>(ctx->inv64.as<double>(), ctx->inv32.as<float>(), M, st)));
   const float* Lc[3] = {ctx->L32[0].as<float>(), ctx->L32[1].as<float>(), ctx->L32[2].as<float>()};
   const float* A32c[4] = {A32[0], A32[1], A32[2], A32[3]};
   double* x64 = ctx->x64.as<double>();
@@ -499,8 +506,8 @@ int batch_solve(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<IOT>>& S
     float* b32 = ctx->A32[4].as<float>();
     XFP_CUDA(ctx, copy_vec<float>(ctx->r32.as<float>(), b32, M, st));
     std::vector<PcgScalars> hin;
-    rc = batch_pcg<float, double, double>(ctx, B, A32c, b32, ctx->x32.as<float>(), ctx->r32.as<float>(),
-                                          ctx->s32.as<float>(), ctx->z32.as<float>(), Lc, ctx->inv64.as<double>(),
+    rc = batch_pcg<float, float, double>(ctx, B, A32c, b32, ctx->x32.as<float>(), ctx->r32.as<float>(),
+                                         ctx->s32.as<float>(), ctx->z32.as<float>(), Lc, ctx->inv32.as<float>(),
                                           0.5, maxit, B->tols.as<double>(), B->maxits.as<int>(), dsc, hin, maxit);
     if (rc < 0) return rc;
     for (int q = 0; q < n; ++q)
@@ -756,11 +763,12 @@ int project_batch(xfp_ctx* ctx, int n, const xfp_scene* scenes, xfp_stats* stats
       o.ms_solve = ms[1];
       o.ms_apply = ms[2];
       o.ms_total = ms[0] + ms[1] + ms[2] + ms[3];
-      const double bpr = prec == XFP_PREC_F64 ? 224.0 : prec == XFP_PREC_F32 ? 112.0 : 120.0;
+      const double bpr = prec == XFP_PREC_F64 ? 224.0 : 112.0;   // FP32 pivots in the mixed solves
       const double cells = (double)scenes[s].ni * scenes[s].nj * scenes[s].nk;
       o.bytes = bpr * (double)o.rows * o.iterations + 33.0 * cells + 24.0 * (double)o.rows + 29.0 * cells;
       o.launches = launches;
       o.tile_k = B->nw;
+      o.graph = B->graph_used ? 1 : 0;
     }
   }
   return status;

@@ -69,7 +69,9 @@ int build_layout(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk) {
   ctx->M = cnt[0]; ctx->rows = cnt[1]; ctx->nlines_act = cnt[2]; ctx->ntiles = cnt[3];
   ctx->nlines_all = nlines;
   XFP_CUDA(ctx, ctx->cell_line.ensure((std::max<long long>(ctx->M, 4) + 8) * sizeof(int)));
-  XFP_CUDA(ctx, build_cell_line(ctx->lines.as<Line>(), nlines, ctx->cell_line.as<int>(), ctx->stream));
+  XFP_CUDA(ctx, ctx->group_line.ensure((std::max<long long>(ctx->M, 4) / 4 + 8) * sizeof(int)));
+  XFP_CUDA(ctx, build_cell_line(ctx->lines.as<Line>(), nlines, ctx->cell_line.as<int>(), ctx->group_line.as<int>(),
+                                ctx->stream));
   return build_sweep_layout(ctx);
 }
 
@@ -119,6 +121,7 @@ int ensure_compact(xfp_ctx* ctx, int prec) {
   }
   if (prec == XFP_PREC_F32 || prec == XFP_PREC_MIXED) {
     for (auto& b : ctx->A32) XFP_CUDA(ctx, b.ensure(M * 4));
+    XFP_CUDA(ctx, ctx->inv32.ensure(M * 4));
     XFP_CUDA(ctx, ctx->x32.ensure(M * 4));
     XFP_CUDA(ctx, ctx->r32.ensure(M * 4));
     XFP_CUDA(ctx, ctx->s32.ensure(M * 4));
@@ -183,16 +186,19 @@ int run_sweep(xfp_ctx* ctx, int op, const SweepGrid& g, const SweepData<VT, IT, 
   XFP_CUDA(ctx, sweep_launch(op, gl, d, ctx->nw, grid, ctx->stream));
   if (timed) {
     cudaEventRecord(ctx->sweep_ev[ctx->sweep_ev_used + 1], ctx->stream);
+    ctx->sweep_work[ctx->sweep_ev_used / 2] = 1;
     ctx->sweep_ev_used += 2;
   }
   return XFP_OK;
 }
 
-// Sum of the timed sweep durations (after the stream has been synchronised).
+// Sum of the timed durations of the sweep launches that did work (after the
+// stream has been synchronised).
 double sweep_ms(xfp_ctx* ctx, int* n) {
   double tot = 0;
   int cnt = 0;
   for (int q = 0; q + 1 < ctx->sweep_ev_used; q += 2) {
+    if (!ctx->sweep_work[q / 2]) continue;
     float ms = 0;
     if (cudaEventElapsedTime(&ms, ctx->sweep_ev[q], ctx->sweep_ev[q + 1]) == cudaSuccess) {
       tot += ms;
@@ -282,6 +288,7 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   SweepGrid gs[2] = {make_grid(ctx, dsc, 0), make_grid(ctx, dsc, 1)};
   int rc;
   if ((rc = sweep_copies<VT, IT, DT>(ctx, L, inv, r, gs, 2, &d)) != XFP_OK) return rc;
+  const int first_timed = ctx->sweep_ev_used / 2;
   const SweepGrid& g0 = gs[0];
   const SweepGrid& g1 = gs[1];
   // with a sweep layout, r is kept in both layouts (update_xr writes both)
@@ -302,7 +309,7 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   for (int done_iters = 0;;) {
     for (int q = 0; q < K; ++q) {
       XFP_CUDA(ctx, (spmv_dot<VT, VT, DT>(A[0], A[1], A[2], A[3], s, z, ctx->lines.as<Line>(),
-                                          ctx->cell_line.as<int>(), ctx->nj, ctx->nk, M, dsc, part, NBLK_MAX, 0,
+                                          ctx->group_line.as<int>(), ctx->nj, ctx->nk, M, dsc, part, NBLK_MAX, 0,
                                           st)));
       XFP_CUDA(ctx, (update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), NBLK_MAX, st, rsw, perm)));
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g1, d)) != XFP_OK) return rc;
@@ -316,6 +323,10 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
     if (hsc->done) break;
     if (done_iters > maxit + 2 * K) return fail(ctx, XFP_ERR_CUDA, "PCG loop did not terminate");
   }
+  // the preconditioner's two sweeps, then two per iteration but the last (the
+  // converged iteration skips its preconditioner): 2 * iterations did work;
+  // the launches after them in the last chunk returned at once
+  for (int q = first_timed + 2 * std::max(hsc->iters, 1); q < ctx->sweep_ev_used / 2; ++q) ctx->sweep_work[q] = 0;
   if (hsc->status == XFP_ERR_BREAKDOWN) return fail(ctx, XFP_ERR_BREAKDOWN, "PCG breakdown: rho is zero or NaN");
   return hsc->status == 0 ? XFP_OK : XFP_NOT_CONVERGED;
 }
@@ -483,6 +494,8 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     if ((rc = factor<float, double, double>(ctx, Ac, F, ctx->inv64.as<double>(), omega, ratio)) != XFP_OK) return rc;
     if ((rc = check_sweep_error(ctx)) != XFP_OK) return rc;
     for (int q = 0; q < 3; ++q) XFP_CUDA(ctx, (convert<double, float>(F[q], ctx->L32[q].as<float>(), M, st)));
+    // the pivots are computed in FP64 (above); the FP32 solves stream them rounded to FP32
+    XFP_CUDA(ctx, (convert<double, float>(ctx->inv64.as<double>(), ctx->inv32.as<float>(), M, st)));
     ev_record(ctx, 2);
     const float* Lc[3] = {ctx->L32[0].as<float>(), ctx->L32[1].as<float>(), ctx->L32[2].as<float>()};
     const float* A32c[4] = {A32[0], A32[1], A32[2], A32[3]};
@@ -519,9 +532,9 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
         // inner rhs lives in s32 scratch's partner: use r32 as b, z32/s32/x32 work
         float* b32 = ctx->A32[4].as<float>();
         XFP_CUDA(ctx, copy_vec<float>(ctx->r32.as<float>(), b32, M, st));
-        int irc = pcg<float, double, double>(ctx, A32c, b32, ctx->x32.as<float>(), ctx->r32.as<float>(),
-                                             ctx->s32.as<float>(), ctx->z32.as<float>(), Lc,
-                                             ctx->inv64.as<double>(), inner, maxit - total, dsc, &hsc);
+        int irc = pcg<float, float, double>(ctx, A32c, b32, ctx->x32.as<float>(), ctx->r32.as<float>(),
+                                            ctx->s32.as<float>(), ctx->z32.as<float>(), Lc,
+                                            ctx->inv32.as<float>(), inner, maxit - total, dsc, &hsc);
         if (irc < 0) return irc;
         total += hsc.iters;
         XFP_CUDA(ctx, refine_update(x64, ctx->x32.as<float>(), M, st));
@@ -569,7 +582,9 @@ int solution_dense(xfp_ctx* ctx, IOT* dense) {
   return XFP_OK;
 }
 
-double bytes_per_row_iter(int prec) { return prec == XFP_PREC_F64 ? 224.0 : prec == XFP_PREC_F32 ? 112.0 : 120.0; }
+// Algorithmic bytes per unknown row and PCG iteration: FP32 vectors, L and
+// pivots (the mixed form streams its FP64 pivots as FP32) 112, FP64 224.
+double bytes_per_row_iter(int prec) { return prec == XFP_PREC_F64 ? 224.0 : 112.0; }
 
 void fill_stats(xfp_ctx* ctx, xfp_stats* s, int status, double ms_total) {
   if (!s) return;
@@ -811,8 +826,10 @@ int dump_dense(xfp_ctx* ctx, const T* compact, double* host_out) {
 }
 
 // VT/IT/CT as in the solve of the context's precision; A: coefficients used by
-// the factor (CT) and by the SpMV (VT).
-template <typename VT, typename IT, typename CT>
+// the factor (CT) and by the SpMV (VT).  SIT: the inverse-pivot type the
+// triangular solves stream (the mixed form factors in FP64 and solves with an
+// FP32 copy, as its PCG does); the dumped inv is the factor's own.
+template <typename VT, typename IT, typename CT, typename SIT = IT>
 int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* const F[6], IT* inv,
                const VT* const L[3], const double* dr, double* out[12]) {
   int rc;
@@ -839,22 +856,28 @@ int debug_core(xfp_ctx* ctx, const CT* const Af[5], const VT* const Av[4], CT* c
       XFP_CUDA(ctx, copy_vec<double>(ctx->io_gv.as<double>(), (double*)r, M, st));
     else
       XFP_CUDA(ctx, (convert<double, float>(ctx->io_gv.as<double>(), (float*)r, M, st)));
-    SweepData<VT, IT, CT> d;
-    d.r = r; d.y = z; d.lx = L[0]; d.ly = L[1]; d.lz = L[2]; d.inv = inv;
+    const SIT* sinv = reinterpret_cast<const SIT*>(inv);
+    if (!std::is_same<SIT, IT>::value) {
+      XFP_CUDA(ctx, ctx->inv32.ensure((M + 8) * sizeof(float)));
+      XFP_CUDA(ctx, (convert<IT, SIT>(inv, reinterpret_cast<SIT*>(ctx->inv32.p), M, st)));
+      sinv = reinterpret_cast<const SIT*>(ctx->inv32.p);
+    }
+    SweepData<VT, SIT, CT> d;
+    d.r = r; d.y = z; d.lx = L[0]; d.ly = L[1]; d.lz = L[2]; d.inv = sinv;
     d.partials = ctx->tpartials.as<double>();
     d.sy = ctx->sy.as<unsigned long long>();
     d.sz = ctx->sz.as<unsigned long long>();
     SweepGrid g = make_grid(ctx, nullptr, 0);
-    if ((rc = sweep_copies<VT, IT, CT>(ctx, L, inv, r, &g, 1, &d))) return rc;
-    if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_FWD, g, d))) return rc;
+    if ((rc = sweep_copies<VT, SIT, CT>(ctx, L, sinv, r, &g, 1, &d))) return rc;
+    if ((rc = run_sweep<VT, SIT, CT>(ctx, SWEEP_FWD, g, d))) return rc;
     // the solve results are in the sweep layout: back to the line layout
     if ((rc = sweep_result<VT>(ctx, z))) return rc;
     XFP_CUDA(ctx, cudaStreamSynchronize(st));
     if ((rc = dump_dense<VT>(ctx, z, out[9]))) return rc;
-    if ((rc = run_sweep<VT, IT, CT>(ctx, SWEEP_BWD, g, d))) return rc;
+    if ((rc = run_sweep<VT, SIT, CT>(ctx, SWEEP_BWD, g, d))) return rc;
     if ((rc = sweep_result<VT>(ctx, z))) return rc;
     XFP_CUDA(ctx, (spmv_dot<VT, VT, VT>(Av[0], Av[1], Av[2], Av[3], r, qv, ctx->lines.as<Line>(),
-                                        ctx->cell_line.as<int>(), ctx->nj, ctx->nk, M, nullptr, (VT*)nullptr,
+                                        ctx->group_line.as<int>(), ctx->nj, ctx->nk, M, nullptr, (VT*)nullptr,
                                         NBLK_MAX, 1, st)));
   }
   XFP_CUDA(ctx, cudaStreamSynchronize(st));
@@ -1048,6 +1071,7 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
   }
   for (auto& e : ctx->ev) cudaEventCreate(&e);
   ctx->sweep_ev.resize(2048);
+  ctx->sweep_work.assign(1024, 0);
   for (auto& e : ctx->sweep_ev) cudaEventCreate(&e);
   if (getenv("XFP_TRACE")) {
     ctx->tracing = true;
@@ -1068,7 +1092,7 @@ int xfp_destroy(xfp_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   DevBuf* all[] = {&ctx->io_mat, &ctx->io_u, &ctx->io_v, &ctx->io_w, &ctx->io_wu, &ctx->io_wv, &ctx->io_ww,
                    &ctx->io_p, &ctx->io_gu, &ctx->io_gv, &ctx->io_gw, &ctx->lines, &ctx->lens,
-                   &ctx->tile_active, &ctx->tiles, &ctx->counters, &ctx->cell_line, &ctx->inv64, &ctx->inv32, &ctx->x64,
+                   &ctx->tile_active, &ctx->tiles, &ctx->counters, &ctx->cell_line, &ctx->group_line, &ctx->inv64, &ctx->inv32, &ctx->x64,
                    &ctx->r64, &ctx->x32, &ctx->r32, &ctx->s32, &ctx->z32, &ctx->s64, &ctx->z64, &ctx->dense,
                    &ctx->sy, &ctx->sz, &ctx->ctl, &ctx->scal, &ctx->scal2, &ctx->partials, &ctx->tpartials};
   for (DevBuf* b : all) b->release();
@@ -1205,7 +1229,7 @@ int xfp_debug_stages(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* materi
     const double* Af[5] = {A[0], A[1], A[2], A[3], A[4]};
     const float* Av[4] = {A32[0], A32[1], A32[2], A32[3]};
     const float* L[3] = {ctx->L32[0].as<float>(), ctx->L32[1].as<float>(), ctx->L32[2].as<float>()};
-    return debug_core<float, double, double>(ctx, Af, Av, F, ctx->inv64.as<double>(), L, r, out);
+    return debug_core<float, double, double, float>(ctx, Af, Av, F, ctx->inv64.as<double>(), L, r, out);
   }
 }
 

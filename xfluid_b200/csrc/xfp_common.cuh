@@ -73,8 +73,9 @@ struct SweepCtl {
 // kernels give it (line-based and cell-based grids, consecutive per scene).
 struct BatchSeg {
   int ni, nj, nk;
-  int blk_lines, blk_lines_start;   // line-based kernels (SpMV)
+  int blk_lines, blk_lines_start;   // line-based kernels (residual)
   int blk_cells, blk_cells_start;   // cell-based kernels (updates, norms)
+  int blk_groups, blk_groups_start; // the SpMV (one thread per 4-cell group)
   int pad;
   long long base, M;
   const Line* lines;
@@ -152,6 +153,25 @@ __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, 
 __device__ __forceinline__ double rsqrt_ref(double x) { return __ddiv_rn(1.0, __dsqrt_rn(x)); }
 __device__ __forceinline__ float rsqrt_ref(float x) { return __fdiv_rn(1.0f, __fsqrt_rn(x)); }
 
+// One group of XFP_ALIGN (4) consecutive cells of an array, from/to a
+// group-aligned index: one 16-byte access (FP32) or two (FP64).  Groups of 8
+// with 32-byte accesses were measured too in the sweeps: faster on long full
+// lines, slower on the 256^3 blob scene (more padding steps, more registers).
+__device__ __forceinline__ void ldg(float (&v)[4], const float* p) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ldg(double (&v)[4], const double* p) {
+  const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void stg(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void stg(double* p, const double (&v)[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
 template <typename T>
 __device__ __forceinline__ T shfl_up(T v, int d) { return __shfl_up_sync(XFP_FULL, v, d); }
 template <typename T>

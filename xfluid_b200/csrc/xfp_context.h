@@ -55,7 +55,7 @@ struct xfp_ctx {
   // I/O staging (host-pointer mode)
   DevBuf io_mat, io_u, io_v, io_w, io_wu, io_wv, io_ww, io_p, io_gu, io_gv, io_gw;
   // layout
-  DevBuf lines, lens, tile_active, tiles, counters, cell_line;
+  DevBuf lines, lens, tile_active, tiles, counters, cell_line, group_line;
   // compact arrays
   DevBuf A64[5];                  // diag, ax, ay, az, b (FP64)
   DevBuf A32[5];                  // same in FP32
@@ -93,6 +93,9 @@ struct xfp_ctx {
   // device timing of the triangular-solve sweeps (pairs of events, read at the end)
   std::vector<cudaEvent_t> sweep_ev;
   int sweep_ev_used = 0;
+  // per timed sweep launch (event pair): 1 when it did work, 0 for the
+  // launches a PCG loop issues after convergence (they return at once)
+  std::vector<char> sweep_work;
   long long launches = 0;
   // batched scenes (xfp_project_batch_*): buffers, tables and tuning cache
   xfp_host::BatchState* batch = nullptr;

@@ -87,7 +87,8 @@ int solve_max_grid(int op, int nw);
   int sweep_max_grid(int op, const SweepData<VT, IT, CT>& d, int nw);
 XFP_SWEEP_DECL(double, double, double)
 XFP_SWEEP_DECL(float, float, float)
-XFP_SWEEP_DECL(float, double, double)
+XFP_SWEEP_DECL(float, double, double)   // mixed form: factorisation only
+XFP_SWEEP_DECL(float, float, double)    // mixed form: triangular solves only
 #undef XFP_SWEEP_DECL
 
 // ---- sweep layout (xfp_swlayout.cu) ----
@@ -155,14 +156,17 @@ cudaError_t rhs_T(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww, 
                   const FT* gw, FT* du, FT* dv, FT* dw, cudaStream_t st);
 
 // PCG vector kernels over the compact arrays (length M).
-// z = A s with the fused dot s.z; one thread per stored cell (cell_line maps a
-// cell to its line).
+// z = A s with the fused dot s.z; one thread per aligned 4-cell group
+// (group_line maps a group to its line).
 template <typename VT, typename AT, typename DT>
 cudaError_t spmv_dot(const AT* diag, const AT* ax, const AT* ay, const AT* az, const VT* s, VT* z,
-                     const Line* lines, const int* cell_line, int nj, int nk, long long M, PcgScalars* sc,
+                     const Line* lines, const int* group_line, int nj, int nk, long long M, PcgScalars* sc,
                      DT* partials, int nblk_max, int mode, cudaStream_t st);
-// cell_line[c] = index of the line storing cell c (for every cell of every line).
-cudaError_t build_cell_line(const Line* lines, long long nlines, int* cell_line, cudaStream_t st);
+// SpMV blocks for M stored cells (the batch gives each scene the same count).
+long long spmv_block_count(long long M, int nblk_max);
+// cell_line[c] = index of the line storing cell c (for every cell of every
+// line); group_line[c / 4] the same per aligned 4-cell group.
+cudaError_t build_cell_line(const Line* lines, long long nlines, int* cell_line, int* group_line, cudaStream_t st);
 // rsw/perm (optional): the updated r is also stored at rsw[perm[c]].
 template <typename VT, typename DT>
 cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgScalars* sc,
@@ -187,7 +191,7 @@ cudaError_t copy_vec(const T* in, T* out, long long n, cudaStream_t st);
 // nseg scenes, per-scene scalars sc[nseg]); grid = the table's total blocks ----
 template <typename VT, typename AT, typename DT>
 cudaError_t batch_spmv_dot(const BatchSeg* segs, int nseg, int blocks, const AT* diag, const AT* ax,
-                           const AT* ay, const AT* az, const VT* s, VT* z, const int* cell_line, PcgScalars* sc,
+                           const AT* ay, const AT* az, const VT* s, VT* z, const int* group_line, PcgScalars* sc,
                            int mode, cudaStream_t st);
 // rsw/perm, zsw/perm (optional): as update_xr / update_s, perm indexed by global cell
 template <typename VT>

@@ -10,10 +10,15 @@
 //
 // The kernel is a variant of the solve's |b|_inf reduction: instead of reading
 // the assembled right-hand side from the context's scratch pool, each thread
-// forms b for its cells straight from material/u/v/w (same operation order as
-// the assembly kernel, so the FP64 result equals xfp_solve_f64's
-// stats.b_inf bit for bit), and the per-block maxima go to one file-scope
-// __device__ array instead of allocated scratch.
+// forms b for its cells straight from material/u/v/w and the per-block maxima
+// go to one file-scope __device__ array instead of allocated scratch.  b is
+// the variational matrix's right-hand side with no body force, formed in the
+// assembly kernel's operation order, so the result equals bit for bit the
+// stats.b_inf of an FP64 solve with options.matrix = XFP_MATRIX_VARIATIONAL
+// (xfp_solve_f64 / xfp_project_f64).  It is not the b of a normal-matrix solve
+// (which drops solid rows) nor of xfp_project_step_* (which adds force*dt to
+// the faces first).  A NaN anywhere in b makes the result NaN, so a blown-up
+// field is not reported as finite.
 //
 // Limits and sharing:
 //  * the array holds kMaxBlocks block maxima of kCellsPerBlock cells each, so
@@ -25,12 +30,13 @@
 //    and the last block leaves it at zero.  Two calls whose kernels overlap on
 //    the GPU (different streams, or different host threads) race on the array
 //    and may return wrong values: serialise them.
-//  * the first call on a device looks up the array's device address with that
-//    device current and clears the counter synchronously; make that first call
-//    before any stream capture begins.
+//  * every call looks up the array's device address with cudaGetSymbolAddress
+//    in the current device's context (a lookup, no allocation), so the address
+//    stays right after a cudaDeviceReset re-creates the context.  The first
+//    call on a device also loads this file's device code into the context;
+//    make that first call before any stream capture begins.
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 
 #include "xfp.h"
 #include "xfp_common.cuh"
@@ -44,7 +50,6 @@ constexpr int kCellsPerThread = 64;
 constexpr long long kCellsPerBlock = (long long)kThreads * kCellsPerThread;  // 16384
 constexpr int kMaxBlocks = 16384;
 constexpr long long kMaxCells = kCellsPerBlock * kMaxBlocks;  // 2^28
-constexpr int kMaxDevices = 64;
 
 struct RhsInfScratch {
   double block_max[kMaxBlocks];  // one partial per block, written before `done` counts it
@@ -59,6 +64,9 @@ struct RhsInfScratch {
 static __device__ __align__(256) RhsInfScratch g_rhs_inf_scratch;
 
 namespace {
+
+// a max that keeps a NaN from either operand
+__device__ __forceinline__ double nan_max(double a, double b) { return (a > b || a != a) ? a : b; }
 
 __device__ __forceinline__ size_t nu_ix(int ni, int nj, int i, int j, int k) {
   return ((size_t)k * nj + j) * (size_t)(ni + 1) + i;
@@ -129,17 +137,17 @@ __global__ void __launch_bounds__(kThreads) rhs_inf_kernel(
     const int i = (int)(c % ni);
     const long long jk = c / ni;
     const int j = (int)(jk % nj), k = (int)(jk / nj);
-    mx = fmax(mx, fabs(cell_rhs(mat, u, v, w, wu, wv, ww, ni, nj, nk, i, j, k)));
+    mx = nan_max(fabs(cell_rhs(mat, u, v, w, wu, wv, ww, ni, nj, nk, i, j, k)), mx);
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(XFP_FULL, mx, o));
+  for (int o = 16; o > 0; o >>= 1) mx = nan_max(mx, __shfl_xor_sync(XFP_FULL, mx, o));
   __shared__ double s_warp[kThreads / 32];
   __shared__ bool s_last;
   if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = mx;
   __syncthreads();
   if (threadIdx.x == 0) {
     double t = 0.0;
-    for (int q = 0; q < kThreads / 32; ++q) t = fmax(t, s_warp[q]);
+    for (int q = 0; q < kThreads / 32; ++q) t = nan_max(t, s_warp[q]);
     scratch->block_max[blockIdx.x] = t;
     __threadfence();
     s_last = atomicAdd(&scratch->done, 1u) == gridDim.x - 1;
@@ -150,21 +158,18 @@ __global__ void __launch_bounds__(kThreads) rhs_inf_kernel(
   __threadfence();
   double t = 0.0;
   for (int q = threadIdx.x; q < (int)gridDim.x; q += kThreads)
-    t = fmax(t, *(volatile const double*)&scratch->block_max[q]);
+    t = nan_max(t, *(volatile const double*)&scratch->block_max[q]);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(XFP_FULL, t, o));
+  for (int o = 16; o > 0; o >>= 1) t = nan_max(t, __shfl_xor_sync(XFP_FULL, t, o));
   if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = t;
   __syncthreads();
   if (threadIdx.x == 0) {
     double r = 0.0;
-    for (int q = 0; q < kThreads / 32; ++q) r = fmax(r, s_warp[q]);
+    for (int q = 0; q < kThreads / 32; ++q) r = nan_max(r, s_warp[q]);
     *b_inf = r;
     scratch->done = 0;  // leave the counter ready for the next call
   }
 }
-
-std::mutex g_setup_mu;
-RhsInfScratch* g_scratch_ptr[kMaxDevices] = {};
 
 int report(char* err, size_t err_len, int rc, const char* msg) {
   if (err && err_len) snprintf(err, err_len, "%s", msg);
@@ -207,7 +212,7 @@ extern "C" int xfp_rhs_inf_noalloc_f64(int ni, int nj, int nk, const uint8_t* ma
   if ((wu == nullptr) != (wv == nullptr) || (wu == nullptr) != (ww == nullptr))
     return report(err, err_len, XFP_ERR_ARGS, "face weights: pass all three or none");
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
     cudaGetLastError();
     return report(err, err_len, XFP_ERR_CUDA, "no usable current CUDA device");
   }
@@ -216,23 +221,17 @@ extern "C" int xfp_rhs_inf_noalloc_f64(int ni, int nj, int nk, const uint8_t* ma
     if (!on_device(p, dev))
       return report(err, err_len, XFP_ERR_ARGS,
                     "every array must be device (or managed) memory on the current device");
-  RhsInfScratch* scratch;
-  {
-    std::lock_guard<std::mutex> lock(g_setup_mu);
-    scratch = g_scratch_ptr[dev];
-    if (!scratch) {
-      void* p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_rhs_inf_scratch);
-      if (e == cudaSuccess) e = cudaMemset(&static_cast<RhsInfScratch*>(p)->done, 0, sizeof(unsigned int));
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        char msg[160];
-        snprintf(msg, sizeof msg, "set-up of the fixed scratch failed: %s", cudaGetErrorString(e));
-        return report(err, err_len, XFP_ERR_CUDA, msg);
-      }
-      scratch = g_scratch_ptr[dev] = static_cast<RhsInfScratch*>(p);
-    }
+  // The array's address in the current context, looked up on every call: a
+  // context re-created after cudaDeviceReset maps the array elsewhere.
+  void* sym = nullptr;
+  cudaError_t se = cudaGetSymbolAddress(&sym, g_rhs_inf_scratch);
+  if (se != cudaSuccess || sym == nullptr) {
+    cudaGetLastError();
+    char msg[160];
+    snprintf(msg, sizeof msg, "looking up the fixed scratch failed: %s", cudaGetErrorString(se));
+    return report(err, err_len, XFP_ERR_CUDA, msg);
   }
+  RhsInfScratch* scratch = static_cast<RhsInfScratch*>(sym);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(&scratch->done, 0, sizeof(unsigned int), st);
   if (e == cudaSuccess) {

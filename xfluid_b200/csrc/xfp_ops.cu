@@ -590,14 +590,17 @@ __device__ __forceinline__ bool last_block(PcgScalars* sc, unsigned nblk) {
 // Batch of scenes in one launch: block b belongs to the scene whose range of
 // blocks [start, start + count) holds it; the scene's blocks then run exactly
 // the decomposition a single-scene launch of `count` blocks would.
-__device__ __forceinline__ int batch_scene_of(const BatchSeg* __restrict__ segs, int nseg, bool by_lines) {
+// kind: which block range of the scene a block belongs to (0 cell-based
+// kernels, 1 line-based kernels, 2 the SpMV's 4-cell groups).
+__device__ __forceinline__ int batch_scene_of(const BatchSeg* __restrict__ segs, int nseg, int kind) {
   __shared__ int s_seg;
   if (threadIdx.x == 0) {
     int lo = 0, hi = nseg - 1;
     const int b = (int)blockIdx.x;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      const int start = by_lines ? segs[mid].blk_lines_start : segs[mid].blk_cells_start;
+      const int start = kind == 1 ? segs[mid].blk_lines_start
+                                  : kind == 2 ? segs[mid].blk_groups_start : segs[mid].blk_cells_start;
       if (start <= b) lo = mid; else hi = mid - 1;
     }
     s_seg = lo;
@@ -606,70 +609,98 @@ __device__ __forceinline__ int batch_scene_of(const BatchSeg* __restrict__ segs,
   return s_seg;
 }
 
+// The last block's sum over the nblk per-block partials: partial b goes to
+// thread b mod blockDim, each thread adds its share in increasing b, then the
+// block tree.  The order depends only on nblk and blockDim, so the result is
+// deterministic (and the same for a batch scene as for its single launch).
+// Call from every thread of the block; the result is valid in thread 0.
+template <typename DT>
+__device__ __forceinline__ DT partials_sum(const DT* partials, unsigned nblk, DT* sh) {
+  DT t = DT(0);
+  for (unsigned b = threadIdx.x; b < nblk; b += blockDim.x) t = add_rn(t, ((volatile const DT*)partials)[b]);
+  return block_sum(t, sh);
+}
+
 // ---------------------------------------------------------------------------
 // z = A s (7-point, row order of sparse_matrix.h:264-276: columns c-nn, c-ni,
 // c-1, c, c+1, c+ni, c+nn; absent entries skipped) fused with the partial dot
 // s.z.  mode 0: alpha = rho / (s.z) (pcg_solver.h:269); mode 1: no dot.
-// One thread per stored cell (cell_line gives its line); block partials of the
-// dot are summed in block order by the last block.
+//
+// One thread per aligned group of 4 stored cells.  Lines start at multiples
+// of 4 and hold multiples of 4 cells, so a group never straddles two lines:
+// the thread reads its line once (group_line), loads s and the four
+// coefficient arrays as 16-byte vectors (two for FP64), takes its x
+// neighbours from the vectors (plus one cell either side), and finds its y/z
+// neighbours through the four neighbouring lines' records (shared by every
+// group of the line, so L1 hits).  Per cell the products are added in the
+// reference's column order, so the FP64 result is the reference's.
 // ---------------------------------------------------------------------------
 template <typename VT, typename AT, typename DT>
 __device__ __forceinline__ void spmv_dot_body(
     unsigned bid, unsigned nblk, const AT* __restrict__ diag, const AT* __restrict__ ax,
     const AT* __restrict__ ay, const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
-    const Line* __restrict__ lines, const int* __restrict__ cell_line, int nj, int nk, long long base, long long M,
+    const Line* __restrict__ lines, const int* __restrict__ group_line, int nj, int nk, long long base, long long M,
     PcgScalars* sc, DT* __restrict__ partials, int mode) {
+  static_assert(std::is_same<VT, AT>::value, "the vector and coefficient types agree");
   __shared__ DT sh[32];
   if (sc && *(volatile int*)&sc->done) return;
   DT acc = DT(0);
-  for (long long q = (long long)bid * blockDim.x + threadIdx.x; q < M; q += (long long)nblk * blockDim.x) {
-    const size_t c = (size_t)(base + q);
-    const int line = cell_line[c];
+  const long long G = M >> 2;
+  for (long long q = (long long)bid * blockDim.x + threadIdx.x; q < G; q += (long long)nblk * blockDim.x) {
+    const long long c = base + 4 * q;
+    const int line = group_line[(base >> 2) + q];
     const Line L = lines[line];
-    const int i = L.lo + (int)((long long)c - L.off);
+    const int i0 = L.lo + (int)(c - L.off);
     const int j = line % nj, k = line / nj;
-    VT acc_z = VT(0);
-    const VT dz = (VT)az[c], dy = (VT)ay[c], dx = (VT)ax[c], dd = (VT)diag[c];
-    if (dz != VT(0)) {
-      const Line Lzm = lines[line - nj];
-      acc_z = add_rn(acc_z, mul_rn(dz, s[(size_t)Lzm.off + (i - Lzm.lo)]));
-    }
-    if (dy != VT(0)) {
-      const Line Lym = lines[line - 1];
-      acc_z = add_rn(acc_z, mul_rn(dy, s[(size_t)Lym.off + (i - Lym.lo)]));
-    }
-    if (dx != VT(0)) acc_z = add_rn(acc_z, mul_rn(dx, s[c - 1]));
-    const VT sc_ = s[c];
-    if (dd != VT(0)) acc_z = add_rn(acc_z, mul_rn(dd, sc_));
-    if ((long long)c + 1 < (long long)L.off + L.len) {
-      const VT cx = (VT)ax[c + 1];
-      if (cx != VT(0)) acc_z = add_rn(acc_z, mul_rn(cx, s[c + 1]));
-    }
-    if (j + 1 < nj) {
-      const Line Lyp = lines[line + 1];
+    VT sv[4], dv[4], xv[4], yv[4], zv[4];
+    ldg(sv, s + c);
+    ldg(dv, diag + c);
+    ldg(xv, ax + c);
+    ldg(yv, ay + c);
+    ldg(zv, az + c);
+    // one cell either side of the group (when the line has it)
+    const VT sl = c > L.off ? s[c - 1] : VT(0);
+    const bool right = c + 4 < (long long)L.off + L.len;
+    const VT sr = right ? s[c + 4] : VT(0);
+    const VT xr = right ? ax[c + 4] : VT(0);
+    const Line Z = {0, 0, 0, 0};
+    const Line Lym = j > 0 ? lines[line - 1] : Z;
+    const Line Lyp = j + 1 < nj ? lines[line + 1] : Z;
+    const Line Lzm = k > 0 ? lines[line - nj] : Z;
+    const Line Lzp = k + 1 < nk ? lines[line + nj] : Z;
+    VT out[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int i = i0 + e;
+      VT a = VT(0);
+      // a nonzero lower coefficient means the neighbour is an unknown, stored in its line
+      if (zv[e] != VT(0)) a = add_rn(a, mul_rn(zv[e], s[(size_t)Lzm.off + (i - Lzm.lo)]));
+      if (yv[e] != VT(0)) a = add_rn(a, mul_rn(yv[e], s[(size_t)Lym.off + (i - Lym.lo)]));
+      if (xv[e] != VT(0)) a = add_rn(a, mul_rn(xv[e], e == 0 ? sl : sv[e == 0 ? 0 : e - 1]));
+      if (dv[e] != VT(0)) a = add_rn(a, mul_rn(dv[e], sv[e]));
+      const VT cx = e < 3 ? xv[e < 3 ? e + 1 : 3] : xr;
+      if (cx != VT(0)) a = add_rn(a, mul_rn(cx, e < 3 ? sv[e < 3 ? e + 1 : 3] : sr));
       if ((unsigned)(i - Lyp.lo) < (unsigned)Lyp.len) {
         const size_t n = (size_t)Lyp.off + (i - Lyp.lo);
-        const VT cy = (VT)ay[n];
-        if (cy != VT(0)) acc_z = add_rn(acc_z, mul_rn(cy, s[n]));
+        const VT cy = ay[n];
+        if (cy != VT(0)) a = add_rn(a, mul_rn(cy, s[n]));
       }
-    }
-    if (k + 1 < nk) {
-      const Line Lzp = lines[line + nj];
       if ((unsigned)(i - Lzp.lo) < (unsigned)Lzp.len) {
         const size_t n = (size_t)Lzp.off + (i - Lzp.lo);
-        const VT cz = (VT)az[n];
-        if (cz != VT(0)) acc_z = add_rn(acc_z, mul_rn(cz, s[n]));
+        const VT cz = az[n];
+        if (cz != VT(0)) a = add_rn(a, mul_rn(cz, s[n]));
       }
+      out[e] = a;
+      if (mode == 0) acc = add_rn(acc, mul_rn((DT)sv[e], (DT)a));
     }
-    z[c] = acc_z;
-    if (mode == 0) acc = add_rn(acc, mul_rn((DT)sc_, (DT)acc_z));
+    stg(z + c, out);
   }
   if (mode != 0) return;
   DT t = block_sum(acc, sh);
   if (threadIdx.x == 0) partials[bid] = t;
-  if (last_block(sc, nblk) && threadIdx.x == 0) {
-    DT tot = DT(0);
-    for (unsigned b = 0; b < nblk; ++b) tot = add_rn(tot, ((volatile DT*)partials)[b]);
+  if (!last_block(sc, nblk)) return;   // uniform over the block
+  const DT tot = partials_sum(partials, nblk, sh);
+  if (threadIdx.x == 0) {
     if (std::is_same<DT, float>::value)
       sc->alpha = (double)__fdiv_rn((float)sc->rho, (float)tot);
     else
@@ -677,33 +708,38 @@ __device__ __forceinline__ void spmv_dot_body(
     sc->red_count = 0;
   }
 }
+// Blocks of the SpMV for M stored cells (one thread per 4-cell group); a batch
+// gives each scene the same count, so its reduction order is the single one's.
+long long spmv_block_count(long long M, int nblk_max) {
+  const long long b = ((M >> 2) + 255) / 256;
+  return b < 1 ? 1 : (b < nblk_max ? b : nblk_max);
+}
 template <typename VT, typename AT, typename DT>
 __global__ void __launch_bounds__(256) spmv_dot_kernel(
     const AT* __restrict__ diag, const AT* __restrict__ ax, const AT* __restrict__ ay,
     const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
-    const Line* __restrict__ lines, const int* __restrict__ cell_line, int nj, int nk, long long M, PcgScalars* sc,
+    const Line* __restrict__ lines, const int* __restrict__ group_line, int nj, int nk, long long M, PcgScalars* sc,
     DT* __restrict__ partials, int mode) {
-  spmv_dot_body<VT, AT, DT>(blockIdx.x, gridDim.x, diag, ax, ay, az, s, z, lines, cell_line, nj, nk, 0, M, sc,
+  spmv_dot_body<VT, AT, DT>(blockIdx.x, gridDim.x, diag, ax, ay, az, s, z, lines, group_line, nj, nk, 0, M, sc,
                             partials, mode);
 }
 template <typename VT, typename AT, typename DT>
 __global__ void __launch_bounds__(256) batch_spmv_dot_kernel(
     const BatchSeg* __restrict__ segs, int nseg, const AT* __restrict__ diag, const AT* __restrict__ ax,
     const AT* __restrict__ ay, const AT* __restrict__ az, const VT* __restrict__ s, VT* __restrict__ z,
-    const int* __restrict__ cell_line, PcgScalars* sc, int mode) {
-  const int q = batch_scene_of(segs, nseg, false);
+    const int* __restrict__ group_line, PcgScalars* sc, int mode) {
+  const int q = batch_scene_of(segs, nseg, 2);
   const BatchSeg& S = segs[q];
-  spmv_dot_body<VT, AT, DT>(blockIdx.x - S.blk_cells_start, S.blk_cells, diag, ax, ay, az, s, z, S.lines,
-                            cell_line, S.nj, S.nk, S.base, S.M, sc + q, reinterpret_cast<DT*>(S.partials), mode);
+  spmv_dot_body<VT, AT, DT>(blockIdx.x - S.blk_groups_start, S.blk_groups, diag, ax, ay, az, s, z, S.lines,
+                            group_line, S.nj, S.nk, S.base, S.M, sc + q, reinterpret_cast<DT*>(S.partials), mode);
 }
 template <typename VT, typename AT, typename DT>
 cudaError_t spmv_dot(const AT* diag, const AT* ax, const AT* ay, const AT* az, const VT* s, VT* z,
-                     const Line* lines, const int* cell_line, int nj, int nk, long long M, PcgScalars* sc,
+                     const Line* lines, const int* group_line, int nj, int nk, long long M, PcgScalars* sc,
                      DT* partials, int nblk_max, int mode, cudaStream_t st) {
-  int blocks = (int)std::min<long long>((M + 255) / 256, (long long)nblk_max);
-  if (blocks < 1) blocks = 1;
+  const int blocks = (int)spmv_block_count(M, nblk_max);
   ++g_kernel_launches;
-  spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(diag, ax, ay, az, s, z, lines, cell_line, nj, nk, M, sc,
+  spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(diag, ax, ay, az, s, z, lines, group_line, nj, nk, M, sc,
                                                      partials, mode);
   return cudaGetLastError();
 }
@@ -722,6 +758,11 @@ template cudaError_t spmv_dot<float, float, double>(const float*, const float*, 
 // x += alpha s ; r += (-alpha) z ; |r|_inf  (pcg_solver.h:270-276).  The last
 // block decides convergence: |r|_inf <= tol*|b|_inf, or the iteration cap.
 // ---------------------------------------------------------------------------
+//
+// One thread per aligned 4-cell group, with 16-byte vector accesses (two for
+// FP64).  With a sweep layout the group's four cells sit at four consecutive
+// sweep-layout elements (consecutive forward steps, aligned to a group of 4),
+// so r goes there with one vector store at perm[c].
 template <typename VT>
 __device__ __forceinline__ void update_xr_body(unsigned bid, unsigned nblk, VT* __restrict__ x,
                                                VT* __restrict__ r, const VT* __restrict__ s,
@@ -733,12 +774,23 @@ __device__ __forceinline__ void update_xr_body(unsigned bid, unsigned nblk, VT* 
   const VT alpha = (VT)sc->alpha;
   const VT nalpha = -alpha;
   double m = 0.0;
-  for (long long c = (long long)bid * blockDim.x + threadIdx.x; c < M; c += (long long)nblk * blockDim.x) {
-    x[c] = add_rn(x[c], mul_rn(alpha, s[c]));
-    const VT rv = add_rn(r[c], mul_rn(nalpha, z[c]));
-    r[c] = rv;
-    if (rsw != nullptr) rsw[perm[c]] = rv;
-    m = fmax(m, (double)fabs(rv));
+  const long long G = M >> 2;
+  for (long long q = (long long)bid * blockDim.x + threadIdx.x; q < G; q += (long long)nblk * blockDim.x) {
+    const long long c = 4 * q;
+    VT xv[4], rv[4], sv[4], zv[4];
+    ldg(xv, x + c);
+    ldg(rv, r + c);
+    ldg(sv, s + c);
+    ldg(zv, z + c);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      xv[e] = add_rn(xv[e], mul_rn(alpha, sv[e]));
+      rv[e] = add_rn(rv[e], mul_rn(nalpha, zv[e]));
+      m = fmax(m, (double)fabs(rv[e]));
+    }
+    stg(x + c, xv);
+    stg(r + c, rv);
+    if (rsw != nullptr) stg(rsw + perm[c], rv);
   }
   double t = block_max(m, sh);
   if (threadIdx.x == 0) partials[bid] = t;
@@ -771,7 +823,7 @@ __global__ void __launch_bounds__(256) batch_update_xr_kernel(const BatchSeg* __
                                                               const VT* __restrict__ s, const VT* __restrict__ z,
                                                               PcgScalars* sc, VT* __restrict__ rsw,
                                                               const int* __restrict__ perm) {
-  const int q = batch_scene_of(segs, nseg, false);
+  const int q = batch_scene_of(segs, nseg, 0);
   const BatchSeg& S = segs[q];
   update_xr_body<VT>(blockIdx.x - S.blk_cells_start, S.blk_cells, x + S.base, r + S.base, s + S.base,
                      z + S.base, S.M, sc + q, S.partials, rsw, perm ? perm + S.base : nullptr);
@@ -792,7 +844,9 @@ template cudaError_t update_xr<float, float>(float*, float*, const float*, const
 template cudaError_t update_xr<float, double>(float*, float*, const float*, const float*, long long,
                                               PcgScalars*, double*, int, cudaStream_t, float*, const int*);
 
-// s = z + beta s  (add_scaled(beta, s, z) then swap, pcg_solver.h:280)
+// s = z + beta s  (add_scaled(beta, s, z) then swap, pcg_solver.h:280); one
+// thread per aligned 4-cell group, z read from the sweep layout at perm[c]
+// (four consecutive elements) when there is one.
 template <typename VT>
 __device__ __forceinline__ void update_s_body(unsigned bid, unsigned nblk, VT* __restrict__ s,
                                               const VT* __restrict__ z, long long M, PcgScalars* sc,
@@ -800,8 +854,16 @@ __device__ __forceinline__ void update_s_body(unsigned bid, unsigned nblk, VT* _
                                               const int* __restrict__ perm = nullptr) {
   if (*(volatile int*)&sc->done) return;
   const VT beta = (VT)sc->beta;
-  for (long long c = (long long)bid * blockDim.x + threadIdx.x; c < M; c += (long long)nblk * blockDim.x)
-    s[c] = add_rn(zsw != nullptr ? zsw[perm[c]] : z[c], mul_rn(beta, s[c]));
+  const long long G = M >> 2;
+  for (long long q = (long long)bid * blockDim.x + threadIdx.x; q < G; q += (long long)nblk * blockDim.x) {
+    const long long c = 4 * q;
+    VT sv[4], zv[4];
+    ldg(sv, s + c);
+    ldg(zv, zsw != nullptr ? zsw + perm[c] : z + c);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) sv[e] = add_rn(zv[e], mul_rn(beta, sv[e]));
+    stg(s + c, sv);
+  }
 }
 template <typename VT>
 __global__ void update_s_kernel(VT* __restrict__ s, const VT* __restrict__ z, long long M,
@@ -812,7 +874,7 @@ template <typename VT>
 __global__ void batch_update_s_kernel(const BatchSeg* __restrict__ segs, int nseg, VT* __restrict__ s,
                                       const VT* __restrict__ z, PcgScalars* sc, const VT* __restrict__ zsw,
                                       const int* __restrict__ perm) {
-  const int q = batch_scene_of(segs, nseg, false);
+  const int q = batch_scene_of(segs, nseg, 0);
   const BatchSeg& S = segs[q];
   update_s_body<VT>(blockIdx.x - S.blk_cells_start, S.blk_cells, s + S.base, z + S.base, S.M, sc + q, zsw,
                     perm ? perm + S.base : nullptr);
@@ -865,7 +927,7 @@ template <typename VT>
 __global__ void batch_absmax_init_kernel(const BatchSeg* __restrict__ segs, int nseg, const VT* __restrict__ b,
                                          PcgScalars* sc, double tol, int maxit, const double* __restrict__ tols,
                                          const int* __restrict__ maxits) {
-  const int q = batch_scene_of(segs, nseg, false);
+  const int q = batch_scene_of(segs, nseg, 0);
   const BatchSeg& S = segs[q];
   absmax_init_body<VT>(blockIdx.x - S.blk_cells_start, S.blk_cells, b + S.base, S.M, sc + q, S.partials,
                        tols ? tols[q] : tol, maxits ? maxits[q] : maxit);
@@ -972,7 +1034,7 @@ __global__ void __launch_bounds__(256) batch_residual64_kernel(
     const BatchSeg* __restrict__ segs, int nseg, const double* __restrict__ diag, const double* __restrict__ ax,
     const double* __restrict__ ay, const double* __restrict__ az, const double* __restrict__ b,
     const double* __restrict__ x, double* __restrict__ r, PcgScalars* sc) {
-  const int q = batch_scene_of(segs, nseg, true);
+  const int q = batch_scene_of(segs, nseg, 1);
   const BatchSeg& S = segs[q];
   residual64_body(blockIdx.x - S.blk_lines_start, S.blk_lines, diag, ax, ay, az, b, x, r, S.lines, S.ni, S.nj,
                   S.nk, sc + q, S.partials);
@@ -1001,10 +1063,10 @@ cudaError_t residual64(const double* diag, const double* ax, const double* ay, c
 // ---------------------------------------------------------------------------
 template <typename VT, typename AT, typename DT>
 cudaError_t batch_spmv_dot(const BatchSeg* segs, int nseg, int blocks, const AT* diag, const AT* ax,
-                           const AT* ay, const AT* az, const VT* s, VT* z, const int* cell_line, PcgScalars* sc,
+                           const AT* ay, const AT* az, const VT* s, VT* z, const int* group_line, PcgScalars* sc,
                            int mode, cudaStream_t st) {
   ++g_kernel_launches;
-  batch_spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(segs, nseg, diag, ax, ay, az, s, z, cell_line, sc,
+  batch_spmv_dot_kernel<VT, AT, DT><<<blocks, 256, 0, st>>>(segs, nseg, diag, ax, ay, az, s, z, group_line, sc,
                                                            mode);
   return cudaGetLastError();
 }
@@ -1019,20 +1081,24 @@ template cudaError_t batch_spmv_dot<float, float, double>(const BatchSeg*, int, 
                                                           const float*, const float*, const float*, float*,
                                                           const int*, PcgScalars*, int, cudaStream_t);
 
-// cell_line[c] = the line (index in its scene's table) that stores cell c.
-__global__ void cell_line_kernel(const Line* __restrict__ lines, long long nlines, int* __restrict__ cell_line) {
+// cell_line[c] = the line (index in its scene's table) that stores cell c;
+// group_line[c / 4] the same for every aligned 4-cell group (lines start at
+// multiples of 4 and hold multiples of 4 cells).
+__global__ void cell_line_kernel(const Line* __restrict__ lines, long long nlines, int* __restrict__ cell_line,
+                                 int* __restrict__ group_line) {
   const int lane = threadIdx.x & 31;
   for (long long line = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); line < nlines;
        line += (long long)gridDim.x * (blockDim.x >> 5)) {
     const Line L = lines[line];
     for (int q = lane; q < L.len; q += 32) cell_line[(size_t)L.off + q] = (int)line;
+    for (int q = lane; q < (L.len >> 2); q += 32) group_line[((size_t)L.off >> 2) + q] = (int)line;
   }
 }
-cudaError_t build_cell_line(const Line* lines, long long nlines, int* cell_line, cudaStream_t st) {
+cudaError_t build_cell_line(const Line* lines, long long nlines, int* cell_line, int* group_line, cudaStream_t st) {
   if (nlines <= 0) return cudaSuccess;
   ++g_kernel_launches;
   cell_line_kernel<<<(unsigned)std::min<long long>((nlines + 7) / 8, 65535LL * 8), 256, 0, st>>>(lines, nlines,
-                                                                                              cell_line);
+                                                                                              cell_line, group_line);
   return cudaGetLastError();
 }
 

@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstring>
 #include <string>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -710,6 +711,53 @@ int distance_field_impl(xfp_ctx* ctx, int ni, int nj, int nk, double dx, int sub
   return XFP_OK;
 }
 
+// FluidSimulator::_maxVelocity (FluidSimulator.cpp:387-400): the largest
+// v.v over the particles, v.v formed as x*x + y*y + z*z left to right with
+// every product and sum rounded (Vec3::operator*, array3d.h:33-36), then its
+// square root.  The max is exact in any order: each block's maximum goes to
+// one 64-bit word by atomicMax on the bit pattern (non-negative doubles order
+// like their bits); NaN speeds propagate as the largest pattern.
+__global__ void max_speed_kernel(const double* __restrict__ p, long long n, unsigned long long* __restrict__ out) {
+  unsigned long long m = 0ull;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const double vx = p[6 * q + 3], vy = p[6 * q + 4], vz = p[6 * q + 5];
+    const double vv = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
+    const unsigned long long b = (unsigned long long)__double_as_longlong(vv);
+    m = b > m ? b : m;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long t = __shfl_xor_sync(0xffffffffu, m, o);
+    m = t > m ? t : m;
+  }
+  if ((threadIdx.x & 31) == 0 && m != 0ull) atomicMax(out, m);
+}
+
+int max_speed_impl(xfp_ctx* ctx, long long n, const xfp_particle* parts, double* max_speed) {
+  if (!ctx) return XFP_ERR_ARGS;
+  if (!max_speed) return fail(ctx, XFP_ERR_ARGS, "max_speed is NULL");
+  if (n < 0 || (n > 0 && !parts)) return fail(ctx, XFP_ERR_ARGS, "bad particle arguments");
+  XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  *max_speed = 0.0;
+  if (n == 0) return XFP_OK;
+  const double* dp;
+  int rc;
+  if ((rc = stage_particles(ctx, parts, n, &dp))) return rc;
+  XFP_CUDA(ctx, ctx->part_tmp.ensure(std::max<size_t>(ctx->part_tmp.cap, 64)));
+  unsigned long long* word = reinterpret_cast<unsigned long long*>(ctx->part_tmp.p);
+  XFP_CUDA(ctx, cudaMemsetAsync(word, 0, sizeof(unsigned long long), ctx->stream));
+  ++g_kernel_launches;
+  max_speed_kernel<<<pgrid(n), 256, 0, ctx->stream>>>(dp, n, word);
+  XFP_CUDA(ctx, cudaGetLastError());
+  unsigned long long h = 0ull;
+  XFP_CUDA(ctx, cudaMemcpyAsync(&h, word, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  double vv;
+  std::memcpy(&vv, &h, sizeof(vv));
+  *max_speed = std::sqrt(vv);
+  return XFP_OK;
+}
+
 }  // namespace xfp_host
 
 using namespace xfp_host;
@@ -727,6 +775,10 @@ int xfp_advect_particles_f64(xfp_ctx* ctx, int ni, int nj, int nk, double dx, co
 int xfp_particles_to_grid_f64(xfp_ctx* ctx, int ni, int nj, int nk, double dx, long long n,
                               const xfp_particle* particles, double* u, double* v, double* w) {
   return particles_to_grid_impl(ctx, ni, nj, nk, dx, n, particles, u, v, w);
+}
+
+int xfp_max_speed_f64(xfp_ctx* ctx, long long n, const xfp_particle* particles, double* max_speed) {
+  return max_speed_impl(ctx, n, particles, max_speed);
 }
 
 int xfp_update_material(xfp_ctx* ctx, int ni, int nj, int nk, double dx, long long n, const xfp_particle* particles,

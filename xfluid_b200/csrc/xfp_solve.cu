@@ -51,26 +51,14 @@ constexpr int SRING = 32;   // loader ring depth (steps)
 constexpr int SLB = 8;      // loader batch: steps polled together
 static_assert(SRING >= SLB + 1, "the loader could wait for a slot the gate cannot free");
 
-// y = t * inv rounded to the solve type.  FP64 and FP32 solves multiply in
-// their own type.  The mixed solve (FP32 values, FP64 inverse pivot) splits the
-// pivot into FP32 parts hi + lo (exact to about 48 bits, split before the
-// step's barrier, off the dependency chain) and forms fma(t, hi, t*lo): within
-// about half an FP32 ulp of the FP64 product, at a fraction of the latency of
-// converting t to FP64, multiplying and converting back.
+// y = t * inv, rounded to the solve type.  The mixed form's solves stream
+// its FP64 pivots rounded to FP32 (the pivots themselves are computed in FP64
+// by the factorisation), so every solve multiplies in its value type.
 template <typename VT, typename IT>
 struct Pivot {
   IT v;
   __device__ __forceinline__ explicit Pivot(IT inv) : v(inv) {}
   __device__ __forceinline__ VT mul(VT t) const { return VT(mul_rn((IT)t, v)); }
-};
-template <>
-struct Pivot<float, double> {
-  float hi, lo;
-  __device__ __forceinline__ explicit Pivot(double inv) {
-    hi = __double2float_rn(inv);
-    lo = __double2float_rn(__dsub_rn(inv, (double)hi));
-  }
-  __device__ __forceinline__ float mul(float t) const { return __fmaf_rn(t, hi, __fmul_rn(t, lo)); }
 };
 
 __device__ __forceinline__ void step_barrier(int nthreads) {
@@ -93,7 +81,8 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
     solve_kernel(SweepGrid g, SweepData<VT, IT, CT> d) {
   constexpr bool REV = (OP == SWEEP_BWD);
   constexpr int P = Words<VT>::P;
-  constexpr bool DOT32 = std::is_same<VT, float>::value && !std::is_same<IT, double>::value;
+  // z.r is accumulated in the dot type: FP32 for the plain FP32 form, FP64 otherwise
+  constexpr bool DOT32 = std::is_same<CT, float>::value;
   constexpr int GATE = NW, LOADER = NW + 1;
   constexpr int NT = (NW + 1) * 32;   // threads at the per-step barrier: compute warps + gate
   constexpr int GS = XFP_ALIGN;
@@ -664,6 +653,6 @@ int solve_max_grid(int op, int nw) {
   template int solve_max_grid<VT, IT, CT>(int, int);
 XFP_SOLVE_INST(double, double, double)
 XFP_SOLVE_INST(float, float, float)
-XFP_SOLVE_INST(float, double, double)
+XFP_SOLVE_INST(float, float, double)
 
 }  // namespace xfp

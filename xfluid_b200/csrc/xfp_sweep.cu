@@ -602,6 +602,24 @@ static int max_grid_op(int nw) {
 
 XFP_SWEEP_INST(double, double, double)
 XFP_SWEEP_INST(float, float, float)
-XFP_SWEEP_INST(float, double, double)
+
+// The mixed form: the factorisation runs with FP32 L and FP64 pivots
+// (float, double, double) and the triangular solves stream FP32 L and the
+// pivots rounded to FP32, with FP64 dots (float, float, double).
+cudaError_t sweep_launch(int op, const SweepGrid& g, const SweepData<float, double, double>& d, int nw, int grid,
+                         cudaStream_t st) {
+  return op == SWEEP_FACTOR ? launch_op<SWEEP_FACTOR, float, double, double>(g, d, nw, grid, st)
+                            : cudaErrorInvalidValue;
+}
+int sweep_max_grid(int op, const SweepData<float, double, double>&, int nw) {
+  return op == SWEEP_FACTOR ? max_grid_op<SWEEP_FACTOR, float, double, double>(nw) : 0;
+}
+cudaError_t sweep_launch(int op, const SweepGrid& g, const SweepData<float, float, double>& d, int nw, int grid,
+                         cudaStream_t st) {
+  return op == SWEEP_FACTOR ? cudaErrorInvalidValue : solve_launch<float, float, double>(op, g, d, nw, grid, st);
+}
+int sweep_max_grid(int op, const SweepData<float, float, double>&, int nw) {
+  return op == SWEEP_FACTOR ? 0 : solve_max_grid<float, float, double>(op, nw);
+}
 
 }  // namespace xfp

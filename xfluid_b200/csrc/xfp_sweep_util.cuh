@@ -80,25 +80,6 @@ __device__ __forceinline__ void st_gpu64(unsigned long long* p, unsigned long lo
 }
 
 
-// One group of XFP_ALIGN (4) consecutive cells of an array, from/to a
-// group-aligned index: one 16-byte access (FP32) or two (FP64).  Groups of 8
-// with 32-byte accesses were measured too: faster on long full lines, slower
-// on the 256^3 blob scene (more padding steps, more registers).
-__device__ __forceinline__ void ldg(float (&v)[4], const float* p) {
-  const float4 t = *reinterpret_cast<const float4*>(p);
-  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-}
-__device__ __forceinline__ void ldg(double (&v)[4], const double* p) {
-  const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
-  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-}
-__device__ __forceinline__ void stg(float* p, const float (&v)[4]) {
-  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-}
-__device__ __forceinline__ void stg(double* p, const double (&v)[4]) {
-  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
-  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
-}
 struct Spin {
   long long n = 0;
   __device__ __forceinline__ bool step(const SweepCtl* ctl, long long limit) {
