@@ -3,10 +3,14 @@
 
 Workload (the standalone-projection configuration): a 256^3 MAC grid whose fluid
 mask is 32 seeded Gaussian blobs (sigma ~ U[0.03,0.12]) thresholded at 0.5, a
-random box obstacle covering 10% of the volume with fractional face weights, a
-solid border and U[-1,1] FP32 face velocities (xfluid_b200.scenes.blob_scene,
-seed 3).  One step = one projection: layout + assembly, MIC(0) factorisation,
-PCG to |r|_inf <= 1e-6 |b|_inf, pressure scatter and velocity update.
+random box obstacle covering 10% of the volume, a solid border and U[-1,1] FP32
+face velocities (xfluid_b200.scenes.blob_scene, seed 3).  The headline solves
+xFluid's own matrix on it (no fractional face weights), the same computation
+the reference arm times, so the two arms' figures compare like for like; the
+same scene with the obstacle's fractional face weights is timed beside it
+(forms.fractional_faces_mixed).  One step = one projection: layout + assembly,
+MIC(0) factorisation, PCG to |r|_inf <= 1e-6 |b|_inf, pressure scatter and
+velocity update.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -48,8 +52,9 @@ SEED = 3
 
 
 def workload_config(n, rows=None, iters=None):
-    cfg = {"workload": f"blob scene {n}^3 (32 Gaussian blobs, 10% box obstacle with fractional faces, "
-                       f"U[-1,1] FP32 faces, seed {SEED}); tol 1e-6 relative inf-norm",
+    cfg = {"workload": f"blob scene {n}^3 (32 Gaussian blobs, 10% box obstacle, U[-1,1] FP32 faces, seed {SEED}), "
+                       f"xFluid's variational matrix (the obstacle's fractional face weights: "
+                       f"forms.fractional_faces_mixed); tol 1e-6 relative inf-norm",
            "grid": [n, n, n], "tol": TOL, "l2": "inputs larger than L2: a distinct input copy per step"}
     if rows is not None:
         cfg["rows"] = rows
@@ -110,25 +115,33 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------- CPU baseline
-def cpu_project_seconds(sc):
-    """One projection of the scene by xFluid's own CPU solver when it was built
-    (oracle/_ref), else by the oracle's C port.  Returns (seconds, kind)."""
+def cpu_project_seconds(sc, keep=False):
+    """One projection of the scene (xFluid's matrix: no face weights) by
+    xFluid's own CPU solver when it was built (oracle/_ref): its solve and its
+    applyPressure, single-threaded; else by the oracle's C port.  Returns
+    (seconds, kind), and with keep=True also the reference's result
+    {p, iters, u, v, w}."""
     import oracle
-    s64 = sc.astype(np.float64)
+    s64 = sc.astype(np.float64).reference_mode()
     if oracle.reference_available():
         R = oracle.Reference()
         before = R.set_threads(1)   # the single-core figure: applyPressure's OpenMP loop on one thread
         try:
             t = time.perf_counter()
-            R.project(s64.reference_mode(), tol=TOL, maxit=MAXIT)
-            return time.perf_counter() - t, "reference"
+            sol = R.solve(s64, tol=TOL, maxit=MAXIT)
+            u, v, w = R.apply(s64, sol["p"])
+            sec = time.perf_counter() - t
         finally:
             R.set_threads(before)
+        out = {"p": sol["p"], "iters": sol["iters"], "u": u, "v": v, "w": w}
+        return (sec, "reference", out) if keep else (sec, "reference")
     oracle.build_oracle()
     O = oracle.Oracle()
     t = time.perf_counter()
-    O.project(s64, tol=TOL, maxit=MAXIT)
-    return time.perf_counter() - t, "port"
+    res = O.project(s64, tol=TOL, maxit=MAXIT)
+    sec = time.perf_counter() - t
+    out = {"p": res["p"], "iters": res["iters"], "u": res["u"], "v": res["v"], "w": res["w"]}
+    return (sec, "port", out) if keep else (sec, "port")
 
 
 def cpu_apply_pressure(sc):
@@ -152,24 +165,59 @@ def cpu_apply_pressure(sc):
 def _ref_worker(conn, n):
     from xfluid_b200 import scenes
     sc = scenes.blob_scene(n, seed=SEED, dtype=np.float32)
+    small = scenes.blob_scene(64, seed=SEED, dtype=np.float32)
     conn.send("ready")
     while True:
         msg = conn.recv()
         if msg == "stop":
             break
-        sec, kind = cpu_project_seconds(sc)
+        sec, kind = cpu_project_seconds(small if msg == "warm" else sc)
         conn.send((sec, kind))
 
 
+REF_PROC_BYTES = 4.5e9   # peak host memory of one 256^3 reference projection (measured 3.7 GB) plus margin
+
+
+def reference_processes(n):
+    """How many reference projections run at once: one per usable host core,
+    unless host memory holds fewer (each 256^3 projection peaks near 3.7 GB:
+    xFluid's row-list matrix spans every cell).  Returns (processes, cores,
+    reason or None)."""
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    need = REF_PROC_BYTES * (n / 256.0) ** 3
+    avail = None
+    try:
+        for line in Path("/proc/meminfo").read_text().splitlines():
+            if line.startswith("MemAvailable:"):
+                avail = float(line.split()[1]) * 1024
+    except OSError:
+        pass
+    if avail is None:
+        return cores, cores, None
+    by_mem = max(1, int(0.8 * avail // need))
+    if by_mem < cores:
+        return by_mem, cores, (f"host memory: {avail / 1e9:.0f} GB available holds {by_mem} concurrent "
+                               f"{n}^3 projections at ~{need / 1e9:.1f} GB each")
+    return cores, cores, None
+
+
 def reference_arm(args, rank, world):
-    """xFluid's CPU solver on every usable host core, one projection per core per step."""
+    """xFluid's CPU solver on every usable host core: one process per core, each
+    running whole projections.  A timed step is a round in which every process
+    completes one projection; ceil(K / processes) rounds are timed, so the run
+    stays within a few minutes on a many-core host while every core works.
+    Warm-up rounds project the 64^3 scene (code and allocator warm-up; the
+    reference has nothing to compile)."""
     import multiprocessing as mp
     if rank != 0:
         return
-    cores = min(os.cpu_count() or 1, 16)
+    nproc, cores, why = reference_processes(args.n)
     ctxmp = mp.get_context("spawn")
     pipes, procs = [], []
-    for _ in range(cores):
+    for _ in range(nproc):
         a, b = ctxmp.Pipe()
         p = ctxmp.Process(target=_ref_worker, args=(b, args.n), daemon=True)
         p.start()
@@ -179,31 +227,40 @@ def reference_arm(args, rank, world):
         a.recv()
     kinds = set()
 
-    def step():
+    def step(msg="go"):
         for a in pipes:
-            a.send("go")
+            a.send(msg)
         res = [a.recv() for a in pipes]
         kinds.update(k for _, k in res)
+        return [sec for sec, _ in res]
 
-    for _ in range(args.warmup):
-        step()
+    for _ in range(max(1, args.warmup)):
+        step("warm")
+    rounds = max(1, -(-args.steps // nproc))
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
+    per = []
+    for _ in range(rounds):
+        per += step()
     el = time.perf_counter() - t0
     for a in pipes:
         a.send("stop")
     for p in procs:
         p.join(timeout=30)
-    value = cores * args.steps / el
+    done = nproc * rounds
+    value = done / el
     kind = "reference" if kinds == {"reference"} else "port"
-    sample = (f"{cores} processes, each one full {args.n}^3 projection per step (assemble + MIC(0)-PCG to "
-              f"1e-6 + applyPressure), same seeded scene without fractional face weights (xFluid has none)")
+    sample = (f"{nproc} processes on {cores} usable host cores, {rounds} round(s) of one full {args.n}^3 "
+              f"projection per process ({done} projections; assemble + MIC(0)-PCG to 1e-6 + applyPressure, "
+              f"{statistics.median(per):.1f} s median each), same seeded scene as the GPU arm's headline "
+              f"(xFluid's matrix: no fractional face weights)")
+    cpu = {"value": value, "unit": UNIT, "cores": nproc, "host_cores": cores, "kind": kind, "sample": sample}
+    if why:
+        cpu["fewer_processes_than_cores"] = why
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)", "config": workload_config(args.n),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -222,6 +279,128 @@ def sweep_traffic_per_row():
             except ValueError:
                 return None
     return None
+
+
+FULL_FIXTURE = ROOT / "tests" / "golden" / "full_blob256.npz"
+
+
+def stall_cases(args, stream, ctx_for, project_dev, mat, vel0):
+    """Where the mixed form earns its keep: cases in which plain FP32 PCG needs
+    many more iterations, or stalls, before reaching the accuracy the mixed
+    form reaches.  Each case times one projection per form (after one
+    untimed), reports iterations, status and the pressure's relative L2
+    error against an FP64 solve of the same system to tol 1e-12 (the FP64
+    path follows the reference's operation order), and the mixed form's
+    speed over plain FP32.
+      blob_tol_1e-8  the headline scene at tol 1e-8;
+      dam_256_tol_1e-6  the 256^3 dam break (fluid x < 0.4, y < 0.5, solid
+                        border, the first step's gravity impulse), tol 1e-6
+                        (the reference needs 125 iterations here)."""
+    import torch
+    from xfluid_b200 import scenes
+    cases = {}
+    dam = scenes.dam_break(args.n, seed=1, dtype=np.float32) if args.n >= 64 else None
+    specs = [("blob_tol_1e-8", mat, vel0, 1e-8)]
+    if dam is not None:
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+        specs.append(("dam_256_tol_1e-6" if args.n == 256 else f"dam_{args.n}_tol_1e-6",
+                      torch.from_numpy(dam.mat).cuda(), [t(a) for a in (dam.u, dam.v, dam.w)], 1e-6))
+    for name, m, v0, tol in specs:
+        shape = tuple(m.shape)
+
+        def run(prec, tol_, reps, maxit=MAXIT):
+            c = ctx_for(prec, 1)
+            o = c.opts
+            o.tol, o.max_iter = tol_, maxit
+            c.set_options(o)
+            p = torch.zeros(shape, dtype=torch.float32, device="cuda")
+            ms, st = None, None
+            try:
+                for k in range(reps):
+                    vel = [a.clone() for a in v0]
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    _, st = project_dev(c, vel, p, m=m)
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    ms = e0.elapsed_time(e1)
+            finally:
+                c.close()
+            return p.double(), ms, st
+
+        pe, _, _ = run("f64", 1e-12, 1, maxit=20000)
+        entry = {"tol": tol}
+        for prec in ("f32", "mixed"):
+            p, ms, st = run(prec, tol, 2)
+            entry["plain_f32" if prec == "f32" else "mixed"] = {
+                "projections_per_s": 1000.0 / ms, "iterations": int(st["iterations"]), "status": int(st["status"]),
+                "refinements": int(st["refinements"]),
+                "pressure_rel_l2_vs_fp64_exact": float(torch.linalg.norm(p - pe) / torch.linalg.norm(pe))}
+        entry["mixed_over_plain_f32"] = entry["mixed"]["projections_per_s"] / entry["plain_f32"]["projections_per_s"]
+        cases[name] = entry
+    return cases
+
+
+
+
+
+def parity_report(sc, kind, ref, gpu):
+    """The GPU forms' results on the headline scene against xFluid's own solver
+    run on the same scene at the same tolerance (the CPU-baseline leg's
+    projection): pressure and projected-velocity relative L2, iterations, and
+    both divergence figures after the projection -- the m-weighted one the
+    projection drives to tol * |b|_inf (per cell it equals b - A p) and the
+    reference's own unweighted diagnostic (variational_pressuresolver.cpp:
+    526-597, which leaves solid faces out).  The convergence error against the
+    exact solution (the reference solved to 1e-12, committed as a sample in
+    tests/golden/full_blob256.npz for the 256^3 scene) is reported separately
+    from the precision error."""
+    import oracle
+    from xfluid_b200 import scenes  # noqa: F401
+    oracle.build_oracle()
+    O = oracle.Oracle()
+    s64 = sc.astype(np.float64).reference_mode()
+    b_inf = float(np.abs(O.assemble(s64)["b"]).max())
+    ref_vel = np.concatenate([a.ravel() for a in (ref["u"], ref["v"], ref["w"])])
+    exact = None
+    if FULL_FIXTURE.exists():
+        import hashlib
+        g = np.load(FULL_FIXTURE)
+        h = hashlib.sha256()
+        for a in (sc.mat, sc.u, sc.v, sc.w):
+            h.update(np.ascontiguousarray(a).tobytes())
+        if int(g["n"]) == sc.ni and h.hexdigest() == str(g["digest"]):
+            exact = (g["idx_p"], g["pe"])
+
+    def rl2(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    def divs(u, v, w):
+        dw = O.weighted_divergence(s64, u, v, w)
+        du = O.divergence_ref(s64, u, v, w)
+        return {"weighted_div_inf_over_b_inf": float(np.abs(dw).max()) / b_inf,
+                "unweighted_div_inf": float(np.abs(du).max())}
+
+    out = {"scene": "the headline scene, xFluid's matrix", "tol": TOL,
+           "reference": dict({"kind": kind, "iterations": int(ref["iters"])},
+                             **divs(ref["u"], ref["v"], ref["w"]))}
+    if exact is not None:
+        idx, pe = exact
+        out["reference"]["pressure_rel_l2_vs_exact_sample"] = rl2(ref["p"].ravel()[idx], pe)
+    for name, r in gpu.items():
+        p = r["p"].double().cpu().numpy()
+        u, v, w = (a.double().cpu().numpy() for a in r["vel"])
+        e = {"iterations": int(r["iterations"]),
+             "iterations_vs_reference": int(r["iterations"]) - int(ref["iters"]),
+             "pressure_rel_l2_vs_reference": rl2(p, ref["p"]),
+             "velocity_rel_l2_vs_reference": rl2(np.concatenate([u.ravel(), v.ravel(), w.ravel()]), ref_vel),
+             "rel_residual_reported": float(r["rel_residual"])}
+        if exact is not None:
+            e["pressure_rel_l2_vs_exact_sample"] = rl2(p.ravel()[idx], pe)
+        e.update(divs(u, v, w))
+        out[name] = e
+    return out
 
 
 def ours(args, rank, world):
@@ -251,16 +430,17 @@ def ours(args, rank, world):
 
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
     mat = t(sc.mat)
-    wts = [t(a) for a in (sc.wu, sc.wv, sc.ww)]
+    wts = [t(a) for a in (sc.wu, sc.wv, sc.ww)]   # the obstacle's fractional face weights (their own form)
     nsteps = args.steps + args.warmup
     vel0 = [t(a) for a in (sc.u, sc.v, sc.w)]
     copies = [[a.clone() for a in vel0] for _ in range(nsteps)]
     pres = torch.zeros((nk, nj, ni), dtype=torch.float32, device="cuda")
     P = lambda x: C.c_void_p(x.data_ptr())
 
-    def project_dev(ctx, vel, p, weights=True):
+    def project_dev(ctx, vel, p, weights=False, m=None):
         st = _lib.XfpStats()
-        rc = ctx.lib.xfp_project_f32(ctx.ptr, ni, nj, nk, P(mat), P(vel[0]), P(vel[1]), P(vel[2]),
+        m = mat if m is None else m
+        rc = ctx.lib.xfp_project_f32(ctx.ptr, ni, nj, nk, P(m), P(vel[0]), P(vel[1]), P(vel[2]),
                                      *(map(P, wts) if weights else (None, None, None)), P(p), C.byref(st))
         ctx.check(rc)
         return rc, st.as_dict()
@@ -301,10 +481,12 @@ def ours(args, rank, world):
     launches = int(sum(s["launches"] for _, s in stats))
     sweep_ms = sum(s["ms_sweeps"] for _, s in stats)
     sweeps = sum(s["sweeps"] for _, s in stats)
-    # algorithmic bytes of one sweep launch (mixed: FP32 vectors/L, FP64 invdiag):
-    # forward r 4 + L 12 + invdiag 8 + y 4 = 28 B/row; backward y 4 + L 12 +
-    # invdiag 8 + r 4 + z 4 = 32 B/row; launches alternate -> 30 B/row average
-    bytes_per_launch = 30.0 * rows
+    # algorithmic bytes of one sweep launch (mixed: FP32 vectors and L, the FP64
+    # pivots streamed as FP32): forward r 4 + L 12 + invdiag 4 + y 4 = 24 B/row;
+    # backward y 4 + L 12 + invdiag 4 + r 4 + z 4 = 28 B/row; launches
+    # alternate -> 26 B/row average.  Only launches that did work are timed
+    # (the PCG loop's launches after convergence return at once).
+    bytes_per_launch = 26.0 * rows
     avg_launch_s = (sweep_ms / max(sweeps, 1)) / 1000.0
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
@@ -322,7 +504,6 @@ def ours(args, rank, world):
     ctx_h = ctx_for("mixed", 0)
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     hmat = pin(sc.mat)
-    hw = [pin(a) for a in (sc.wu, sc.wv, sc.ww)]
     hvel0 = [pin(a) for a in (sc.u, sc.v, sc.w)]
     hp = torch.zeros((nk, nj, ni), dtype=torch.float32).pin_memory()
     e2e_steps = max(2, min(args.steps, 5))
@@ -331,7 +512,7 @@ def ours(args, rank, world):
     def project_host(vel):
         st = _lib.XfpStats()
         rc = ctx_h.lib.xfp_project_f32(ctx_h.ptr, ni, nj, nk, P(hmat), P(vel[0]), P(vel[1]), P(vel[2]),
-                                       *map(P, hw), P(hp), C.byref(st))
+                                       None, None, None, P(hp), C.byref(st))
         ctx_h.check(rc)
 
     project_host(hcopies[0])
@@ -342,57 +523,54 @@ def ours(args, rank, world):
         project_host(hcopies[1 + s])
     torch.cuda.synchronize()
     el = max_over_ranks(time.perf_counter() - t0)
-    h2d = sc.mat.nbytes + sum(a.nbytes for a in (sc.u, sc.v, sc.w, sc.wu, sc.wv, sc.ww))
+    h2d = sc.mat.nbytes + sum(a.nbytes for a in (sc.u, sc.v, sc.w))
     d2h = hp.numel() * 4 + sum(a.nbytes for a in (sc.u, sc.v, sc.w))
     e2e = {"value": world * e2e_steps / el, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "path": "xfp_project_f32, host pointers (pinned)"}
 
-    # ---------------- plain forms and accuracy against an FP64 solve ----------------
+    # ---------------- the other forms on the same scene ----------------
+    # plain FP32 and FP64 at the same tolerance (their pressures and projected
+    # velocities are kept for the parity report), and the mixed form with the
+    # obstacle's fractional face weights
     forms = {}
-    ref_p = None
-    ctx64 = ctx_for("f64", 1)
-    o = ctx64.opts
-    o.tol = 1e-12
-    ctx64.set_options(o)
-    p64 = torch.zeros((nk, nj, ni), dtype=torch.float32, device="cuda")
-    project_dev(ctx64, [a.clone() for a in vel0], p64)
-    ref_p = p64.double()
-    accs = {}
-
-    def rel(a):
-        return float(torch.linalg.norm(a.double() - ref_p) / torch.linalg.norm(ref_p))
-
-    accs["mixed"] = {"pressure_rel_l2_vs_fp64": rel(pres), "rel_residual": last["rel_residual"],
-                     "iterations": iters, "refinements": int(last["refinements"])}
-    for prec in ("f32", "f64"):
+    gpu_results = {"mixed": {"p": pres, "vel": copies[args.warmup + args.steps - 1] if args.steps else None,
+                             "iterations": iters, "rel_residual": last["rel_residual"],
+                             "refinements": int(last["refinements"])}}
+    for prec, weights, name in (("f32", False, "plain_f32"), ("f64", False, "plain_f64"),
+                                ("mixed", True, "fractional_faces_mixed")):
         c2 = ctx_for(prec, 1)
         p2 = torch.zeros_like(pres)
-        project_dev(c2, [a.clone() for a in vel0], p2)
+        project_dev(c2, [a.clone() for a in vel0], p2, weights=weights)
         torch.cuda.synchronize()
         reps = 2
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         vs = [[a.clone() for a in vel0] for _ in range(reps)]
         e0.record(stream)
         for r_ in range(reps):
-            rc2, st2 = project_dev(c2, vs[r_], p2)
+            rc2, st2 = project_dev(c2, vs[r_], p2, weights=weights)
         e1.record(stream)
         torch.cuda.synchronize()
-        forms["plain_" + prec] = {"value": reps / (e0.elapsed_time(e1) / 1000.0), "unit": UNIT,
-                                  "iterations": int(st2["iterations"]), "rel_residual": st2["rel_residual"],
-                                  "pressure_rel_l2_vs_fp64": rel(p2), "status": rc2}
+        forms[name] = {"value": reps / (e0.elapsed_time(e1) / 1000.0), "unit": UNIT,
+                       "iterations": int(st2["iterations"]), "rel_residual": st2["rel_residual"], "status": rc2}
+        if weights:
+            forms[name]["note"] = ("the obstacle's fractional face weights (open fractions), an extension with no "
+                                   "counterpart in xFluid")
+        else:
+            gpu_results[prec] = {"p": p2, "vel": vs[-1], "iterations": int(st2["iterations"]),
+                                 "rel_residual": st2["rel_residual"]}
         c2.close()
     # xFluid's NormalPressureSolver matrix (classic Poisson, no face weights)
     # on the same scene and tolerance, mixed precision
     cn = ctx_for("mixed", 1, "normal")
     pn = torch.zeros_like(pres)
-    project_dev(cn, [a.clone() for a in vel0], pn, weights=False)
+    project_dev(cn, [a.clone() for a in vel0], pn)
     torch.cuda.synchronize()
     reps = 2
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     vs = [[a.clone() for a in vel0] for _ in range(reps)]
     e0.record(stream)
     for r_ in range(reps):
-        rcn, stn = project_dev(cn, vs[r_], pn, weights=False)
+        rcn, stn = project_dev(cn, vs[r_], pn)
     e1.record(stream)
     torch.cuda.synchronize()
     forms["normal_matrix_mixed"] = {"value": reps / (e0.elapsed_time(e1) / 1000.0), "unit": UNIT,
@@ -409,7 +587,7 @@ def ours(args, rank, world):
     def step_fused(vel, p):
         st = _lib.XfpStats()
         cs.check(cs.lib.xfp_project_step_f32(cs.ptr, ni, nj, nk, P(mat), P(vel[0]), P(vel[1]), P(vel[2]),
-                                             *map(P, wts), P(p), f3, dt_s, layers, C.byref(st)))
+                                             None, None, None, P(p), f3, dt_s, layers, C.byref(st)))
 
     def step_separate(vel, p):
         cs.check(cs.lib.xfp_apply_forces_f32(cs.ptr, ni, nj, nk, P(mat), P(vel[0]), P(vel[1]), P(vel[2]), f3,
@@ -435,6 +613,7 @@ def ours(args, rank, world):
         "force": [0.0, -9.8, 0.0], "dt": dt_s, "unit": "ms per step"}
     cs.close()
     forms["mixed_over_plain_f32"] = value / world / forms["plain_f32"]["value"]
+    forms["stall_cases"] = stall_cases(args, stream, ctx_for, project_dev, mat, vel0)
     forms["mixed_over_plain_f64"] = value / world / forms["plain_f64"]["value"]
 
     # ---------------- batched uneven scenes (C4) beside the headline ----------------
@@ -454,19 +633,34 @@ def ours(args, rank, world):
         else:
             particles = particles_leg(stream, barrier, max_over_ranks, cpu=(rank == 0 and not args.no_cpu))
 
-    # ---------------- CPU baseline (rank 0, N=1 only) ----------------
+    # ---------------- xFluid's whole time step on the device, beside the headline ----------------
+    timestep = None
+    if not args.no_batch:
+        if world == 1:
+            try:
+                timestep = timestep_leg(stream, barrier, max_over_ranks)
+            except Exception as e:
+                timestep = {"error": repr(e)[:300]}
+        else:
+            timestep = timestep_leg(stream, barrier, max_over_ranks)
+
+    # ---------------- CPU baseline and parity (rank 0, N=1 only) ----------------
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        sec, kind = cpu_project_seconds(sc)
+        sec, kind, ref = cpu_project_seconds(sc, keep=True)
         cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": 1, "kind": kind,
                "sample": (f"one full {args.n}^3 projection ({sec:.1f} s): assemble + MIC(0)-PCG to 1e-6 + "
-                          "applyPressure, single-threaded as xFluid's PCG is"
-                          + ("; same scene without fractional face weights (xFluid has none)" if kind == "reference"
-                             else "; oracle C port, same scene"))}
+                          "applyPressure, single-threaded as xFluid's PCG is, on the headline's scene"
+                          + ("" if kind == "reference" else " (oracle C port)"))}
         try:
             cpu["apply_pressure"] = cpu_apply_pressure(sc)
         except Exception as e:   # a reported extra: never lose the line over it
             cpu["apply_pressure"] = {"error": repr(e)[:200]}
+        try:
+            parity = parity_report(sc, kind, ref, gpu_results)
+        except Exception as e:
+            parity = {"error": repr(e)[:300]}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -476,10 +670,11 @@ def ours(args, rank, world):
                            parallelism="replicas" if world > 1 else "single GPU",
                            tile_k=int(last.get("tile_k", 0))),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk.summary(), "accuracy": accs, "forms": forms, "batch": batch, "rollout": rollout, "particles": particles}
+            "clocks": clk.summary(), "parity": parity, "forms": forms, "batch": batch, "rollout": rollout, "particles": particles,
+            "timestep": timestep}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    for c in (ctx, ctx_h, ctx64):
+    for c in (ctx, ctx_h):
         c.close()
     if world > 1:
         dist.destroy_process_group()
@@ -583,13 +778,20 @@ def profile_case(n, tile_k=8):
     ctx.close()
 
 
+ROLLOUT_BOXES = {"configured": ((0.6, 0.9), (0.6, 0.9), (0.6, 0.9)),
+                 "inside_dam": ((0.1, 0.35), (0.1, 0.45), (0.2, 0.8))}
+
+
 def rollout_leg(stream, barrier, max_over_ranks):
     """One gradient of the differentiable rollout at 128^3: 16 steps of
     (semi-Lagrangian advection -> projection) over the dam-break mask from
     u0 ~ U[-0.5,0.5] (seed 5), dt = 1/30, dx = 1/128, checkpoints every 4 steps,
-    loss = sum of squared velocity in [0.6,0.9]^3; mixed precision (FP32
-    fields).  The gradient costs 16 forward, 16 recomputed and 16 adjoint
-    projections."""
+    loss = sum of squared velocity in a box; mixed precision (FP32 fields).
+    The gradient costs 16 forward, 16 recomputed and 16 adjoint projections.
+    Two boxes: the configured [0.6,0.9]^3, which lies in air away from the dam
+    (the adjoint projections' right-hand sides G^T g stay zero there, so their
+    solves do nothing; reported), and a box inside the dam's fluid, where every
+    adjoint projection solves a nonzero system."""
     import torch
     from xfluid_b200 import scenes
     from xfluid_b200.rollout import Rollout
@@ -597,29 +799,77 @@ def rollout_leg(stream, barrier, max_over_ranks):
     sc = scenes.dam_break(n, seed=1)
     rng = np.random.default_rng(5)
     u0 = [torch.from_numpy(rng.uniform(-0.5, 0.5, a.shape).astype(np.float32)).cuda() for a in (sc.u, sc.v, sc.w)]
-    r = Rollout(torch.from_numpy(sc.mat).cuda(), steps=16, checkpoint_every=4, dt_over_dx=n / 30.0,
-                precision="mixed", tol=1e-6, max_iter=MAXIT)
+    out = {}
+    for name, box in ROLLOUT_BOXES.items():
+        r = Rollout(torch.from_numpy(sc.mat).cuda(), steps=16, checkpoint_every=4, dt_over_dx=n / 30.0, box=box,
+                    precision="mixed", tol=1e-6, max_iter=MAXIT)
+        try:
+            r.forward(*u0)
+            r.backward()                         # warm-up
+            barrier()
+            torch.cuda.synchronize()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            r.iterations = {"forward": 0, "backward": 0}
+            e0.record(stream)
+            loss = r.forward(*u0)
+            e1.record(stream)
+            g = r.backward()
+            e2.record(stream)
+            torch.cuda.synchronize()
+            gn = float(sum(float((a.double() ** 2).sum()) for a in g) ** 0.5)
+            rhs = r.adjoint_rhs_inf
+            out[name] = {"box": [list(x) for x in box],
+                         "forward_ms": max_over_ranks(e0.elapsed_time(e1)),
+                         "gradient_ms": max_over_ranks(e0.elapsed_time(e2)), "projections_per_gradient": 48,
+                         "pcg_iterations": dict(r.iterations), "loss": loss, "grad_norm": gn,
+                         "adjoint_rhs_inf": {"max": max(rhs), "min": min(rhs),
+                                             "zero_steps": sum(1 for x in rhs if x == 0.0)}}
+        finally:
+            r.close()
+    return dict(out["configured"],
+                workload="dam break 128^3, 16 advect+project steps, checkpoints every 4, u0 ~ U[-0.5,0.5] "
+                         "(seed 5), box [0.6,0.9]^3, mixed precision, tol 1e-6",
+                box_inside_dam=out["inside_dam"])
+
+
+def timestep_leg(stream, barrier, max_over_ranks, n=128, warm=2, timed=4):
+    """xFluid's whole time step on the device (xfluid_b200.simulation: field
+    and material, forces + projection + extrapolation, particle advection and
+    the particle-to-grid transfer) on the pool drop at n^3: pool y < 0.3 plus a
+    fluid sphere (r 0.15 at (0.5,0.7,0.5)), a static solid sphere (r 0.1 at
+    (0.3,0.2,0.5)) as solid cells, 8 particles per fluid cell seeded as
+    xFluid seeds them, at rest; gravity -9.8, CFL 5, tol 1e-6, FP64 as the
+    reference.  dt from the particles' speed (capped at 1/30).  Each step is
+    blocking library calls; the steps are timed together with CUDA events."""
+    import torch
+    from xfluid_b200 import scenes
+    from xfluid_b200.simulation import Simulation
+    sc = scenes.pool_drop(n, seed=2)
+    dx = 1.0 / n
+    P = scenes.seed_particles(sc.mat, dx, seed=7, vel=np.zeros((int((sc.mat == 1).sum()) * 8, 3)))
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    sim = Simulation(T(sc.mat), T(P), dx, force=(0.0, -9.8, 0.0), cfl=5.0, tol=TOL, max_iter=MAXIT)
     try:
-        r.forward(*u0)
-        r.backward()                         # warm-up
+        for _ in range(warm):
+            sim.time_step(sim.step_dt(max_dt=1.0 / 30.0))
         barrier()
         torch.cuda.synchronize()
-        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        r.iterations = {"forward": 0, "backward": 0}
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        its = []
         e0.record(stream)
-        loss = r.forward(*u0)
+        for _ in range(timed):
+            sim.time_step(sim.step_dt(max_dt=1.0 / 30.0))
+            its.append(int(sim.stats.get("iterations", 0)))
         e1.record(stream)
-        g = r.backward()
-        e2.record(stream)
         torch.cuda.synchronize()
-        gn = float(sum(float((a.double() ** 2).sum()) for a in g) ** 0.5)
-        return {"workload": "dam break 128^3, 16 advect+project steps, checkpoints every 4, u0 ~ U[-0.5,0.5] "
-                            "(seed 5), box [0.6,0.9]^3, mixed precision, tol 1e-6",
-                "forward_ms": max_over_ranks(e0.elapsed_time(e1)),
-                "gradient_ms": max_over_ranks(e0.elapsed_time(e2)), "projections_per_gradient": 48,
-                "pcg_iterations": dict(r.iterations), "loss": loss, "grad_norm": gn}
+        ms = max_over_ranks(e0.elapsed_time(e1)) / timed
+        return {"workload": f"pool drop {n}^3, {len(P)} particles at rest, gravity -9.8, CFL 5, tol 1e-6, FP64; "
+                            f"steps {warm + 1}-{warm + timed}",
+                "particles": len(P), "ms_per_step": ms, "steps_per_s": 1000.0 / ms, "pcg_iterations": its,
+                "stages": "distance field + material, save, forces + projection + extrapolation, advection, "
+                          "particle-to-grid"}
     finally:
-        r.close()
+        sim.close()
 
 
 def particles_leg(stream, barrier, max_over_ranks, cpu=True):

@@ -441,6 +441,7 @@ class RefSim(_Lib):
         L.xfsim_particle_count.argtypes = [C.c_void_p]
         L.xfsim_particle_count.restype = C.c_longlong
         L.xfsim_particles.argtypes = [C.c_void_p, _dp]
+        L.xfsim_fields.argtypes = [C.c_void_p, _u8, _dp, _dp, _dp]
         self.n = n
         self.h = L.xfsim_create(n, cfl, gravity, tol, maxit)
         for lo, hi in (boxes if boxes is not None else [((0.0, 0.0, 0.0), (0.4, 0.5, 1.0))]):
@@ -486,6 +487,14 @@ class RefSim(_Lib):
         P = np.zeros((self.lib.xfsim_particle_count(self.h), 6))
         self.lib.xfsim_particles(self.h, _p(P))
         return P
+
+    def fields(self):
+        """The current (material, u, v, w), without stepping."""
+        sm, su, sv, sw = self._shapes()
+        mat = np.zeros(sm, np.uint8)
+        u, v, w = np.zeros(su), np.zeros(sv), np.zeros(sw)
+        self.lib.xfsim_fields(self.h, _p(mat), _p(u), _p(v), _p(w))
+        return mat, u, v, w
 
 
 class RefSimDropIn(_Lib):

@@ -165,6 +165,18 @@ void xfsim_end_step(void* h) {
 
 int xfsim_fluid_cells(void* h) { return static_cast<Sim*>(h)->fs._countFluidCell(); }
 
+// The simulator's current material and face velocities (no stepping).
+void xfsim_fields(void* h, uint8_t* mat, double* u, double* v, double* w) {
+  FluidSimulator& f = static_cast<Sim*>(h)->fs;
+  for (int k = 0; k < f._material.sizek(); ++k)
+    for (int j = 0; j < f._material.sizej(); ++j)
+      for (int i = 0; i < f._material.sizei(); ++i)
+        mat[(size_t)k * f._ni * f._nj + (size_t)j * f._ni + i] = static_cast<uint8_t>(f._material(i, j, k));
+  dump(f._u, u);
+  dump(f._v, v);
+  dump(f._w, w);
+}
+
 long long xfsim_particle_count(void* h) { return (long long)static_cast<Sim*>(h)->fs._particles.size(); }
 
 // The simulator's particles as (p, v) rows of 6 doubles.

@@ -106,6 +106,15 @@ class ParticleSteps:
                                                    *map(_ptr, saved), float(ratio), float(dt),
                                                    int(parts.shape[0]), _ptr(parts)))
 
+    def maxVelocity(self, parts) -> float:
+        """FluidSimulator::_maxVelocity (FluidSimulator.cpp:387-400): the
+        largest particle speed, rounded as the reference rounds it."""
+        _check(parts, "float64", (parts.shape[0], 6), "particles")
+        ctx = self._context([parts])
+        out = C.c_double(0.0)
+        ctx.check(ctx.lib.xfp_max_speed_f64(ctx.ptr, int(parts.shape[0]), _ptr(parts), C.byref(out)))
+        return out.value
+
     def updateVelocityByParticles(self, parts, uvw) -> None:
         """FluidSimulator::_updateVelocityByParticles (:909-1085) into uvw."""
         nk, nj, ni1 = (int(x) for x in uvw[0].shape)
