@@ -738,12 +738,13 @@ def batch_leg(args, rank, world, stream, barrier, max_over_ranks):
 
     def batched(items):
         ok = bp.project(items) if items else True
-        return ok, [s["iterations"] for s in bp.stats], (bp.stats[0]["tile_k"] if bp.stats else None)
+        return ok, [s["iterations"] for s in bp.stats], ((bp.stats[0]["tile_k"], bp.stats[0]["graph"])
+                                                           if bp.stats else (None, None))
 
     loop(fresh())                       # warm-up
     ms_loop, it_loop = timed(loop, 2)
     batched(fresh())                    # warm-up: tile height timed and cached
-    ms_batch, (ok, it_batch, tile_k) = timed(batched, 3)
+    ms_batch, (ok, it_batch, (tile_k, graph)) = timed(batched, 3)
     ctx.close()
     bp.close()
     return {"workload": "64 scenes, nx,ny,nz ~ U[32,160] (seed 4), 32-blob masks, U[-1,1] FP32 faces, "
@@ -752,6 +753,7 @@ def batch_leg(args, rank, world, stream, barrier, max_over_ranks):
             "loop_value": cells_all / (ms_loop / 1000.0), "speedup_over_loop": ms_loop / ms_batch,
             "ms_batch": ms_batch, "ms_loop": ms_loop, "cells": cells_all, "n_scenes": len(scs_all),
             "all_converged": bool(ok), "iterations_equal_to_single": it_batch == it_loop, "tile_k": tile_k,
+            "pcg_loop": "CUDA graph" if graph else "direct launches (graph capture refused)",
             "sharding": f"LPT over {world} rank(s)"}
 
 

@@ -29,6 +29,9 @@ def test_reference_arm_prints_one_contract_line():
     assert "workload" in d["config"]
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["cores"] >= 1 and cb["kind"] in ("reference", "port") and cb["sample"]
+    # every usable host core runs a projection, or the line says why not
+    assert cb["host_cores"] == len(os.sched_getaffinity(0))
+    assert cb["cores"] == cb["host_cores"] or cb.get("fewer_processes_than_cores")
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
