@@ -93,3 +93,26 @@ def test_rejects_host_pointers():
     rc, msg = _call(lib, sc.ni, sc.nj, sc.nk, [C.c_void_p(a.ctypes.data) for a in host] + [None] * 3,
                     C.c_void_p(out.ctypes.data))
     assert rc == _lib.XFP_ERR_ARGS and "device" in msg
+
+
+@pytest.mark.gpu
+def test_nan_in_a_face_velocity_gives_nan():
+    """A field that has blown up is not reported as finite: one NaN face of a
+    fluid cell makes |b|_inf NaN (a plain fmax reduction would drop it)."""
+    import torch
+
+    lib = _lib.load()
+    sc = scenes.blob_scene(24, seed=3, dtype=np.float64, fractional=False)
+    k, j, i = (int(x[0]) for x in np.nonzero(sc.mat == 1))
+    u = np.ascontiguousarray(sc.u, np.float64).copy()
+    u[k, j, i + 1] = np.nan
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    arrs = [t(np.ascontiguousarray(sc.mat, np.uint8)), t(u), t(sc.v.astype(np.float64)), t(sc.w.astype(np.float64))]
+    outs = [torch.zeros(1, dtype=torch.float64, device="cuda") for _ in range(2)]
+    for n, a in enumerate((arrs, [arrs[0], t(sc.u.astype(np.float64)), arrs[2], arrs[3]])):
+        rc, msg = _call(lib, sc.ni, sc.nj, sc.nk, [C.c_void_p(x.data_ptr()) for x in a] + [None] * 3,
+                        C.c_void_p(outs[n].data_ptr()))
+        assert rc == _lib.XFP_OK, msg
+    torch.cuda.synchronize()
+    assert np.isnan(outs[0].item())
+    assert np.isfinite(outs[1].item()) and outs[1].item() > 0
