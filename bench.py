@@ -288,10 +288,13 @@ def stall_cases(args, stream, ctx_for, project_dev, mat, vel0):
     """Where the mixed form earns its keep: cases in which plain FP32 PCG needs
     many more iterations, or stalls, before reaching the accuracy the mixed
     form reaches.  Each case times one projection per form (after one
-    untimed), reports iterations, status and the pressure's relative L2
-    error against an FP64 solve of the same system to tol 1e-12 (the FP64
-    path follows the reference's operation order), and the mixed form's
-    speed over plain FP32.
+    untimed) -- plain FP32, mixed and plain FP64 at the case's tolerance --
+    and reports iterations, status and the pressure's relative L2 error
+    against an FP64 solve of the same system to tol 1e-12 (the FP64 path
+    follows the reference's operation order), and the mixed form's speed over
+    plain FP32.  Plain FP32 stops on its recursive residual, which drifts
+    from the true one; the mixed form stops on the true FP64 residual, as the
+    FP64 form does.
       blob_tol_1e-8  the headline scene at tol 1e-8;
       dam_256_tol_1e-6  the 256^3 dam break (fluid x < 0.4, y < 0.5, solid
                         border, the first step's gravity impulse), tol 1e-6
@@ -331,9 +334,9 @@ def stall_cases(args, stream, ctx_for, project_dev, mat, vel0):
 
         pe, _, _ = run("f64", 1e-12, 1, maxit=20000)
         entry = {"tol": tol}
-        for prec in ("f32", "mixed"):
+        for prec in ("f32", "mixed", "f64"):
             p, ms, st = run(prec, tol, 2)
-            entry["plain_f32" if prec == "f32" else "mixed"] = {
+            entry[{"f32": "plain_f32", "mixed": "mixed", "f64": "plain_f64"}[prec]] = {
                 "projections_per_s": 1000.0 / ms, "iterations": int(st["iterations"]), "status": int(st["status"]),
                 "refinements": int(st["refinements"]),
                 "pressure_rel_l2_vs_fp64_exact": float(torch.linalg.norm(p - pe) / torch.linalg.norm(pe))}
@@ -499,6 +502,20 @@ def ours(args, rank, world):
                 "traffic": (tr * rows) if tr is not None else None,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_launch_s * 1000,
                 "sweep_share_of_step": sweep_ms / ms if ms > 0 else None}
+    # the PCG loop's vector kernels, event-timed the same way (launches after
+    # convergence excluded): algorithmic bytes per unknown row (FP32 vectors
+    # and coefficients) -- SpMV s + 4 coefficients + z = 24; x/r update x, s,
+    # r, z read + x, r written = 24; s update z, s read + s written = 12
+    vec_ms = [sum(s_["ms_vec"][k] for _, s_ in stats) for k in range(3)]
+    vec_n = [sum(s_["vec_launches"][k] for _, s_ in stats) for k in range(3)]
+    vk = {}
+    for k, (name, bpr) in enumerate((("spmv_dot", 24.0), ("update_xr", 24.0), ("update_s", 12.0))):
+        if vec_n[k] > 0 and vec_ms[k] > 0:
+            avg = vec_ms[k] / vec_n[k]
+            gbs = bpr * rows / (avg / 1000.0) / 1e9
+            vk[name] = {"avg_launch_ms": avg, "launches": vec_n[k], "algorithmic_bytes_per_row": bpr,
+                        "achieved_gbs": gbs, "frac": gbs / peak, "share_of_step": vec_ms[k] / ms}
+    roofline["vector_kernels"] = vk
 
     # ---------------- e2e: through the C ABI from pinned host buffers ----------------
     ctx_h = ctx_for("mixed", 0)
@@ -719,7 +736,8 @@ def batch_leg(args, rank, world, stream, barrier, max_over_ranks):
         return best, out
 
     o = _lib.default_options()
-    o.precision, o.tol, o.max_iter, o.device_pointers, o.tile_k = _lib.PREC["mixed"], TOL, MAXIT, 1, tile_k
+    # single solves with their tile height tuned per grid shape (cached by the warm-up loop)
+    o.precision, o.tol, o.max_iter, o.device_pointers, o.tile_k = _lib.PREC["mixed"], TOL, MAXIT, 1, 0
     o.stream = C.c_void_p(stream.cuda_stream)
     ctx = _lib.Context(o)
     P = lambda x: None if x is None else C.c_void_p(x.data_ptr())

@@ -99,6 +99,9 @@ typedef struct xfp_stats {
   long long launches;    /* device kernels launched by this call */
   int tile_k;            /* sweep tile height the call used (k-lines) */
   int graph;             /* 1: the PCG iterations ran as a CUDA graph; 0: launched one by one */
+  double ms_vec[3];      /* device time of the PCG loop's vector kernels (CUDA events): SpMV + dot,
+                            x/r update, s update -- launches after convergence excluded */
+  int vec_launches[3];   /* launches timed in ms_vec, per kernel */
 } xfp_stats;
 
 /* Fills opt with defaults: tol 1e-5, max_iter 100, omega 0.97, ratio 0.25 --

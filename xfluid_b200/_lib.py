@@ -75,10 +75,15 @@ class XfpStats(C.Structure):
         ("launches", C.c_longlong),
         ("tile_k", C.c_int),
         ("graph", C.c_int),
+        ("ms_vec", C.c_double * 3),
+        ("vec_launches", C.c_int * 3),
     ]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["ms_vec"] = list(self.ms_vec)
+        d["vec_launches"] = list(self.vec_launches)
+        return d
 
 
 _lib = None

@@ -154,7 +154,9 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
     g.ni = S[s].ni; g.nj = S[s].nj; g.nk = S[s].nk;
     g.blk_lines = (int)std::max<long long>(1, std::min<long long>((nl + 7) / 8, NBLK_MAX));
     g.blk_lines_start = bl;
-    g.blk_cells = (int)std::max<long long>(1, std::min<long long>((Ms + 255) / 256, NBLK_MAX));
+    // the cell-based kernels run one thread per 4-cell group (absmax_init and
+    // the residual stride over single cells with the same blocks)
+    g.blk_cells = (int)std::max<long long>(1, std::min<long long>((Ms / 4 + 255) / 256, NBLK_MAX));
     g.blk_cells_start = bc;
     g.blk_groups = (int)spmv_block_count(Ms, NBLK_MAX);
     g.blk_groups_start = bg;
@@ -237,13 +239,14 @@ SweepGrid batch_grid(xfp_ctx* ctx, BatchState* B, PcgScalars* sc) {
   g.tile_scene = B->tile_scene.as<int>();
   g.segs = B->segs.as<BatchSeg>();
   g.scal_batch = sc;
+  g.stage = ctx->stage_solves;
   return g;
 }
 
 template <typename VT, typename IT, typename CT>
 cudaError_t batch_sweep(xfp_ctx* ctx, BatchState* B, int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d) {
   if (B->ntiles <= 0) return cudaSuccess;
-  const int maxg = sweep_max_grid(op, d, B->nw);
+  const int maxg = sweep_max_grid(op, d, B->nw, g.stage);
   if (maxg <= 0) return cudaErrorLaunchOutOfResources;
   return sweep_launch(op, g, d, B->nw, std::min(maxg, B->ntiles), ctx->stream);
 }

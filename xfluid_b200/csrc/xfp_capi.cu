@@ -163,13 +163,14 @@ SweepGrid make_grid(xfp_ctx* ctx, PcgScalars* sc, int bwd_mode) {
   g.spin_limit = spin_limit(ctx);
   g.scal = sc;
   g.trace = ctx->tracing ? ctx->trace.as<int>() : nullptr;
+  g.stage = ctx->stage_solves;
   return g;
 }
 
 template <typename VT, typename IT, typename CT>
 int run_sweep(xfp_ctx* ctx, int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d) {
   if (g.ntiles <= 0) return XFP_OK;
-  int maxg = sweep_max_grid(op, d, ctx->nw);
+  int maxg = sweep_max_grid(op, d, ctx->nw, g.stage);
   if (maxg <= 0) {
     const cudaError_t e = cudaGetLastError();
     return fail(ctx, XFP_ERR_CUDA, std::string("sweep kernel cannot be resident (op ") + std::to_string(op) +
@@ -190,6 +191,21 @@ int run_sweep(xfp_ctx* ctx, int op, const SweepGrid& g, const SweepData<VT, IT, 
     ctx->sweep_ev_used += 2;
   }
   return XFP_OK;
+}
+
+// Event pair around one vector-kernel launch of the PCG loop (kind, iteration).
+template <typename F>
+cudaError_t timed_kernel(xfp_ctx* ctx, int kind, int iter, F&& launch) {
+  const bool timed = ctx->kern_ev_used + 2 <= (int)ctx->kern_ev.size();
+  if (timed) cudaEventRecord(ctx->kern_ev[ctx->kern_ev_used], ctx->stream);
+  const cudaError_t e = launch();
+  if (timed) {
+    cudaEventRecord(ctx->kern_ev[ctx->kern_ev_used + 1], ctx->stream);
+    ctx->kern_kind[ctx->kern_ev_used / 2] = kind;
+    ctx->kern_iter[ctx->kern_ev_used / 2] = iter;
+    ctx->kern_ev_used += 2;
+  }
+  return e;
 }
 
 // Sum of the timed durations of the sweep launches that did work (after the
@@ -289,6 +305,7 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   int rc;
   if ((rc = sweep_copies<VT, IT, DT>(ctx, L, inv, r, gs, 2, &d)) != XFP_OK) return rc;
   const int first_timed = ctx->sweep_ev_used / 2;
+  const int first_kern = ctx->kern_ev_used / 2;
   const SweepGrid& g0 = gs[0];
   const SweepGrid& g1 = gs[1];
   // with a sweep layout, r is kept in both layouts (update_xr writes both)
@@ -308,13 +325,17 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   DT* part = reinterpret_cast<DT*>(ctx->partials.p);
   for (int done_iters = 0;;) {
     for (int q = 0; q < K; ++q) {
-      XFP_CUDA(ctx, (spmv_dot<VT, VT, DT>(A[0], A[1], A[2], A[3], s, z, ctx->lines.as<Line>(),
-                                          ctx->group_line.as<int>(), ctx->nj, ctx->nk, M, dsc, part, NBLK_MAX, 0,
-                                          st)));
-      XFP_CUDA(ctx, (update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), NBLK_MAX, st, rsw, perm)));
+      const int it = done_iters + q + 1;   // this launch's PCG iteration (1-based)
+      XFP_CUDA(ctx, timed_kernel(ctx, 0, it, [&] {
+        return spmv_dot<VT, VT, DT>(A[0], A[1], A[2], A[3], s, z, ctx->lines.as<Line>(), ctx->group_line.as<int>(),
+                                    ctx->nj, ctx->nk, M, dsc, part, NBLK_MAX, 0, st);
+      }));
+      XFP_CUDA(ctx, timed_kernel(ctx, 1, it, [&] {
+        return update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), NBLK_MAX, st, rsw, perm);
+      }));
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g1, d)) != XFP_OK) return rc;
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_BWD, g1, d)) != XFP_OK) return rc;
-      XFP_CUDA(ctx, update_s<VT>(s, z, M, dsc, st, zsw, perm));
+      XFP_CUDA(ctx, timed_kernel(ctx, 2, it, [&] { return update_s<VT>(s, z, M, dsc, st, zsw, perm); }));
     }
     done_iters += K;
     XFP_CUDA(ctx, cudaMemcpyAsync(hsc, dsc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
@@ -327,6 +348,11 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   // converged iteration skips its preconditioner): 2 * iterations did work;
   // the launches after them in the last chunk returned at once
   for (int q = first_timed + 2 * std::max(hsc->iters, 1); q < ctx->sweep_ev_used / 2; ++q) ctx->sweep_work[q] = 0;
+  // vector kernels of this call that ran after convergence: SpMV and the x/r
+  // update of iterations past the last, the s update of the last and later
+  for (int q = first_kern; q < ctx->kern_ev_used / 2; ++q)
+    if (ctx->kern_iter[q] > hsc->iters || (ctx->kern_kind[q] == 2 && ctx->kern_iter[q] >= hsc->iters))
+      ctx->kern_kind[q] = -1;
   if (hsc->status == XFP_ERR_BREAKDOWN) return fail(ctx, XFP_ERR_BREAKDOWN, "PCG breakdown: rho is zero or NaN");
   return hsc->status == 0 ? XFP_OK : XFP_NOT_CONVERGED;
 }
@@ -389,7 +415,8 @@ int tune_tile_height(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, 
     SweepGrid g = make_grid(ctx, nullptr, 0);
     const float* Lc[3] = {F[0], F[1], F[2]};
     if ((rc = sweep_copies<float, float, float>(ctx, Lc, ctx->inv32.as<float>(), A[4], &g, 1, &d)) != XFP_OK) break;
-    const int maxg = sweep_max_grid(SWEEP_FWD, d, cand);
+    const int maxg = std::min(sweep_max_grid(SWEEP_FWD, d, cand, g.stage),
+                              sweep_max_grid(SWEEP_BWD, d, cand, g.stage));
     if (maxg <= 0) continue;
     const int grid = std::min(maxg, (int)ctx->ntiles);
     cudaError_t e = sweep_launch(SWEEP_FWD, g, d, cand, grid, st);   // warm-up
@@ -424,6 +451,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
   ev_record(ctx, 0);
   if ((rc = tune_tile_height<IOT>(ctx, ni, nj, nk, dmat, du_, dv, dw, dwu, dwv, dww)) != XFP_OK) return rc;
   ctx->sweep_ev_used = 0;
+  ctx->kern_ev_used = 0;
   if ((rc = build_layout(ctx, dmat, ni, nj, nk)) != XFP_OK) return rc;
   if ((rc = ensure_compact(ctx, prec)) != XFP_OK) return rc;
   const Line* lines = ctx->lines.as<Line>();
@@ -609,6 +637,17 @@ void fill_stats(xfp_ctx* ctx, xfp_stats* s, int status, double ms_total) {
   int n = 0;
   s->ms_sweeps = sweep_ms(ctx, &n);
   s->sweeps = n;
+  for (int k = 0; k < 3; ++k) {
+    s->ms_vec[k] = 0.0;
+    s->vec_launches[k] = 0;
+  }
+  for (int q = 0; q + 1 < ctx->kern_ev_used; q += 2) {
+    const int k = ctx->kern_kind[q / 2];
+    float ms = 0;
+    if (k < 0 || cudaEventElapsedTime(&ms, ctx->kern_ev[q], ctx->kern_ev[q + 1]) != cudaSuccess) continue;
+    s->ms_vec[k] += ms;
+    s->vec_launches[k] += 1;
+  }
   s->launches = g_kernel_launches - ctx->launches;
   s->tile_k = ctx->nw;
 }
@@ -1073,6 +1112,11 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
   ctx->sweep_ev.resize(2048);
   ctx->sweep_work.assign(1024, 0);
   for (auto& e : ctx->sweep_ev) cudaEventCreate(&e);
+  ctx->kern_ev.resize(3072);
+  ctx->kern_kind.assign(1536, -1);
+  ctx->kern_iter.assign(1536, 0);
+  for (auto& e : ctx->kern_ev) cudaEventCreate(&e);
+  if (const char* e = getenv("XFP_STAGE_SOLVES")) ctx->stage_solves = atoi(e) != 0;
   if (getenv("XFP_TRACE")) {
     ctx->tracing = true;
     ctx->trace.ensure(1024 * 40 * 4 * sizeof(int));
@@ -1106,6 +1150,8 @@ int xfp_destroy(xfp_ctx* ctx) {
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : ctx->sweep_ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : ctx->kern_ev)
     if (e) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -80,6 +80,10 @@ struct xfp_ctx {
   DevBuf xmarker;
   long long Msw = 0;
   bool tracing = false;
+  // FP32/mixed triangular solves stage their group blocks through shared
+  // memory with cp.async (1, the default) or load them into registers (0,
+  // XFP_STAGE_SOLVES=0)
+  int stage_solves = 1;
   // sizes of the current layout
   int ni = 0, nj = 0, nk = 0, NJt = 0, NKt = 0, nw = 8;
   long long M = 0, rows = 0, nlines_act = 0, ntiles = 0;
@@ -96,6 +100,12 @@ struct xfp_ctx {
   // per timed sweep launch (event pair): 1 when it did work, 0 for the
   // launches a PCG loop issues after convergence (they return at once)
   std::vector<char> sweep_work;
+  // the PCG loop's vector kernels, timed the same way: event pairs with the
+  // kernel kind (0 SpMV + dot, 1 x/r update, 2 s update) and its PCG iteration
+  // (launches after the converged iteration return at once and are dropped)
+  std::vector<cudaEvent_t> kern_ev;
+  std::vector<int> kern_kind, kern_iter;
+  int kern_ev_used = 0;
   long long launches = 0;
   // batched scenes (xfp_project_batch_*): buffers, tables and tuning cache
   xfp_host::BatchState* batch = nullptr;

@@ -37,6 +37,9 @@ struct SweepGrid {
   // Sweep layout of the solve arrays (one entry per tile of `tiles`), or null:
   // the solves then read the factor and write y in the line layout.
   const SwTile* swt = nullptr;
+  // triangular solves of 4-byte types: stage the group blocks through shared
+  // memory with cp.async (1) or load them into registers (0)
+  int stage = 0;
 };
 
 // Arrays of one sweep.  VT: vector/L type of the solves, IT: invdiag type,
@@ -79,12 +82,12 @@ template <typename VT, typename IT, typename CT>
 cudaError_t solve_launch(int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d, int nw, int grid,
                          cudaStream_t st);
 template <typename VT, typename IT, typename CT>
-int solve_max_grid(int op, int nw);
+int solve_max_grid(int op, int nw, int stage);
 
 #define XFP_SWEEP_DECL(VT, IT, CT)                                                             \
   cudaError_t sweep_launch(int op, const SweepGrid& g, const SweepData<VT, IT, CT>& d, int nw, \
                            int grid, cudaStream_t st);                                         \
-  int sweep_max_grid(int op, const SweepData<VT, IT, CT>& d, int nw);
+  int sweep_max_grid(int op, const SweepData<VT, IT, CT>& d, int nw, int stage = 0);
 XFP_SWEEP_DECL(double, double, double)
 XFP_SWEEP_DECL(float, float, float)
 XFP_SWEEP_DECL(float, double, double)   // mixed form: factorisation only

@@ -831,7 +831,8 @@ __global__ void __launch_bounds__(256) batch_update_xr_kernel(const BatchSeg* __
 template <typename VT, typename DT>
 cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgScalars* sc,
                       double* partials, int nblk_max, cudaStream_t st, VT* rsw, const int* perm) {
-  int blocks = (int)std::min<long long>((M + 255) / 256, (long long)nblk_max);
+  // 4-cell groups over at most nblk_max blocks
+  int blocks = (int)std::min<long long>((M / 4 + 255) / 256, (long long)nblk_max);
   if (blocks < 1) blocks = 1;
   ++g_kernel_launches;
   update_xr_kernel<VT><<<blocks, 256, 0, st>>>(x, r, s, z, M, sc, partials, rsw, perm);
@@ -882,7 +883,9 @@ __global__ void batch_update_s_kernel(const BatchSeg* __restrict__ segs, int nse
 template <typename VT>
 cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st, const VT* zsw,
                      const int* perm) {
-  int blocks = (int)std::min<long long>((M + 255) / 256, 148LL * 16);
+  // 4-cell groups over at most 148 x 16 blocks (one thread per group measured
+  // slower at 256^3: more blocks, fewer groups per thread)
+  int blocks = (int)std::min<long long>((M / 4 + 255) / 256, 148LL * 16);
   if (blocks < 1) blocks = 1;
   ++g_kernel_launches;
   update_s_kernel<VT><<<blocks, 256, 0, st>>>(s, z, M, sc, zsw, perm);

@@ -593,10 +593,10 @@ static int max_grid_op(int nw) {
       default: return solve_launch<VT, IT, CT>(op, g, d, nw, grid, st);                         \
     }                                                                                           \
   }                                                                                             \
-  int sweep_max_grid(int op, const SweepData<VT, IT, CT>&, int nw) {                            \
+  int sweep_max_grid(int op, const SweepData<VT, IT, CT>&, int nw, int stage) {                \
     switch (op) {                                                                               \
       case SWEEP_FACTOR: return max_grid_op<SWEEP_FACTOR, VT, IT, CT>(nw);                      \
-      default: return solve_max_grid<VT, IT, CT>(op, nw);                                       \
+      default: return solve_max_grid<VT, IT, CT>(op, nw, stage);                                \
     }                                                                                           \
   }
 
@@ -611,15 +611,15 @@ cudaError_t sweep_launch(int op, const SweepGrid& g, const SweepData<float, doub
   return op == SWEEP_FACTOR ? launch_op<SWEEP_FACTOR, float, double, double>(g, d, nw, grid, st)
                             : cudaErrorInvalidValue;
 }
-int sweep_max_grid(int op, const SweepData<float, double, double>&, int nw) {
+int sweep_max_grid(int op, const SweepData<float, double, double>&, int nw, int) {
   return op == SWEEP_FACTOR ? max_grid_op<SWEEP_FACTOR, float, double, double>(nw) : 0;
 }
 cudaError_t sweep_launch(int op, const SweepGrid& g, const SweepData<float, float, double>& d, int nw, int grid,
                          cudaStream_t st) {
   return op == SWEEP_FACTOR ? cudaErrorInvalidValue : solve_launch<float, float, double>(op, g, d, nw, grid, st);
 }
-int sweep_max_grid(int op, const SweepData<float, float, double>&, int nw) {
-  return op == SWEEP_FACTOR ? 0 : solve_max_grid<float, float, double>(op, nw);
+int sweep_max_grid(int op, const SweepData<float, float, double>&, int nw, int stage) {
+  return op == SWEEP_FACTOR ? 0 : solve_max_grid<float, float, double>(op, nw, stage);
 }
 
 }  // namespace xfp
