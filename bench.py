@@ -406,6 +406,13 @@ def parity_report(sc, kind, ref, gpu):
     return out
 
 
+def phases(st):
+    """A projection's phases (CUDA events inside the library): layout + assembly
+    (+ the FP32 copies in mixed precision), MIC(0) factorisation (+ its FP32
+    copies), PCG, pressure scatter + velocity update."""
+    return {k: round(float(st[k]), 4) for k in ("ms_setup", "ms_factor", "ms_solve", "ms_apply")}
+
+
 def ours(args, rank, world):
     import ctypes as C
     import torch
@@ -568,7 +575,8 @@ def ours(args, rank, world):
         e1.record(stream)
         torch.cuda.synchronize()
         forms[name] = {"value": reps / (e0.elapsed_time(e1) / 1000.0), "unit": UNIT,
-                       "iterations": int(st2["iterations"]), "rel_residual": st2["rel_residual"], "status": rc2}
+                       "iterations": int(st2["iterations"]), "rel_residual": st2["rel_residual"], "status": rc2,
+                       "phases_ms": phases(st2)}
         if weights:
             forms[name]["note"] = ("the obstacle's fractional face weights (open fractions), an extension with no "
                                    "counterpart in xFluid")
@@ -629,6 +637,7 @@ def ours(args, rank, world):
         "ms_fused": times["fused"], "ms_separate": times["separate"], "layers": layers,
         "force": [0.0, -9.8, 0.0], "dt": dt_s, "unit": "ms per step"}
     cs.close()
+    forms["mixed_phases_ms"] = phases(last)
     forms["mixed_over_plain_f32"] = value / world / forms["plain_f32"]["value"]
     forms["stall_cases"] = stall_cases(args, stream, ctx_for, project_dev, mat, vel0)
     forms["mixed_over_plain_f64"] = value / world / forms["plain_f64"]["value"]

@@ -264,7 +264,8 @@ int batch_assemble(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<FT>>&
 template <typename VT, typename IT, typename CT>
 int batch_factor(xfp_ctx* ctx, BatchState* B, const CT* const A[4], CT* const F[6], IT* inv, CT omega, CT ratio) {
   const size_t M = (size_t)std::max<long long>(B->M, 1);
-  for (int q = 0; q < 6; ++q) XFP_CUDA(ctx, cudaMemsetAsync(F[q], 0, M * sizeof(CT), ctx->stream));
+  // the factorisation writes L only where a coupling exists: clear the three L arrays first
+  for (int q = 0; q < 3; ++q) XFP_CUDA(ctx, cudaMemsetAsync(F[q], 0, M * sizeof(CT), ctx->stream));
   XFP_CUDA(ctx, cudaMemsetAsync(inv, 0, M * sizeof(IT), ctx->stream));
   SweepData<VT, IT, CT> d;
   d.diag = A[0]; d.ax = A[1]; d.ay = A[2]; d.az = A[3];

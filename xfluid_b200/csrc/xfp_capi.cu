@@ -267,7 +267,8 @@ int check_sweep_error(xfp_ctx* ctx) {
 template <typename VT, typename IT, typename CT>
 int factor(xfp_ctx* ctx, const CT* const A[4], CT* const F[6], IT* inv, CT omega, CT ratio) {
   const size_t M = (size_t)ctx->M;
-  for (int q = 0; q < 6; ++q) XFP_CUDA(ctx, cudaMemsetAsync(F[q], 0, M * sizeof(CT), ctx->stream));
+  // the factorisation writes L only where a coupling exists: clear the three L arrays first
+  for (int q = 0; q < 3; ++q) XFP_CUDA(ctx, cudaMemsetAsync(F[q], 0, M * sizeof(CT), ctx->stream));
   XFP_CUDA(ctx, cudaMemsetAsync(inv, 0, M * sizeof(IT), ctx->stream));
   SweepData<VT, IT, CT> d;
   d.diag = A[0]; d.ax = A[1]; d.ay = A[2]; d.az = A[3];
@@ -328,10 +329,10 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
       const int it = done_iters + q + 1;   // this launch's PCG iteration (1-based)
       XFP_CUDA(ctx, timed_kernel(ctx, 0, it, [&] {
         return spmv_dot<VT, VT, DT>(A[0], A[1], A[2], A[3], s, z, ctx->lines.as<Line>(), ctx->group_line.as<int>(),
-                                    ctx->nj, ctx->nk, M, dsc, part, NBLK_MAX, 0, st);
+                                    ctx->nj, ctx->nk, M, dsc, part, ctx->vec_blocks, 0, st);
       }));
       XFP_CUDA(ctx, timed_kernel(ctx, 1, it, [&] {
-        return update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), NBLK_MAX, st, rsw, perm);
+        return update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), ctx->vec_blocks, st, rsw, perm);
       }));
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g1, d)) != XFP_OK) return rc;
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_BWD, g1, d)) != XFP_OK) return rc;
@@ -506,15 +507,13 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
     // ---- mixed: FP64 system and refinement, FP32 inner PCG ----
     double* A[5];
     for (int q = 0; q < 5; ++q) A[q] = ctx->A64[q].as<double>();
+    float* A32[4];
+    for (int q = 0; q < 4; ++q) A32[q] = ctx->A32[q].as<float>();
+    // the FP32 stencil comes out of the same assembly pass
     XFP_CUDA(ctx, (assemble<IOT, double>(dmat, du_, dv, dw, dwu, dwv, dww, ni, nj, nk, lines, A[0], A[1], A[2],
-                                         A[3], A[4], st, ctx->opt.matrix, ctx->force)));
+                                         A[3], A[4], st, ctx->opt.matrix, ctx->force, A32)));
     if (adj_gu) XFP_CUDA(ctx, (apply_pressure_T<IOT, double>(dmat, dwu, dwv, dww, adj_gu, adj_gv, adj_gw, ni, nj,
                                                              nk, lines, A[4], st)));
-    float* A32[4];
-    for (int q = 0; q < 4; ++q) {
-      A32[q] = ctx->A32[q].as<float>();
-      XFP_CUDA(ctx, (convert<double, float>(A[q], A32[q], M, st)));
-    }
     ev_record(ctx, 1);
     double* F[6];
     for (int q = 0; q < 6; ++q) F[q] = ctx->F64[q].as<double>();
@@ -1117,6 +1116,7 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
   ctx->kern_iter.assign(1536, 0);
   for (auto& e : ctx->kern_ev) cudaEventCreate(&e);
   if (const char* e = getenv("XFP_STAGE_SOLVES")) ctx->stage_solves = atoi(e) != 0;
+  if (const char* e = getenv("XFP_VEC_BLOCKS")) ctx->vec_blocks = std::max(148, std::min(xfp_host::NBLK_MAX, atoi(e)));
   if (getenv("XFP_TRACE")) {
     ctx->tracing = true;
     ctx->trace.ensure(1024 * 40 * 4 * sizeof(int));

@@ -84,6 +84,11 @@ struct xfp_ctx {
   // memory with cp.async (1, the default) or load them into registers (0,
   // XFP_STAGE_SOLVES=0)
   int stage_solves = 1;
+  // block cap of the PCG loop's SpMV and x/r update: 148 x 4 measured best at
+  // 256^3 (SpMV 37.4 us and x/r update 23.0 us per launch, against 38.7 and
+  // 27.9 at 148 x 8 and 54.5 / 26.5 at 148 x 2).  XFP_VEC_BLOCKS overrides,
+  // within [148, NBLK_MAX]; the dot's reduction order follows it.
+  int vec_blocks = 148 * 4;
   // sizes of the current layout
   int ni = 0, nj = 0, nk = 0, NJt = 0, NKt = 0, nw = 8;
   long long M = 0, rows = 0, nlines_act = 0, ntiles = 0;

@@ -128,7 +128,8 @@ template <typename FT, typename AT>
 cudaError_t assemble(const uint8_t* mat, const FT* u, const FT* v, const FT* w, const FT* wu,
                      const FT* wv, const FT* ww, int ni, int nj, int nk, const Line* lines,
                      AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st,
-                     int matrix = XFP_MATRIX_VARIATIONAL, Force3 frc = Force3());
+                     int matrix = XFP_MATRIX_VARIATIONAL, Force3 frc = Force3(),
+                     float* const A32[4] = nullptr);   // also write diag..az as FP32 (mixed form)
 
 template <typename T>
 cudaError_t scatter_dense(const T* x, const Line* lines, int ni, int nj, int nk, T* dense,

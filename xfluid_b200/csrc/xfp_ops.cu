@@ -44,7 +44,8 @@ __global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __res
                                 const FT* __restrict__ ww, int ni, int nj, int nk,
                                 const Line* __restrict__ lines, AT* __restrict__ diag,
                                 AT* __restrict__ ax, AT* __restrict__ ay, AT* __restrict__ az,
-                                AT* __restrict__ b, int matrix, Force3 frc) {
+                                AT* __restrict__ b, int matrix, Force3 frc, float* __restrict__ d32,
+                                float* __restrict__ x32, float* __restrict__ y32, float* __restrict__ z32) {
   const int lane = threadIdx.x & 31;
   const long long nlines = (long long)nj * nk;
   const size_t nn = (size_t)ni * nj;
@@ -153,6 +154,10 @@ __global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __res
         }
       }
       diag[o] = d; ax[o] = ox; ay[o] = oy; az[o] = oz; b[o] = bb;
+      // the mixed form's FP32 stencil, written by the assembly itself
+      if (d32 != nullptr) {
+        d32[o] = (float)d; x32[o] = (float)ox; y32[o] = (float)oy; z32[o] = (float)oz;
+      }
     }
   }
 }
@@ -160,31 +165,33 @@ __global__ void assemble_kernel(const uint8_t* __restrict__ mat, const FT* __res
 template <typename FT, typename AT>
 cudaError_t assemble(const uint8_t* mat, const FT* u, const FT* v, const FT* w, const FT* wu,
                      const FT* wv, const FT* ww, int ni, int nj, int nk, const Line* lines,
-                     AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st, int matrix, Force3 frc) {
+                     AT* diag, AT* ax, AT* ay, AT* az, AT* b, cudaStream_t st, int matrix, Force3 frc,
+                     float* const A32[4]) {
   const long long nlines = (long long)nj * nk;
   long long blocks = (nlines + 7) / 8;
   if (blocks > 65535 * 8) blocks = 65535 * 8;
   ++g_kernel_launches;
-  assemble_kernel<FT, AT><<<(unsigned)blocks, 256, 0, st>>>(mat, u, v, w, wu, wv, ww, ni, nj, nk, lines,
-                                                          diag, ax, ay, az, b, matrix, frc);
+  assemble_kernel<FT, AT><<<(unsigned)blocks, 256, 0, st>>>(
+      mat, u, v, w, wu, wv, ww, ni, nj, nk, lines, diag, ax, ay, az, b, matrix, frc, A32 ? A32[0] : nullptr,
+      A32 ? A32[1] : nullptr, A32 ? A32[2] : nullptr, A32 ? A32[3] : nullptr);
   return cudaGetLastError();
 }
 template cudaError_t assemble<double, double>(const uint8_t*, const double*, const double*,
                                               const double*, const double*, const double*,
                                               const double*, int, int, int, const Line*, double*,
-                                              double*, double*, double*, double*, cudaStream_t, int, Force3);
+                                              double*, double*, double*, double*, cudaStream_t, int, Force3, float* const*);
 template cudaError_t assemble<float, float>(const uint8_t*, const float*, const float*, const float*,
                                             const float*, const float*, const float*, int, int, int,
                                             const Line*, float*, float*, float*, float*, float*,
-                                            cudaStream_t, int, Force3);
+                                            cudaStream_t, int, Force3, float* const*);
 template cudaError_t assemble<float, double>(const uint8_t*, const float*, const float*,
                                              const float*, const float*, const float*, const float*,
                                              int, int, int, const Line*, double*, double*, double*,
-                                             double*, double*, cudaStream_t, int, Force3);
+                                             double*, double*, cudaStream_t, int, Force3, float* const*);
 template cudaError_t assemble<double, float>(const uint8_t*, const double*, const double*,
                                              const double*, const double*, const double*,
                                              const double*, int, int, int, const Line*, float*,
-                                             float*, float*, float*, float*, cudaStream_t, int, Force3);
+                                             float*, float*, float*, float*, cudaStream_t, int, Force3, float* const*);
 
 // ---------------------------------------------------------------------------
 // Compact -> dense pressure grid: every cell written, 0 outside unknowns
