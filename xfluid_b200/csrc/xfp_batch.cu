@@ -160,7 +160,7 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
     g.blk_cells_start = bc;
     g.blk_groups = (int)spmv_block_count(Ms, NBLK_MAX);
     g.blk_groups_start = bg;
-    g.pad = 0;
+    g.tile_base = (int)tile_base[s];
     g.base = base[s];
     g.M = Ms;
     g.lines = lines + B->line_base[s];
@@ -187,6 +187,8 @@ int batch_layout(xfp_ctx* ctx, BatchState* B, const std::vector<DevScene<T>>& S,
   B->ntiles = nt;
   B->M = base[n];
   ctx->nw = nw;
+  ctx->bnd_ni = 0;
+  for (int s = 0; s < n; ++s) ctx->bnd_ni = std::max(ctx->bnd_ni, S[s].ni);
   ctx->M = B->M;
   ctx->ntiles = nt;
   ctx->nlines_all = nlines;

@@ -65,6 +65,7 @@ int build_layout(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk) {
   XFP_CUDA(ctx, cudaMemcpyAsync(cnt, ctx->counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
   XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->ni = ni; ctx->nj = nj; ctx->nk = nk;
+  ctx->bnd_ni = ni;
   ctx->NJt = NJt; ctx->NKt = NKt;
   ctx->M = cnt[0]; ctx->rows = cnt[1]; ctx->nlines_act = cnt[2]; ctx->ntiles = cnt[3];
   ctx->nlines_all = nlines;
@@ -1138,7 +1139,8 @@ int xfp_destroy(xfp_ctx* ctx) {
                    &ctx->io_p, &ctx->io_gu, &ctx->io_gv, &ctx->io_gw, &ctx->lines, &ctx->lens,
                    &ctx->tile_active, &ctx->tiles, &ctx->counters, &ctx->cell_line, &ctx->group_line, &ctx->inv64, &ctx->inv32, &ctx->x64,
                    &ctx->r64, &ctx->x32, &ctx->r32, &ctx->s32, &ctx->z32, &ctx->s64, &ctx->z64, &ctx->dense,
-                   &ctx->sy, &ctx->sz, &ctx->ctl, &ctx->scal, &ctx->scal2, &ctx->partials, &ctx->tpartials};
+                   &ctx->sy, &ctx->sz, &ctx->bnd, &ctx->ctl, &ctx->scal, &ctx->scal2, &ctx->partials,
+                   &ctx->tpartials};
   for (DevBuf* b : all) b->release();
   batch_state_free(ctx->batch);
   ctx->batch = nullptr;

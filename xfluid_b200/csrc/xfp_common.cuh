@@ -76,7 +76,7 @@ struct BatchSeg {
   int blk_lines, blk_lines_start;   // line-based kernels (residual)
   int blk_cells, blk_cells_start;   // cell-based kernels (updates, norms)
   int blk_groups, blk_groups_start; // the SpMV (one thread per 4-cell group)
-  int pad;
+  int tile_base;                    // first slot of this scene's (K, J) -> tile map
   long long base, M;
   const Line* lines;
   double* partials;                 // this scene's reduction slots

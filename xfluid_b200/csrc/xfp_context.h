@@ -72,6 +72,10 @@ struct xfp_ctx {
   // and the copies the solves stream (lx, ly, lz, inv, r, y; 8 bytes per
   // element covers every precision)
   DevBuf swt, tile_pos, sw_perm, sw_l[3], sw_inv, sw_r, sw_y;
+  // the triangular solves' tile-boundary rows (SweepData::bk, bj), and the
+  // largest ni of the layout, which sets the rows per tile
+  DevBuf bnd;
+  int bnd_ni = 0;
   // xfp_project_step_*: body force fused into assembly and apply, and the
   // extrapolation layers run after the apply (zero outside such a call);
   // xmarker is the extrapolation's layer-marker scratch
@@ -185,7 +189,24 @@ int sweep_copies(xfp_ctx* ctx, const VT* const L[3], const IT* inv, const VT* r,
   d->invs = ctx->sw_inv.as<IT>();
   d->rs = ctx->sw_r.as<VT>();
   d->ys = ctx->sw_y.as<VT>();
-  for (int q = 0; q < ng; ++q) gs[q].swt = ctx->swt.as<xfp::SwTile>();
+  // boundary rows: per active tile, one row per wavefront step it can span,
+  // 32 k-edge words and nw j-edge words of P 64-bit words each; zeroed when
+  // (re)allocated so no stale word can carry a live generation
+  const int P = (int)(sizeof(VT) / 4);
+  const long long rows = (long long)ctx->bnd_ni + ctx->nw + 36;
+  const size_t kwords = (size_t)ctx->ntiles * rows * 32 * P, jwords = (size_t)ctx->ntiles * rows * ctx->nw * P;
+  const size_t bbytes = (kwords + jwords) * sizeof(unsigned long long);
+  if (ctx->bnd.cap < bbytes || !ctx->bnd.p) {
+    XFP_CUDA(ctx, ctx->bnd.ensure(bbytes));
+    XFP_CUDA(ctx, cudaMemsetAsync(ctx->bnd.p, 0, ctx->bnd.cap, st));
+  }
+  d->bk = ctx->bnd.as<unsigned long long>();
+  d->bj = d->bk + kwords;
+  for (int q = 0; q < ng; ++q) {
+    gs[q].swt = ctx->swt.as<xfp::SwTile>();
+    gs[q].tile_pos = ctx->tile_pos.as<int>();
+    gs[q].brows = (int)rows;
+  }
   return XFP_OK;
 }
 

@@ -40,6 +40,11 @@ struct SweepGrid {
   // triangular solves of 4-byte types: stage the group blocks through shared
   // memory with cp.async (1) or load them into registers (0)
   int stage = 0;
+  // Triangular solves: (scene tile base + K * NJt + J) -> position in
+  // `tiles`, or -1 for an inactive tile; and the number of boundary rows per
+  // tile (one per wavefront step a tile can span: max ni + tile height + 36).
+  const int* tile_pos = nullptr;
+  int brows = 0;
 };
 
 // Arrays of one sweep.  VT: vector/L type of the solves, IT: invdiag type,
@@ -66,6 +71,13 @@ struct SweepData {
   // 64-bit words (32-bit payload chunk | launch generation << 32).
   unsigned long long* sy = nullptr;  // to the j-neighbour tile
   unsigned long long* sz = nullptr;  // to the k-neighbour tile
+  // Triangular solves: the same words kept by wavefront step instead of by
+  // cell, one row per step of the producing tile, so that a step's
+  // publication and a loader's poll each touch one contiguous row:
+  // bk[((tile * brows + row) * 32 + lane) * P + p] from the tile's k-edge warp,
+  // bj[((tile * brows + row) * NW + warp) * P + p] from its j-edge lanes.
+  unsigned long long* bk = nullptr;
+  unsigned long long* bj = nullptr;
   // Sweep-layout copies (used when SweepGrid::swt is set): the factor, r,
   // and y, which the forward solve writes and the backward solve overwrites
   // with z (the line-layout r and y are then not touched).

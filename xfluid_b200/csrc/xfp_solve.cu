@@ -122,7 +122,7 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
   for (int pos = blockIdx.x, seq = 0; pos < g.ntiles; pos += gridDim.x, ++seq) {
     const int tpos = REV ? g.ntiles - 1 - pos : pos;
     // the tile's grid: the launch's one scene, or its scene of the batch
-    int nj = g.nj, nk = g.nk, maxT = g.maxT;
+    int ni = g.ni, nj = g.nj, nk = g.nk, maxT = g.maxT, NJt = g.NJt, NKt = g.NKt, tbase = 0;
     const Line* lines = g.lines;
     long long line_base = 0;
     if (g.tile_scene != nullptr) {
@@ -131,15 +131,28 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
       // a converged scene's tiles are skipped (its scalars only change between
       // launches, so every CTA of this launch decides the same way)
       if (g.scal_batch != nullptr && *(volatile int*)&g.scal_batch[sid].done != 0) continue;
+      ni = S.ni;
       nj = S.nj;
       nk = S.nk;
       maxT = S.ni + S.nj + S.nk;
+      NJt = (S.nj + 31) >> 5;
+      NKt = (S.nk + NW - 1) / NW;
+      tbase = S.tile_base;
       lines = S.lines;
       line_base = S.line_base;
     }
     const int packed = g.tiles[tpos];
     const int J = packed & 0xffff, K = packed >> 16;
     const int j0 = J * 32, k0 = K * NW;
+    // First wavefront step a tile (Jt, Kt) can have a stored cell at: its
+    // boundary rows are indexed by step - this.  Stored cells include the
+    // group padding, i in [-3, ni + 2], so i + j + k runs from 32 Jt + NW Kt - 3
+    // to 32 Jt + NW Kt + ni + NW + 32: at most ni + NW + 36 steps.
+    auto row_base = [&](int Jt, int Kt) -> int {
+      const int lowest = 32 * Jt + NW * Kt - 3;
+      return REV ? maxT - (lowest + ni + NW + 35) : lowest;
+    };
+    const int R = g.brows;
 
     // ---------------- setup: wavefront ranges, cleared hand-off ring ----------------
     Line L = {0, 0, 0, 0};
@@ -194,6 +207,11 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
       const bool kpub = REV ? (warp == 0) : (warp == NW - 1);
 
       VT out_x = VT(0), out_y = VT(0);
+      // this thread's column of the tile's boundary rows (used by the j-edge
+      // lanes and the k-edge warp)
+      const int rb_self = row_base(J, K);
+      unsigned long long* const bj_me = d.bj + ((size_t)tpos * R * NW + warp) * P;
+      unsigned long long* const bk_me = d.bk + ((size_t)tpos * R * 32 + lane) * P;
 
       // Sweep layout (when the launch has one): this warp's stream of
       // 32-lane blocks, one per group of 4 forward steps.
@@ -261,7 +279,7 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
       // One wavefront step: everything that needs only this warp's previous
       // step is done before the barrier; after it, the z and boundary inputs
       // of step tau-1 are in shared memory.
-      auto step = [&](const int tau, const Grp& G, const int e, const bool in, const int c) -> VT {
+      auto step = [&](const int tau, const Grp& G, const int e, const bool in) -> VT {
         const VT vy_sh = REV ? shfl_down_any(out_y) : shfl_up_any(out_y);
         const int slot = tau & (SRING - 1);
         VT res;
@@ -286,14 +304,16 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           if (in && jpub) {
             uint32_t w[P];
             to_words(y, w);
+            unsigned long long* o = bj_me + (size_t)(tau - rb_self) * (NW * P);
 #pragma unroll
-            for (int p = 0; p < P; ++p) st_gpu64(&d.sy[(size_t)c * P + p], stamped(gen, w[p]));
+            for (int p = 0; p < P; ++p) st_gpu64(o + p, stamped(gen, w[p]));
           }
           if (in && kpub) {
             uint32_t w[P];
             to_words(y, w);
+            unsigned long long* o = bk_me + (size_t)(tau - rb_self) * (32 * P);
 #pragma unroll
-            for (int p = 0; p < P; ++p) st_gpu64(&d.sz[(size_t)c * P + p], stamped(gen, w[p]));
+            for (int p = 0; p < P; ++p) st_gpu64(o + p, stamped(gen, w[p]));
           }
         } else {
           // solve_lower_transpose_in_place: x[c] -= L(m,c) x[m] for m = c+1,
@@ -321,14 +341,16 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           if (in && jpub) {
             uint32_t w[P];
             to_words(oy, w);
+            unsigned long long* o = bj_me + (size_t)(tau - rb_self) * (NW * P);
 #pragma unroll
-            for (int p = 0; p < P; ++p) st_gpu64(&d.sy[(size_t)c * P + p], stamped(gen, w[p]));
+            for (int p = 0; p < P; ++p) st_gpu64(o + p, stamped(gen, w[p]));
           }
           if (in && kpub) {
             uint32_t w[P];
             to_words(oz, w);
+            unsigned long long* o = bk_me + (size_t)(tau - rb_self) * (32 * P);
 #pragma unroll
-            for (int p = 0; p < P; ++p) st_gpu64(&d.sz[(size_t)c * P + p], stamped(gen, w[p]));
+            for (int p = 0; p < P; ++p) st_gpu64(o + p, stamped(gen, w[p]));
           }
         }
         return res;
@@ -336,13 +358,12 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
       auto run_group = [&](int t0, const Grp& G, int c4, long long si) {
         VT yb[GS];
         const bool in = c4 >= 0;
-        const int cc = in ? c4 : 0;
 #pragma unroll
         for (int q = 0; q < GS; ++q) {
           const int tau = t0 + q;
           const int e = REV ? GS - 1 - q : q;
           yb[e] = VT(0);
-          if (tau >= tileLo && tau <= tileHi) yb[e] = step(tau, G, e, in, cc + e);
+          if (tau >= tileLo && tau <= tileHi) yb[e] = step(tau, G, e, in);
         }
         // with a sweep layout y (forward) and z (backward, in place) go to
         // the sweep-ordered copy, otherwise to the line layout; lanes without
@@ -522,6 +543,12 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           if (!REV) { Sk_lo = a; Sk_hi = b; } else { Sk_lo = maxT - b; Sk_hi = maxT - a; }
         }
       }
+      // source tiles of the boundary rows (-1: outside the grid or inactive;
+      // then no step needs them, since needj/needk require a source cell)
+      const int Jsrc = REV ? J + 1 : J - 1, Ksrc = REV ? K + 1 : K - 1;
+      const int tp_j = (Jsrc >= 0 && Jsrc < NJt) ? g.tile_pos[tbase + K * NJt + Jsrc] : -1;
+      const int tp_k = (Ksrc >= 0 && Ksrc < NKt) ? g.tile_pos[tbase + Ksrc * NJt + J] : -1;
+      const int rb_j = row_base(Jsrc, K), rb_k = row_base(J, Ksrc);
       const unsigned want = gen + g.expect_bias;   // bias != 0 only in the expired-wait diagnostic
       int gate_seen = tileLo - 1;
       bool failed = false;
@@ -547,11 +574,10 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
         // Issue the whole batch's loads, then forward every step as soon as
         // its stamps are current: each poll round re-issues the loads of all
         // steps still missing (all in flight together) and forwards the ready
-        // prefix.  The source cell of step base+q lies q cells further along
-        // the source line (backward: q cells back).
-        const int ij0 = REV ? (maxT - base) - sj_c : base - sj_c;
-        const int ik0 = REV ? (maxT - base) - sk_c : base - sk_c;
-        const int cj0 = Ljs.off + (ij0 - Ljs.lo), ck0 = Lks.off + (ik0 - Lks.lo);
+        // prefix.  Step base+q reads the source tile's row of its step
+        // base+q-1: one contiguous row per step for the whole warp.
+        const long long rj0 = (long long)tp_j * R + (base - 1 - rb_j);
+        const long long rk0 = (long long)tp_k * R + (base - 1 - rb_k);
         auto needj = [&](int q) {
           const int tau = base + q;
           return lane < NW && tau <= tileHi && tau >= Sj_lo && tau <= Sj_hi;
@@ -560,15 +586,15 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
           const int tau = base + q;
           return tau <= tileHi && tau >= Sk_lo && tau <= Sk_hi;
         };
-        auto oj = [&](int q) { return (size_t)(REV ? cj0 - q : cj0 + q) * P; };
-        auto ok_ = [&](int q) { return (size_t)(REV ? ck0 - q : ck0 + q) * P; };
+        auto oj = [&](int q) { return ((size_t)(rj0 + q) * NW + lane) * P; };
+        auto ok_ = [&](int q) { return ((size_t)(rk0 + q) * 32 + lane) * P; };
         unsigned long long vj[SLB][P], vk[SLB][P];
 #pragma unroll
         for (int q = 0; q < SLB; ++q) {
 #pragma unroll
           for (int p = 0; p < P; ++p) {
-            vj[q][p] = needj(q) ? ld_gpu64(&d.sy[oj(q) + p]) : 0ull;
-            vk[q][p] = needk(q) ? ld_gpu64(&d.sz[ok_(q) + p]) : 0ull;
+            vj[q][p] = needj(q) ? ld_gpu64(&d.bj[oj(q) + p]) : 0ull;
+            vk[q][p] = needk(q) ? ld_gpu64(&d.bk[ok_(q) + p]) : 0ull;
           }
         }
         const int nsteps = min(SLB, tileHi - base + 1);
@@ -618,8 +644,8 @@ __global__ void __launch_bounds__((NW + 2) * 32, 1)
             if (q >= fwd && !failed) {
 #pragma unroll
               for (int p = 0; p < P; ++p) {
-                if (needj(q) && (uint32_t)(vj[q][p] >> 32) != want) vj[q][p] = ld_gpu64(&d.sy[oj(q) + p]);
-                if (needk(q) && (uint32_t)(vk[q][p] >> 32) != want) vk[q][p] = ld_gpu64(&d.sz[ok_(q) + p]);
+                if (needj(q) && (uint32_t)(vj[q][p] >> 32) != want) vj[q][p] = ld_gpu64(&d.bj[oj(q) + p]);
+                if (needk(q) && (uint32_t)(vk[q][p] >> 32) != want) vk[q][p] = ld_gpu64(&d.bk[ok_(q) + p]);
               }
             }
           }
