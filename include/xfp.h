@@ -102,6 +102,11 @@ typedef struct xfp_stats {
   double ms_vec[3];      /* device time of the PCG loop's vector kernels (CUDA events): SpMV + dot,
                             x/r update, s update -- launches after convergence excluded */
   int vec_launches[3];   /* launches timed in ms_vec, per kernel */
+  long long h2d_bytes;   /* host-pointer mode: bytes this call moved host -> device */
+  long long d2h_bytes;   /* host-pointer mode: bytes this call moved device -> host */
+  int host_faces;        /* 1: only the faces that border fluid crossed PCIe (page-locked
+                            velocity arrays, read and written in place); 0: whole arrays
+                            were copied, or device pointers */
 } xfp_stats;
 
 /* Fills opt with defaults: tol 1e-5, max_iter 100, omega 0.97, ratio 0.25 --

@@ -77,6 +77,9 @@ class XfpStats(C.Structure):
         ("graph", C.c_int),
         ("ms_vec", C.c_double * 3),
         ("vec_launches", C.c_int * 3),
+        ("h2d_bytes", C.c_longlong),
+        ("d2h_bytes", C.c_longlong),
+        ("host_faces", C.c_int),
     ]
 
     def as_dict(self) -> dict:

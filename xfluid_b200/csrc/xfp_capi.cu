@@ -15,6 +15,9 @@
 #include <string>
 #include <vector>
 #include <cstdlib>
+#include <cstdint>
+
+#include <cuda.h>
 
 #include "../../include/xfp.h"
 #include "xfp_common.cuh"
@@ -650,6 +653,114 @@ void fill_stats(xfp_ctx* ctx, xfp_stats* s, int status, double ms_total) {
   }
   s->launches = g_kernel_launches - ctx->launches;
   s->tile_k = ctx->nw;
+  s->h2d_bytes = ctx->h2d_bytes;
+  s->d2h_bytes = ctx->d2h_bytes;
+  s->host_faces = ctx->host_faces;
+}
+
+// ---------------------------------------------------------------- host I/O
+// Whether [p, p + bytes) lies inside one page-locked host allocation that the
+// device addresses at the same pointer (unified addressing), so that kernels
+// may read and write it in place.  Pageable memory, device memory and ranges
+// that leave their allocation answer false; the caller then copies whole
+// arrays.  The allocation's extent comes from the driver
+// (cuPointerGetAttribute, RANGE_START_ADDR / RANGE_SIZE / MAPPED).
+bool host_in_place(const void* p, size_t bytes) {
+  if (!p || bytes == 0) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type != cudaMemoryTypeHost || a.devicePointer != p) return false;
+  using Fn = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+  static const Fn fn = []() -> Fn {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return reinterpret_cast<Fn>(f);
+  }();
+  if (!fn) return false;
+  unsigned long long start = 0;
+  size_t size = 0;
+  int mapped = 0;
+  const CUdeviceptr d = (CUdeviceptr)(uintptr_t)p;
+  if (fn(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, d) != CUDA_SUCCESS) return false;
+  if (fn(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, d) != CUDA_SUCCESS) return false;
+  if (fn(&mapped, CU_POINTER_ATTRIBUTE_MAPPED, d) != CUDA_SUCCESS || !mapped) return false;
+  const uintptr_t b = (uintptr_t)p;
+  return b >= start && b - start <= size && bytes <= size - (b - start);
+}
+
+// Velocities in: device pointers as they are; page-locked host arrays (all
+// three in place, `sparse_ok`) face-sparse -- only the face rows' spans that
+// border fluid are read, straight from host memory; otherwise whole-array
+// copies.  *sparse tells faces_out which way to go back.
+template <typename IOT>
+int faces_in(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk, const IOT* u, const IOT* v, const IOT* w,
+             const IOT** du_, const IOT** dv, const IOT** dw, bool sparse_ok, bool* sparse) {
+  *sparse = false;
+  if (!ctx->opt.device_pointers && sparse_ok && ctx->host_sparse_ok &&
+      host_in_place(u, nu(ni, nj, nk) * sizeof(IOT)) && host_in_place(v, nv(ni, nj, nk) * sizeof(IOT)) &&
+      host_in_place(w, nw_(ni, nj, nk) * sizeof(IOT))) {
+    XFP_CUDA(ctx, ctx->io_u.ensure(nu(ni, nj, nk) * sizeof(IOT)));
+    XFP_CUDA(ctx, ctx->io_v.ensure(nv(ni, nj, nk) * sizeof(IOT)));
+    XFP_CUDA(ctx, ctx->io_w.ensure(nw_(ni, nj, nk) * sizeof(IOT)));
+    XFP_CUDA(ctx, ctx->hio_span.ensure((size_t)std::max<long long>((long long)nj * nk, 1) * sizeof(int2)));
+    XFP_CUDA(ctx, ctx->hio_bytes.ensure(2 * sizeof(unsigned long long)));
+    XFP_CUDA(ctx, cudaMemsetAsync(ctx->hio_bytes.p, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    XFP_CUDA(ctx, fluid_spans(dmat, ni, nj, nk, ctx->hio_span.as<int2>(), ctx->stream));
+    const IOT* src[3] = {u, v, w};
+    IOT* dst[3] = {ctx->io_u.as<IOT>(), ctx->io_v.as<IOT>(), ctx->io_w.as<IOT>()};
+    XFP_CUDA(ctx, face_rows_copy<IOT>(ctx->hio_span.as<int2>(), ni, nj, nk, src, dst,
+                                      ctx->hio_bytes.as<unsigned long long>(), ctx->stream));
+    *du_ = dst[0];
+    *dv = dst[1];
+    *dw = dst[2];
+    *sparse = true;
+    ctx->host_faces = 1;
+    return XFP_OK;
+  }
+  int rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_u, u, nu(ni, nj, nk), du_))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_v, v, nv(ni, nj, nk), dv))) return rc;
+  if ((rc = stage_in<IOT>(ctx, ctx->io_w, w, nw_(ni, nj, nk), dw))) return rc;
+  return XFP_OK;
+}
+
+// Velocities out (host-pointer mode): the same face spans written straight
+// into the caller's arrays, or whole-array copies.  Faces outside the spans
+// are unchanged by the projection, so the caller's copies of them stay right.
+template <typename IOT>
+int faces_out(xfp_ctx* ctx, int ni, int nj, int nk, const IOT* du_, const IOT* dv, const IOT* dw, IOT* u, IOT* v,
+              IOT* w, bool sparse) {
+  if (ctx->opt.device_pointers) return XFP_OK;
+  if (sparse) {
+    const IOT* src[3] = {du_, dv, dw};
+    IOT* dst[3] = {u, v, w};
+    XFP_CUDA(ctx, face_rows_copy<IOT>(ctx->hio_span.as<int2>(), ni, nj, nk, src, dst,
+                                      ctx->hio_bytes.as<unsigned long long>() + 1, ctx->stream));
+    return XFP_OK;
+  }
+  XFP_CUDA(ctx, cudaMemcpyAsync(u, du_, nu(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+  XFP_CUDA(ctx, cudaMemcpyAsync(v, dv, nv(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+  XFP_CUDA(ctx, cudaMemcpyAsync(w, dw, nw_(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+  ctx->d2h_bytes += (long long)((nu(ni, nj, nk) + nv(ni, nj, nk) + nw_(ni, nj, nk)) * sizeof(IOT));
+  return XFP_OK;
+}
+
+// After the call's last stream synchronisation: the face-sparse byte counts.
+int faces_account(xfp_ctx* ctx, bool sparse) {
+  if (!sparse) return XFP_OK;
+  unsigned long long b[2] = {0, 0};
+  XFP_CUDA(ctx, cudaMemcpy(b, ctx->hio_bytes.p, sizeof(b), cudaMemcpyDeviceToHost));
+  ctx->h2d_bytes += (long long)b[0];
+  ctx->d2h_bytes += (long long)b[1];
+  return XFP_OK;
 }
 
 template <typename IOT>
@@ -666,16 +777,20 @@ int project_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* 
   if (!do_apply && !pressure) return fail(ctx, XFP_ERR_ARGS, "pressure output is NULL");
   XFP_CUDA(ctx, cudaSetDevice(ctx->device));
   ctx->launches = g_kernel_launches;
+  ctx->h2d_bytes = ctx->d2h_bytes = 0;
+  ctx->host_faces = 0;
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
   cudaEventRecord(t0, ctx->stream);
   const uint8_t* dmat;
   const IOT *du_, *dv, *dw, *dwu, *dwv, *dww;
+  bool sparse = false;
   if ((rc = stage_in(ctx, ctx->io_mat, mat, ncells(ni, nj, nk), &dmat))) return rc;
-  if ((rc = stage_in<IOT>(ctx, ctx->io_u, u, nu(ni, nj, nk), &du_))) return rc;
-  if ((rc = stage_in<IOT>(ctx, ctx->io_v, v, nv(ni, nj, nk), &dv))) return rc;
-  if ((rc = stage_in<IOT>(ctx, ctx->io_w, w, nw_(ni, nj, nk), &dw))) return rc;
+  // the extrapolation layers of xfp_project_step_* write faces away from the
+  // fluid: those calls move whole arrays
+  if ((rc = faces_in<IOT>(ctx, dmat, ni, nj, nk, u, v, w, &du_, &dv, &dw, ctx->step_layers == 0, &sparse)))
+    return rc;
   if ((rc = stage_in<IOT>(ctx, ctx->io_wu, wu, nu(ni, nj, nk), &dwu))) return rc;
   if ((rc = stage_in<IOT>(ctx, ctx->io_wv, wv, nv(ni, nj, nk), &dwv))) return rc;
   if ((rc = stage_in<IOT>(ctx, ctx->io_ww, ww, nw_(ni, nj, nk), &dww))) return rc;
@@ -708,17 +823,16 @@ int project_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* 
   }
   ev_record(ctx, 4);
   if (!ctx->opt.device_pointers) {
-    if (pressure)
+    if (pressure) {
       XFP_CUDA(ctx, cudaMemcpyAsync(pressure, dp, ncells(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost,
                                     ctx->stream));
-    if (do_apply) {
-      XFP_CUDA(ctx, cudaMemcpyAsync(u, du_, nu(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
-      XFP_CUDA(ctx, cudaMemcpyAsync(v, dv, nv(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
-      XFP_CUDA(ctx, cudaMemcpyAsync(w, dw, nw_(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
+      ctx->d2h_bytes += (long long)(ncells(ni, nj, nk) * sizeof(IOT));
     }
+    if (do_apply && (rc = faces_out<IOT>(ctx, ni, nj, nk, du_, dv, dw, u, v, w, sparse))) return rc;
   }
   cudaEventRecord(t1, ctx->stream);
   XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if ((rc = faces_account(ctx, sparse))) return rc;
   ctx->ms_setup = ev_ms(ctx, 0, 1);
   ctx->ms_factor = ev_ms(ctx, 1, 2);
   ctx->ms_solve = ev_ms(ctx, 2, 3);
@@ -741,12 +855,13 @@ int apply_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, const I
   if (ctx->opt.matrix == XFP_MATRIX_NORMAL && (wu || wv || ww))
     return fail(ctx, XFP_ERR_ARGS, "the normal matrix takes no face weights");
   XFP_CUDA(ctx, cudaSetDevice(ctx->device));
+  ctx->h2d_bytes = ctx->d2h_bytes = 0;
+  ctx->host_faces = 0;
   const uint8_t* dmat;
   const IOT *du_, *dv, *dw, *dwu, *dwv, *dww, *dp;
+  bool sparse = false;
   if ((rc = stage_in(ctx, ctx->io_mat, mat, ncells(ni, nj, nk), &dmat))) return rc;
-  if ((rc = stage_in<IOT>(ctx, ctx->io_u, u, nu(ni, nj, nk), &du_))) return rc;
-  if ((rc = stage_in<IOT>(ctx, ctx->io_v, v, nv(ni, nj, nk), &dv))) return rc;
-  if ((rc = stage_in<IOT>(ctx, ctx->io_w, w, nw_(ni, nj, nk), &dw))) return rc;
+  if ((rc = faces_in<IOT>(ctx, dmat, ni, nj, nk, u, v, w, &du_, &dv, &dw, true, &sparse))) return rc;
   if ((rc = stage_in<IOT>(ctx, ctx->io_wu, wu, nu(ni, nj, nk), &dwu))) return rc;
   if ((rc = stage_in<IOT>(ctx, ctx->io_wv, wv, nv(ni, nj, nk), &dwv))) return rc;
   if ((rc = stage_in<IOT>(ctx, ctx->io_ww, ww, nw_(ni, nj, nk), &dww))) return rc;
@@ -754,13 +869,9 @@ int apply_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, const I
   XFP_CUDA(ctx, (apply_pressure<IOT, IOT>(dmat, dwu, dwv, dww, dp, ni, nj, nk, const_cast<IOT*>(du_),
                                           const_cast<IOT*>(dv), const_cast<IOT*>(dw), ctx->stream,
                                           ctx->opt.matrix)));
-  if (!ctx->opt.device_pointers) {
-    XFP_CUDA(ctx, cudaMemcpyAsync(u, du_, nu(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
-    XFP_CUDA(ctx, cudaMemcpyAsync(v, dv, nv(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
-    XFP_CUDA(ctx, cudaMemcpyAsync(w, dw, nw_(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost, ctx->stream));
-  }
+  if ((rc = faces_out<IOT>(ctx, ni, nj, nk, du_, dv, dw, u, v, w, sparse))) return rc;
   XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  return XFP_OK;
+  return faces_account(ctx, sparse);
 }
 
 template <typename IOT>
@@ -1118,6 +1229,7 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
   for (auto& e : ctx->kern_ev) cudaEventCreate(&e);
   if (const char* e = getenv("XFP_STAGE_SOLVES")) ctx->stage_solves = atoi(e) != 0;
   if (const char* e = getenv("XFP_VEC_BLOCKS")) ctx->vec_blocks = std::max(148, std::min(xfp_host::NBLK_MAX, atoi(e)));
+  if (const char* e = getenv("XFP_HOST_FACES")) ctx->host_sparse_ok = strcmp(e, "full") != 0;
   if (getenv("XFP_TRACE")) {
     ctx->tracing = true;
     ctx->trace.ensure(1024 * 40 * 4 * sizeof(int));

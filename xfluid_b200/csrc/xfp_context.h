@@ -76,6 +76,14 @@ struct xfp_ctx {
   // largest ni of the layout, which sets the rows per tile
   DevBuf bnd;
   int bnd_ni = 0;
+  // host-pointer mode: fluid span per x-line and the two byte counters of
+  // the sparse face transfer; bytes moved by the current call; whether its
+  // velocities went face-sparse; XFP_HOST_FACES=full turns the sparse
+  // transfer off
+  DevBuf hio_span, hio_bytes;
+  long long h2d_bytes = 0, d2h_bytes = 0;
+  int host_faces = 0;
+  int host_sparse_ok = 1;
   // xfp_project_step_*: body force fused into assembly and apply, and the
   // extrapolation layers run after the apply (zero outside such a call);
   // xmarker is the extrapolation's layer-marker scratch
@@ -147,6 +155,7 @@ int stage_in(xfp_ctx* ctx, DevBuf& buf, const T* src, size_t n, const T** dev) {
   if (ctx->opt.device_pointers) { *dev = src; return XFP_OK; }
   XFP_CUDA(ctx, buf.ensure(n * sizeof(T)));
   XFP_CUDA(ctx, cudaMemcpyAsync(buf.p, src, n * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h2d_bytes += (long long)(n * sizeof(T));
   *dev = buf.as<T>();
   return XFP_OK;
 }

@@ -146,6 +146,15 @@ cudaError_t assemble(const uint8_t* mat, const FT* u, const FT* v, const FT* w, 
 template <typename T>
 cudaError_t scatter_dense(const T* x, const Line* lines, int ni, int nj, int nk, T* dense,
                           cudaStream_t st);
+// Host-pointer mode, sparse face transfer (xfp_hostio.cu): fluid span of
+// every x-line ({first, last + 1}, or {0, 0}), and the copy of every face
+// row's fluid-bordering span of u, v, w from src to dst (either side may be
+// page-locked host memory addressed in place); *bytes accumulates the bytes.
+cudaError_t fluid_spans(const uint8_t* mat, int ni, int nj, int nk, int2* span, cudaStream_t st);
+template <typename T>
+cudaError_t face_rows_copy(const int2* span, int ni, int nj, int nk, const T* const src[3], T* const dst[3],
+                           unsigned long long* bytes, cudaStream_t st);
+
 template <typename FT, typename PT>
 cudaError_t apply_pressure(const uint8_t* mat, const FT* wu, const FT* wv, const FT* ww,
                            const PT* p, int ni, int nj, int nk, FT* u, FT* v, FT* w,
