@@ -336,11 +336,11 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
                                     ctx->nj, ctx->nk, M, dsc, part, ctx->vec_blocks, 0, st);
       }));
       XFP_CUDA(ctx, timed_kernel(ctx, 1, it, [&] {
-        return update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), ctx->vec_blocks, st, rsw, perm);
+        return update_xr<VT, DT>(x, r, s, z, M, dsc, ctx->partials.as<double>(), ctx->xr_blocks, st, rsw, perm);
       }));
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_FWD, g1, d)) != XFP_OK) return rc;
       if ((rc = run_sweep<VT, IT, DT>(ctx, SWEEP_BWD, g1, d)) != XFP_OK) return rc;
-      XFP_CUDA(ctx, timed_kernel(ctx, 2, it, [&] { return update_s<VT>(s, z, M, dsc, st, zsw, perm); }));
+      XFP_CUDA(ctx, timed_kernel(ctx, 2, it, [&] { return update_s<VT>(s, z, M, dsc, st, zsw, perm, ctx->s_blocks); }));
     }
     done_iters += K;
     XFP_CUDA(ctx, cudaMemcpyAsync(hsc, dsc, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
@@ -1229,6 +1229,8 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
   for (auto& e : ctx->kern_ev) cudaEventCreate(&e);
   if (const char* e = getenv("XFP_STAGE_SOLVES")) ctx->stage_solves = atoi(e) != 0;
   if (const char* e = getenv("XFP_VEC_BLOCKS")) ctx->vec_blocks = std::max(148, std::min(xfp_host::NBLK_MAX, atoi(e)));
+  if (const char* e = getenv("XFP_XR_BLOCKS")) ctx->xr_blocks = std::max(148, std::min(xfp_host::NBLK_MAX, atoi(e)));
+  if (const char* e = getenv("XFP_S_BLOCKS")) ctx->s_blocks = std::max(148, std::min(148 * 32, atoi(e)));
   if (const char* e = getenv("XFP_HOST_FACES")) ctx->host_sparse_ok = strcmp(e, "full") != 0;
   if (getenv("XFP_TRACE")) {
     ctx->tracing = true;

@@ -96,11 +96,19 @@ struct xfp_ctx {
   // memory with cp.async (1, the default) or load them into registers (0,
   // XFP_STAGE_SOLVES=0)
   int stage_solves = 1;
-  // block cap of the PCG loop's SpMV and x/r update: 148 x 4 measured best at
-  // 256^3 (SpMV 37.4 us and x/r update 23.0 us per launch, against 38.7 and
-  // 27.9 at 148 x 8 and 54.5 / 26.5 at 148 x 2).  XFP_VEC_BLOCKS overrides,
-  // within [148, NBLK_MAX]; the dot's reduction order follows it.
+  // block cap of the PCG loop's SpMV: 148 x 4 measured best at 256^3 (37.4 us
+  // per launch, against 38.7 at 148 x 8 and 54.5 at 148 x 2).  XFP_VEC_BLOCKS
+  // overrides, within [148, NBLK_MAX]; the dot's reduction order follows it.
   int vec_blocks = 148 * 4;
+  // block cap of the x/r update (two groups in flight per thread): 148 x 2
+  // measured best at 256^3 (20.6 us, against 21.5 at 148 x 4 and 26.0 at
+  // 148 x 8).  Its |r|_inf is a max, the same in any order.  XFP_XR_BLOCKS
+  // overrides, within [148, NBLK_MAX].
+  int xr_blocks = 148 * 2;
+  // block cap of the PCG loop's s update: 148 x 8 measured best at 256^3
+  // (14.7 us per launch, against 17.0 at 148 x 16, with two groups in flight
+  // per thread).  XFP_S_BLOCKS overrides, within [148, 148 x 32].
+  int s_blocks = 148 * 8;
   // sizes of the current layout
   int ni = 0, nj = 0, nk = 0, NJt = 0, NKt = 0, nw = 8;
   long long M = 0, rows = 0, nlines_act = 0, ntiles = 0;

@@ -200,7 +200,7 @@ cudaError_t update_xr(VT* x, VT* r, const VT* s, const VT* z, long long M, PcgSc
 // zsw/perm (optional): z is read from zsw[perm[c]] instead of z[c].
 template <typename VT>
 cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st, const VT* zsw = nullptr,
-                     const int* perm = nullptr);
+                     const int* perm = nullptr, int nblk_max = 148 * 16);
 template <typename VT>
 cudaError_t absmax_init(const VT* b, long long M, PcgScalars* sc, double* partials, int nblk_max,
                         double tol, int maxit, cudaStream_t st);

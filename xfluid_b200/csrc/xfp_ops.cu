@@ -782,22 +782,43 @@ __device__ __forceinline__ void update_xr_body(unsigned bid, unsigned nblk, VT* 
   const VT nalpha = -alpha;
   double m = 0.0;
   const long long G = M >> 2;
-  for (long long q = (long long)bid * blockDim.x + threadIdx.x; q < G; q += (long long)nblk * blockDim.x) {
+  const long long stride = (long long)nblk * blockDim.x;
+  // two groups in flight per thread: the next group's loads are issued before
+  // the current group's arithmetic and stores (two buffers, no copies)
+  struct Buf {
+    VT x[4], r[4], s[4], z[4];
+    int p;
+  };
+  auto load = [&](Buf& B, long long q) {
     const long long c = 4 * q;
-    VT xv[4], rv[4], sv[4], zv[4];
-    ldg(xv, x + c);
-    ldg(rv, r + c);
-    ldg(sv, s + c);
-    ldg(zv, z + c);
+    ldg(B.x, x + c);
+    ldg(B.r, r + c);
+    ldg(B.s, s + c);
+    ldg(B.z, z + c);
+    B.p = rsw != nullptr ? perm[c] : 0;
+  };
+  auto finish = [&](Buf& B, long long q) {
+    const long long c = 4 * q;
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-      xv[e] = add_rn(xv[e], mul_rn(alpha, sv[e]));
-      rv[e] = add_rn(rv[e], mul_rn(nalpha, zv[e]));
-      m = fmax(m, (double)fabs(rv[e]));
+      B.x[e] = add_rn(B.x[e], mul_rn(alpha, B.s[e]));
+      B.r[e] = add_rn(B.r[e], mul_rn(nalpha, B.z[e]));
+      m = fmax(m, (double)fabs(B.r[e]));
     }
-    stg(x + c, xv);
-    stg(r + c, rv);
-    if (rsw != nullptr) stg(rsw + perm[c], rv);
+    stg(x + c, B.x);
+    stg(r + c, B.r);
+    if (rsw != nullptr) stg(rsw + B.p, B.r);
+  };
+  Buf A, B;
+  long long q = (long long)bid * blockDim.x + threadIdx.x;
+  if (q < G) load(A, q);
+  for (; q < G; q += 2 * stride) {
+    const bool nb = q + stride < G;
+    if (nb) load(B, q + stride);
+    finish(A, q);
+    if (!nb) break;
+    if (q + 2 * stride < G) load(A, q + 2 * stride);
+    finish(B, q + stride);
   }
   double t = block_max(m, sh);
   if (threadIdx.x == 0) partials[bid] = t;
@@ -863,14 +884,31 @@ __device__ __forceinline__ void update_s_body(unsigned bid, unsigned nblk, VT* _
   if (*(volatile int*)&sc->done) return;
   const VT beta = (VT)sc->beta;
   const long long G = M >> 2;
-  for (long long q = (long long)bid * blockDim.x + threadIdx.x; q < G; q += (long long)nblk * blockDim.x) {
+  const long long stride = (long long)nblk * blockDim.x;
+  // two groups in flight per thread (as in update_xr_body)
+  struct Buf {
+    VT s[4], z[4];
+  };
+  auto load = [&](Buf& B, long long q) {
     const long long c = 4 * q;
-    VT sv[4], zv[4];
-    ldg(sv, s + c);
-    ldg(zv, zsw != nullptr ? zsw + perm[c] : z + c);
+    ldg(B.s, s + c);
+    ldg(B.z, zsw != nullptr ? zsw + perm[c] : z + c);
+  };
+  auto finish = [&](Buf& B, long long q) {
 #pragma unroll
-    for (int e = 0; e < 4; ++e) sv[e] = add_rn(zv[e], mul_rn(beta, sv[e]));
-    stg(s + c, sv);
+    for (int e = 0; e < 4; ++e) B.s[e] = add_rn(B.z[e], mul_rn(beta, B.s[e]));
+    stg(s + 4 * q, B.s);
+  };
+  Buf A, B;
+  long long q = (long long)bid * blockDim.x + threadIdx.x;
+  if (q < G) load(A, q);
+  for (; q < G; q += 2 * stride) {
+    const bool nb = q + stride < G;
+    if (nb) load(B, q + stride);
+    finish(A, q);
+    if (!nb) break;
+    if (q + 2 * stride < G) load(A, q + 2 * stride);
+    finish(B, q + stride);
   }
 }
 template <typename VT>
@@ -889,19 +927,19 @@ __global__ void batch_update_s_kernel(const BatchSeg* __restrict__ segs, int nse
 }
 template <typename VT>
 cudaError_t update_s(VT* s, const VT* z, long long M, PcgScalars* sc, cudaStream_t st, const VT* zsw,
-                     const int* perm) {
-  // 4-cell groups over at most 148 x 16 blocks (one thread per group measured
+                     const int* perm, int nblk_max) {
+  // 4-cell groups over at most nblk_max blocks (one thread per group measured
   // slower at 256^3: more blocks, fewer groups per thread)
-  int blocks = (int)std::min<long long>((M / 4 + 255) / 256, 148LL * 16);
+  int blocks = (int)std::min<long long>((M / 4 + 255) / 256, (long long)nblk_max);
   if (blocks < 1) blocks = 1;
   ++g_kernel_launches;
   update_s_kernel<VT><<<blocks, 256, 0, st>>>(s, z, M, sc, zsw, perm);
   return cudaGetLastError();
 }
 template cudaError_t update_s<double>(double*, const double*, long long, PcgScalars*, cudaStream_t, const double*,
-                                      const int*);
+                                      const int*, int);
 template cudaError_t update_s<float>(float*, const float*, long long, PcgScalars*, cudaStream_t, const float*,
-                                     const int*);
+                                     const int*, int);
 
 // |b|_inf, tolerance and loop state at the start of a solve (pcg_solver.h:247-254).
 template <typename VT>
