@@ -508,7 +508,11 @@ def ours(args, rank, world):
                 "frac": (achieved / peak) if achieved else None,
                 "traffic": (tr * rows) if tr is not None else None,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_launch_s * 1000,
-                "sweep_share_of_step": sweep_ms / ms if ms > 0 else None}
+                # events sample every 8th iteration: the share scales the
+                # average launch by the launches that did work (two per
+                # iteration, the preconditioner's first pair included)
+                "sweep_share_of_step": (avg_launch_s * 1000 * sum(2 * max(int(s["iterations"]), 1) for _, s in stats)
+                                        / ms) if ms > 0 else None}
     # the PCG loop's vector kernels, event-timed the same way (launches after
     # convergence excluded): algorithmic bytes per unknown row (FP32 vectors
     # and coefficients) -- SpMV s + 4 coefficients + z = 24; x/r update x, s,
@@ -520,8 +524,10 @@ def ours(args, rank, world):
         if vec_n[k] > 0 and vec_ms[k] > 0:
             avg = vec_ms[k] / vec_n[k]
             gbs = bpr * rows / (avg / 1000.0) / 1e9
-            vk[name] = {"avg_launch_ms": avg, "launches": vec_n[k], "algorithmic_bytes_per_row": bpr,
-                        "achieved_gbs": gbs, "frac": gbs / peak, "share_of_step": vec_ms[k] / ms}
+            # launches that did work: one per iteration (the s update: all but the last)
+            work = sum(max(int(s_["iterations"]) - (k == 2), 0) for _, s_ in stats)
+            vk[name] = {"avg_launch_ms": avg, "launches_timed": vec_n[k], "algorithmic_bytes_per_row": bpr,
+                        "achieved_gbs": gbs, "frac": gbs / peak, "share_of_step": avg * work / ms}
     roofline["vector_kernels"] = vk
 
     # ---------------- e2e: through the C ABI from pinned host buffers ----------------
@@ -1013,6 +1019,11 @@ def particles_leg(stream, barrier, max_over_ranks, cpu=True):
 
 
 def main():
+    # The roofline's solve and vector-kernel durations come from CUDA events on
+    # every 8th PCG iteration of the timed projections (the library records
+    # none by default: an event between two launches serialises them, and
+    # events on every launch cost 6 % of a projection).
+    os.environ.setdefault("XFP_KERNEL_EVENTS", "8")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=25)

@@ -181,7 +181,10 @@ int run_sweep(xfp_ctx* ctx, int op, const SweepGrid& g, const SweepData<VT, IT, 
                                        ", tile height " + std::to_string(ctx->nw) + "): " + cudaGetErrorString(e));
   }
   int grid = std::min(maxg, g.ntiles);
-  const bool timed = op != SWEEP_FACTOR && ctx->sweep_ev_used + 2 <= (int)ctx->sweep_ev.size();
+  // the forward and backward solve of every event_every-th iteration
+  const int ord = op != SWEEP_FACTOR ? ctx->sweep_ord++ : -1;
+  const bool timed = ctx->event_every > 0 && ord >= 0 && (ord / 2) % ctx->event_every == 0 &&
+                     ctx->sweep_ev_used + 2 <= (int)ctx->sweep_ev.size();
   if (timed) cudaEventRecord(ctx->sweep_ev[ctx->sweep_ev_used], ctx->stream);
   SweepGrid gl = g;
   if (ctx->expire_next_sweep) {
@@ -192,6 +195,7 @@ int run_sweep(xfp_ctx* ctx, int op, const SweepGrid& g, const SweepData<VT, IT, 
   if (timed) {
     cudaEventRecord(ctx->sweep_ev[ctx->sweep_ev_used + 1], ctx->stream);
     ctx->sweep_work[ctx->sweep_ev_used / 2] = 1;
+    ctx->sweep_ord_of[ctx->sweep_ev_used / 2] = ord;
     ctx->sweep_ev_used += 2;
   }
   return XFP_OK;
@@ -200,7 +204,8 @@ int run_sweep(xfp_ctx* ctx, int op, const SweepGrid& g, const SweepData<VT, IT, 
 // Event pair around one vector-kernel launch of the PCG loop (kind, iteration).
 template <typename F>
 cudaError_t timed_kernel(xfp_ctx* ctx, int kind, int iter, F&& launch) {
-  const bool timed = ctx->kern_ev_used + 2 <= (int)ctx->kern_ev.size();
+  const bool timed = ctx->event_every > 0 && iter % ctx->event_every == 0 &&
+                     ctx->kern_ev_used + 2 <= (int)ctx->kern_ev.size();
   if (timed) cudaEventRecord(ctx->kern_ev[ctx->kern_ev_used], ctx->stream);
   const cudaError_t e = launch();
   if (timed) {
@@ -311,6 +316,7 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   if ((rc = sweep_copies<VT, IT, DT>(ctx, L, inv, r, gs, 2, &d)) != XFP_OK) return rc;
   const int first_timed = ctx->sweep_ev_used / 2;
   const int first_kern = ctx->kern_ev_used / 2;
+  ctx->sweep_ord = 0;
   const SweepGrid& g0 = gs[0];
   const SweepGrid& g1 = gs[1];
   // with a sweep layout, r is kept in both layouts (update_xr writes both)
@@ -352,7 +358,8 @@ int pcg(xfp_ctx* ctx, const VT* const A[4], const VT* b, VT* x, VT* r, VT* s, VT
   // the preconditioner's two sweeps, then two per iteration but the last (the
   // converged iteration skips its preconditioner): 2 * iterations did work;
   // the launches after them in the last chunk returned at once
-  for (int q = first_timed + 2 * std::max(hsc->iters, 1); q < ctx->sweep_ev_used / 2; ++q) ctx->sweep_work[q] = 0;
+  for (int q = first_timed; q < ctx->sweep_ev_used / 2; ++q)
+    if (ctx->sweep_ord_of[q] >= 2 * std::max(hsc->iters, 1)) ctx->sweep_work[q] = 0;
   // vector kernels of this call that ran after convergence: SpMV and the x/r
   // update of iterations past the last, the s update of the last and later
   for (int q = first_kern; q < ctx->kern_ev_used / 2; ++q)
@@ -1222,6 +1229,7 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
   for (auto& e : ctx->ev) cudaEventCreate(&e);
   ctx->sweep_ev.resize(2048);
   ctx->sweep_work.assign(1024, 0);
+  ctx->sweep_ord_of.assign(1024, 0);
   for (auto& e : ctx->sweep_ev) cudaEventCreate(&e);
   ctx->kern_ev.resize(3072);
   ctx->kern_kind.assign(1536, -1);
@@ -1229,6 +1237,7 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
   for (auto& e : ctx->kern_ev) cudaEventCreate(&e);
   if (const char* e = getenv("XFP_STAGE_SOLVES")) ctx->stage_solves = atoi(e) != 0;
   if (const char* e = getenv("XFP_VEC_BLOCKS")) ctx->vec_blocks = std::max(148, std::min(xfp_host::NBLK_MAX, atoi(e)));
+  if (const char* e = getenv("XFP_KERNEL_EVENTS")) ctx->event_every = std::max(0, atoi(e));
   if (const char* e = getenv("XFP_XR_BLOCKS")) ctx->xr_blocks = std::max(148, std::min(xfp_host::NBLK_MAX, atoi(e)));
   if (const char* e = getenv("XFP_S_BLOCKS")) ctx->s_blocks = std::max(148, std::min(148 * 32, atoi(e)));
   if (const char* e = getenv("XFP_HOST_FACES")) ctx->host_sparse_ok = strcmp(e, "full") != 0;

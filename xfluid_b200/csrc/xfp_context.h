@@ -105,6 +105,14 @@ struct xfp_ctx {
   // 148 x 8).  Its |r|_inf is a max, the same in any order.  XFP_XR_BLOCKS
   // overrides, within [148, NBLK_MAX].
   int xr_blocks = 148 * 2;
+  // CUDA events around the PCG loop's solve and vector-kernel launches
+  // (xfp_stats.ms_sweeps, ms_vec), on every event_every-th iteration; 0 (the
+  // default) records none.  An event between two launches serialises them:
+  // events on every launch cost 1.3 ms of a 21.8 ms projection at 256^3.
+  // XFP_KERNEL_EVENTS=N sets it.
+  int event_every = 0;
+  int sweep_ord = 0;              // triangular-solve launches of the current PCG loop
+  std::vector<int> sweep_ord_of;  // per timed sweep entry: its launch ordinal
   // block cap of the PCG loop's s update: 148 x 8 measured best at 256^3
   // (14.7 us per launch, against 17.0 at 148 x 16, with two groups in flight
   // per thread).  XFP_S_BLOCKS overrides, within [148, 148 x 32].
