@@ -385,6 +385,15 @@ float ev_ms(xfp_ctx* ctx, int a, int b) {
 // the layout at each candidate height, assembles and factors in FP32 and
 // times two forward+backward sweep pairs; the fastest height is cached in the
 // context for that shape and precision.
+// The compute stream waits for the face gather of the I/O stream (host-pointer
+// mode, face-sparse) before it first reads the velocities.
+int inputs_ready(xfp_ctx* ctx) {
+  if (!ctx->io_pending) return XFP_OK;
+  ctx->io_pending = false;
+  XFP_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_io_in, 0));
+  return XFP_OK;
+}
+
 template <typename IOT>
 int tune_tile_height(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const IOT* du_, const IOT* dv,
                      const IOT* dw, const IOT* dwu, const IOT* dwv, const IOT* dww) {
@@ -402,6 +411,7 @@ int tune_tile_height(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, 
   cudaStream_t st = ctx->stream;
   float best = 0.f;
   int best_nw = 8;
+  if (int rc0 = inputs_ready(ctx)) return rc0;
   cudaEvent_t e0, e1;
   XFP_CUDA(ctx, cudaEventCreate(&e0));
   XFP_CUDA(ctx, cudaEventCreate(&e1));
@@ -466,6 +476,7 @@ int solve_core(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* dmat, const 
   ctx->kern_ev_used = 0;
   if ((rc = build_layout(ctx, dmat, ni, nj, nk)) != XFP_OK) return rc;
   if ((rc = ensure_compact(ctx, prec)) != XFP_OK) return rc;
+  if ((rc = inputs_ready(ctx)) != XFP_OK) return rc;
   const Line* lines = ctx->lines.as<Line>();
   const long long M = ctx->M;
   ctx->iters = 0; ctx->refinements = 0; ctx->res = 0; ctx->bnorm = 0;
@@ -711,6 +722,11 @@ template <typename IOT>
 int faces_in(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk, const IOT* u, const IOT* v, const IOT* w,
              const IOT** du_, const IOT** dv, const IOT** dw, bool sparse_ok, bool* sparse) {
   *sparse = false;
+  if (ctx->io_stream) {
+    // a call that stopped early may have left its gather running
+    XFP_CUDA(ctx, cudaStreamSynchronize(ctx->io_stream));
+    ctx->io_pending = false;
+  }
   if (!ctx->opt.device_pointers && sparse_ok && ctx->host_sparse_ok &&
       host_in_place(u, nu(ni, nj, nk) * sizeof(IOT)) && host_in_place(v, nv(ni, nj, nk) * sizeof(IOT)) &&
       host_in_place(w, nw_(ni, nj, nk) * sizeof(IOT))) {
@@ -719,12 +735,24 @@ int faces_in(xfp_ctx* ctx, const uint8_t* dmat, int ni, int nj, int nk, const IO
     XFP_CUDA(ctx, ctx->io_w.ensure(nw_(ni, nj, nk) * sizeof(IOT)));
     XFP_CUDA(ctx, ctx->hio_span.ensure((size_t)std::max<long long>((long long)nj * nk, 1) * sizeof(int2)));
     XFP_CUDA(ctx, ctx->hio_bytes.ensure(2 * sizeof(unsigned long long)));
-    XFP_CUDA(ctx, cudaMemsetAsync(ctx->hio_bytes.p, 0, 2 * sizeof(unsigned long long), ctx->stream));
-    XFP_CUDA(ctx, fluid_spans(dmat, ni, nj, nk, ctx->hio_span.as<int2>(), ctx->stream));
+    // the gather runs on the I/O stream after the material has arrived, beside
+    // the layout build on the compute stream; inputs_ready() joins them before
+    // the first assembly
+    cudaStream_t gs = ctx->io_stream ? ctx->io_stream : ctx->stream;
+    if (ctx->io_stream) {
+      XFP_CUDA(ctx, cudaEventRecord(ctx->ev_io_mat, ctx->stream));
+      XFP_CUDA(ctx, cudaStreamWaitEvent(gs, ctx->ev_io_mat, 0));
+    }
+    XFP_CUDA(ctx, cudaMemsetAsync(ctx->hio_bytes.p, 0, 2 * sizeof(unsigned long long), gs));
+    XFP_CUDA(ctx, fluid_spans(dmat, ni, nj, nk, ctx->hio_span.as<int2>(), gs));
     const IOT* src[3] = {u, v, w};
     IOT* dst[3] = {ctx->io_u.as<IOT>(), ctx->io_v.as<IOT>(), ctx->io_w.as<IOT>()};
     XFP_CUDA(ctx, face_rows_copy<IOT>(ctx->hio_span.as<int2>(), ni, nj, nk, src, dst,
-                                      ctx->hio_bytes.as<unsigned long long>(), ctx->stream));
+                                      ctx->hio_bytes.as<unsigned long long>(), gs));
+    if (ctx->io_stream) {
+      XFP_CUDA(ctx, cudaEventRecord(ctx->ev_io_in, gs));
+      ctx->io_pending = true;
+    }
     *du_ = dst[0];
     *dv = dst[1];
     *dw = dst[2];
@@ -762,6 +790,7 @@ int faces_out(xfp_ctx* ctx, int ni, int nj, int nk, const IOT* du_, const IOT* d
 
 // After the call's last stream synchronisation: the face-sparse byte counts.
 int faces_account(xfp_ctx* ctx, bool sparse) {
+  if (ctx->io_stream) XFP_CUDA(ctx, cudaStreamSynchronize(ctx->io_stream));
   if (!sparse) return XFP_OK;
   unsigned long long b[2] = {0, 0};
   XFP_CUDA(ctx, cudaMemcpy(b, ctx->hio_bytes.p, sizeof(b), cudaMemcpyDeviceToHost));
@@ -815,6 +844,17 @@ int project_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* 
     dp = ctx->io_p.as<IOT>();
   }
   if ((rc = solution_dense<IOT>(ctx, dp))) return rc;
+  // host-pointer mode: the dense pressure is final here; its download runs on
+  // the I/O stream beside the apply (which only reads it)
+  bool p_async = false;
+  if (!ctx->opt.device_pointers && pressure && ctx->io_stream) {
+    XFP_CUDA(ctx, cudaEventRecord(ctx->ev_io_p, ctx->stream));
+    XFP_CUDA(ctx, cudaStreamWaitEvent(ctx->io_stream, ctx->ev_io_p, 0));
+    XFP_CUDA(ctx, cudaMemcpyAsync(pressure, dp, ncells(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost,
+                                  ctx->io_stream));
+    ctx->d2h_bytes += (long long)(ncells(ni, nj, nk) * sizeof(IOT));
+    p_async = true;
+  }
   if (do_apply) {
     IOT* mu = const_cast<IOT*>(du_);
     IOT* mv = const_cast<IOT*>(dv);
@@ -830,12 +870,17 @@ int project_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, IOT* 
   }
   ev_record(ctx, 4);
   if (!ctx->opt.device_pointers) {
-    if (pressure) {
+    if (pressure && !p_async) {
       XFP_CUDA(ctx, cudaMemcpyAsync(pressure, dp, ncells(ni, nj, nk) * sizeof(IOT), cudaMemcpyDeviceToHost,
                                     ctx->stream));
       ctx->d2h_bytes += (long long)(ncells(ni, nj, nk) * sizeof(IOT));
     }
     if (do_apply && (rc = faces_out<IOT>(ctx, ni, nj, nk, du_, dv, dw, u, v, w, sparse))) return rc;
+  }
+  if (p_async) {
+    // the call's total includes the pressure download
+    XFP_CUDA(ctx, cudaEventRecord(ctx->ev_io_mat, ctx->io_stream));
+    XFP_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_io_mat, 0));
   }
   cudaEventRecord(t1, ctx->stream);
   XFP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -873,6 +918,7 @@ int apply_impl(xfp_ctx* ctx, int ni, int nj, int nk, const uint8_t* mat, const I
   if ((rc = stage_in<IOT>(ctx, ctx->io_wv, wv, nv(ni, nj, nk), &dwv))) return rc;
   if ((rc = stage_in<IOT>(ctx, ctx->io_ww, ww, nw_(ni, nj, nk), &dww))) return rc;
   if ((rc = stage_in<IOT>(ctx, ctx->io_p, pressure, ncells(ni, nj, nk), &dp))) return rc;
+  if ((rc = inputs_ready(ctx))) return rc;
   XFP_CUDA(ctx, (apply_pressure<IOT, IOT>(dmat, dwu, dwv, dww, dp, ni, nj, nk, const_cast<IOT*>(du_),
                                           const_cast<IOT*>(dv), const_cast<IOT*>(dw), ctx->stream,
                                           ctx->opt.matrix)));
@@ -1227,6 +1273,13 @@ int xfp_create(xfp_ctx** out, const xfp_options* opt) {
     ctx->own_stream = true;
   }
   for (auto& e : ctx->ev) cudaEventCreate(&e);
+  if (cudaStreamCreateWithFlags(&ctx->io_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_io_mat, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_io_in, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_io_p, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->io_stream = nullptr;
+  }
   ctx->sweep_ev.resize(2048);
   ctx->sweep_work.assign(1024, 0);
   ctx->sweep_ord_of.assign(1024, 0);
@@ -1277,6 +1330,12 @@ int xfp_destroy(xfp_ctx* ctx) {
   for (auto& e : ctx->sweep_ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : ctx->kern_ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->io_stream) {
+    cudaStreamSynchronize(ctx->io_stream);
+    cudaStreamDestroy(ctx->io_stream);
+  }
+  for (cudaEvent_t e : {ctx->ev_io_mat, ctx->ev_io_in, ctx->ev_io_p})
     if (e) cudaEventDestroy(e);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -81,6 +81,13 @@ struct xfp_ctx {
   // velocities went face-sparse; XFP_HOST_FACES=full turns the sparse
   // transfer off
   DevBuf hio_span, hio_bytes;
+  // host-pointer mode: a second stream for the transfers that can run beside
+  // the compute stream (the face gather beside the layout build, the dense
+  // pressure download beside the apply), and its events; io_pending: the
+  // compute stream has still to wait for io_in before it reads the faces
+  cudaStream_t io_stream = nullptr;
+  cudaEvent_t ev_io_mat = nullptr, ev_io_in = nullptr, ev_io_p = nullptr;
+  bool io_pending = false;
   long long h2d_bytes = 0, d2h_bytes = 0;
   int host_faces = 0;
   int host_sparse_ok = 1;
