@@ -94,12 +94,17 @@ typedef struct xfp_stats {
   double ms_apply;       /* pressure scatter + velocity update */
   double ms_total;       /* whole call incl. host<->device copies */
   double bytes;          /* algorithmic bytes moved by the device kernels */
-  double ms_sweeps;      /* device time of the MIC(0) triangular-solve sweeps (CUDA events) */
+  double ms_sweeps;      /* device time of the timed MIC(0) triangular-solve sweeps (CUDA events on
+                            the forward and backward solve of every N-th PCG iteration, with the
+                            environment variable XFP_KERNEL_EVENTS=N at context creation; by
+                            default none are timed and this is 0: an event between two launches
+                            serialises them) */
   int sweeps;            /* triangular-solve sweep launches timed in ms_sweeps */
   long long launches;    /* device kernels launched by this call */
   int tile_k;            /* sweep tile height the call used (k-lines) */
   int graph;             /* 1: the PCG iterations ran as a CUDA graph; 0: launched one by one */
-  double ms_vec[3];      /* device time of the PCG loop's vector kernels (CUDA events): SpMV + dot,
+  double ms_vec[3];      /* device time of the PCG loop's vector kernels (CUDA events, sampled as
+                            ms_sweeps is): SpMV + dot,
                             x/r update, s update -- launches after convergence excluded */
   int vec_launches[3];   /* launches timed in ms_vec, per kernel */
   long long h2d_bytes;   /* host-pointer mode: bytes this call moved host -> device */
