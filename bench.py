@@ -508,7 +508,7 @@ def ours(args, rank, world):
                 "frac": (achieved / peak) if achieved else None,
                 "traffic": (tr * rows) if tr is not None else None,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_launch_s * 1000,
-                # events sample every 8th iteration: the share scales the
+                # events sample every 16th iteration: the share scales the
                 # average launch by the launches that did work (two per
                 # iteration, the preconditioner's first pair included)
                 "sweep_share_of_step": (avg_launch_s * 1000 * sum(2 * max(int(s["iterations"]), 1) for _, s in stats)
@@ -1020,10 +1020,11 @@ def particles_leg(stream, barrier, max_over_ranks, cpu=True):
 
 def main():
     # The roofline's solve and vector-kernel durations come from CUDA events on
-    # every 8th PCG iteration of the timed projections (the library records
-    # none by default: an event between two launches serialises them, and
-    # events on every launch cost 6 % of a projection).
-    os.environ.setdefault("XFP_KERNEL_EVENTS", "8")
+    # every 16th PCG iteration of the timed projections, the preconditioner's
+    # first solve pair included (the library records none by default: an
+    # event between two launches serialises them, and events on every launch
+    # cost 6 % of a projection).
+    os.environ.setdefault("XFP_KERNEL_EVENTS", "16")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=25)
